@@ -1,0 +1,230 @@
+/*
+ * kate_b200.h - C ABI of the B200 state-vector gate-application path.
+ *
+ * Drop-in for the hot path of the Kate simulator (Line-fr/Kate): circuit
+ * building, the compile passes (scheduling, fusion, grouping, allocation),
+ * gate merging, simulation and measurement. The reference is a header-only
+ * C++ class API with no C ABI; each entry point below names the reference
+ * interface it replaces (paths within the reference project). The C++ facade
+ * include/kate_b200/Kate.hpp wraps these calls with the reference's own class
+ * and method names.
+ *
+ * Conventions (identical to the reference):
+ *  - qubit q is bit q of the amplitude index (little-endian);
+ *  - gate ids: 0 dense, 2 Hadamard, 3 CNOT (qbits[0] target, qbits[1]
+ *    control), 4 CRk (phase e^{2 pi i / 2^k} on |11>, k = optarg),
+ *    5 TOFFOLI (qbits[0], qbits[1] controls, qbits[2] target), 6 RX and
+ *    7 RZ (accepted, and applied as no-ops: the reference implements no
+ *    arithmetic for them; pass rotations as dense gates);
+ *  - a dense gate on k qubits is a row-major 2^k x 2^k complex matrix, given
+ *    as 2*4^k doubles (re, im interleaved); bit i of its local index is
+ *    qbits[i];
+ *  - states are 2^n complex amplitudes, (re, im) interleaved.
+ *
+ * Errors: every call returns a kate_status; kate_last_error() gives the
+ * message of the last failure on the calling thread. The reference prints
+ * and continues instead (HIPcode/HIPpreprocessor.hpp:35-40,
+ * backendagnosticcode/basic_host_types.hpp:203-244).
+ *
+ * Ownership: host buffers are the caller's; device memory belongs to the
+ * library and is released by the matching destroy call. A simulator copies
+ * the program at creation, as the reference's Simulator copies its circuit
+ * (HIPcode/simulator.hpp:243-270). Calls on one object are not re-entrant;
+ * distinct objects may be used from distinct threads.
+ */
+#ifndef KATE_B200_H
+#define KATE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define KATE_API __attribute__((visibility("default")))
+#else
+#define KATE_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    KATE_OK = 0,
+    KATE_EINVAL = 1,   /* bad argument: qubit out of range, duplicate qubit, size mismatch */
+    KATE_ENOMEM = 2,   /* device or host allocation failed, or admission budget exceeded */
+    KATE_ECUDA = 3,    /* a CUDA runtime call failed (no device, launch failure, ...) */
+    KATE_ETIMEDOUT = 4,/* a bounded device wait gave up */
+    KATE_ESTATE = 5    /* call out of order (e.g. measuring before executing) */
+} kate_status;
+
+typedef enum {
+    KATE_C128 = 0, /* complex128 state, FP64 arithmetic (the reference's only form) */
+    KATE_C64 = 1   /* complex64 state; fused dense blocks on tensor cores (3xTF32) */
+} kate_precision;
+
+/* Gate identifiers, as the reference defines them (backendagnosticcode/agnosticpreprocessor.hpp:28-33). */
+#define KATE_DENSE 0
+#define KATE_HADAMARD 2
+#define KATE_CNOT 3
+#define KATE_CRK 4
+#define KATE_TOFFOLI 5
+#define KATE_RX 6
+#define KATE_RZ 7
+
+typedef struct kate_circuit kate_circuit;
+typedef struct kate_sim kate_sim;
+typedef struct kate_plan kate_plan;
+
+/* Message of the last failed call on this thread ("" if none). */
+KATE_API const char* kate_last_error(void);
+/* Library version string. */
+KATE_API const char* kate_version(void);
+
+/* ---- circuit building: backendagnosticcode/QuantumCircuit.hpp:18-37 ---- */
+
+/* Circuit(int nqbits)  QuantumCircuit.hpp:18-20. 1 <= nqbits <= 40. */
+KATE_API kate_status kate_circuit_create(int nqbits, kate_circuit** out);
+KATE_API kate_status kate_circuit_destroy(kate_circuit* c);
+/* Deep copy (the reference passes circuits by value). */
+KATE_API kate_status kate_circuit_clone(const kate_circuit* c, kate_circuit** out);
+KATE_API kate_status kate_circuit_nqbits(const kate_circuit* c, int* out);
+
+/* appendGate(Gate(id, qbits, optarg))  QuantumCircuit.hpp:25-37 with
+ * basic_host_types.hpp:198-228. id must be 2..7; qubit count must match the
+ * id (H 1, CNOT 2, CRk 2, TOFFOLI 3; RX/RZ 1). */
+KATE_API kate_status kate_circuit_append_gate(kate_circuit* c, int id, const int* qbits, int nq, int optarg);
+/* appendGate(Gate(Matrix<Complex>, qbits))  basic_host_types.hpp:229-245.
+ * mat: 2*4^nq doubles, row-major, interleaved. 1 <= nq <= 10. */
+KATE_API kate_status kate_circuit_append_dense(kate_circuit* c, const double* mat, const int* qbits, int nq);
+
+KATE_API kate_status kate_circuit_num_gates(const kate_circuit* c, int* out);
+/* Reads gate i. qbits receives *nq ints (capacity 64); dense (nullable)
+ * receives 2*4^nq doubles for a dense gate. */
+KATE_API kate_status kate_circuit_get_gate(const kate_circuit* c, int i, int* id, int* qbits, int* nq, int* optarg,
+                                  double* dense);
+
+/* ---- compile passes: backendagnosticcode/Circuit.hpp ---- */
+
+/* gateScheduling()  Circuit.hpp:12-98 */
+KATE_API kate_status kate_circuit_schedule(kate_circuit* c);
+/* gateFusion(qbitsizelimit = 5, merge_time_matters = 1e-6)  Circuit.hpp:99-175 */
+KATE_API kate_status kate_circuit_fuse(kate_circuit* c, int qbitsizelimit, double merge_time_matters);
+/* gateGrouping(qbitgroupsize = 8)  Circuit.hpp:176-206 */
+KATE_API kate_status kate_circuit_group(kate_circuit* c, int qbitgroupsize);
+/* allocate(numberofgpulog2 = 0, maxlocalqbitnumber = 300)  Circuit.hpp:207-348 */
+KATE_API kate_status kate_circuit_allocate(kate_circuit* c, int numberofgpulog2, int maxlocalqbitnumber);
+/* compileDefault(numberofgpulog2 = 0, maxlocalqbitnumber = 300)  QuantumCircuit.hpp:126-204 */
+KATE_API kate_status kate_circuit_compile_default(kate_circuit* c, int numberofgpulog2, int maxlocalqbitnumber);
+/* compileOPT(5, 1e-6, 10, 0, 300)  Circuit.hpp:349-354 */
+KATE_API kate_status kate_circuit_compile_opt(kate_circuit* c, int qbit_matrix_merge_size_limit, double merge_time_matters,
+                                     int groupsize, int numberofgpulog2, int maxlocalqbitnumber);
+
+KATE_API kate_status kate_circuit_num_groups(const kate_circuit* c, int* out);
+/* Group i: *end = index one past its last gate, qbits (capacity 64) its
+ * sorted qubit set  (QuantumCircuit.hpp:14). */
+KATE_API kate_status kate_circuit_get_group(const kate_circuit* c, int i, int* end, int* qbits, int* nq);
+KATE_API kate_status kate_circuit_num_instructions(const kate_circuit* c, int* out);
+/* Instruction i: *kind 0 = swap pairs (qbits holds 2*pairs ints, capacity
+ * 256), 1 = compute next group  (QuantumCircuit.hpp:17). */
+KATE_API kate_status kate_circuit_get_instruction(const kate_circuit* c, int i, int* kind, int* qbits, int* nq);
+/* initial_permutation / final_inverse_permutation, nqbits ints each;
+ * *valid = 0 before compilation  (QuantumCircuit.hpp:15-16). */
+KATE_API kate_status kate_circuit_get_permutations(const kate_circuit* c, int* initial, int* final_inverse, int* valid);
+
+/* mergeGate / CPUmergeGate(gates [begin, end))  CPUcode/GateMerger.hpp:8-55,
+ * HIPcode/GateMerger.hpp:43-109: the product of the gates as one dense
+ * gate on the sorted union of their qubits, in FP64. out_qbits receives *k
+ * ints (k <= 10), out_mat 2*4^k doubles. */
+KATE_API kate_status kate_merge_gates(const kate_circuit* c, int begin, int end, int* out_qbits, int* k, double* out_mat);
+
+/* exportqcx(filename)  Circuit.hpp:763-774 */
+KATE_API kate_status kate_circuit_export_qcx(const kate_circuit* c, const char* path);
+
+/* ---- simulation: HIPcode/simulator.hpp:220-811 ---- */
+
+/* Simulator(circuit, 1)  HIPcode/simulator.hpp:243-300. Copies the circuit
+ * (compiling it with compileDefault(0) first if it has no instructions, as
+ * the reference does), plans the B200 group passes and allocates the state
+ * on `device`. precision: kate_precision. */
+KATE_API kate_status kate_sim_create(const kate_circuit* c, int precision, int device, kate_sim** out);
+KATE_API kate_status kate_sim_destroy(kate_sim* s);
+
+/* execute(displaytime)  HIPcode/simulator.hpp:301-353: initialise |0..0>,
+ * run every instruction, measure. theta_phi (nullable) receives 2*n
+ * doubles, (theta, phi) per qubit, the reference's proba_state. Blocks until
+ * done. */
+KATE_API kate_status kate_sim_execute(kate_sim* s, double* theta_phi);
+/* execute(proba_state& in, displaytime)  HIPcode/simulator.hpp:354-406: the
+ * initial state is the product state given by 2*n doubles (theta, phi). */
+KATE_API kate_status kate_sim_execute_from(kate_sim* s, const double* theta_phi_in, double* theta_phi_out);
+
+/* Asynchronous form for callers that own a CUDA stream (cudaStream_t passed
+ * as void*; NULL = the simulator's own stream): initialise and run every
+ * group pass, no measurement, no host synchronisation. */
+KATE_API kate_status kate_sim_run_async(kate_sim* s, void* stream);
+/* Waits for work queued on the simulator's streams. */
+KATE_API kate_status kate_sim_synchronize(kate_sim* s);
+/* Measurement of the current state (proba_state, 2*n doubles). */
+KATE_API kate_status kate_sim_proba_state(kate_sim* s, double* theta_phi);
+
+/* The full state after execution, in the reference's amplitude order
+ * (its Simulator/CPUSimulator state array): 2*2^n doubles (c128), or 2*2^n
+ * floats for a c64 simulator when `out` is float* (pass KATE_C64 layout).
+ * For a c64 simulator the values are widened to double. */
+KATE_API kate_status kate_sim_get_state(kate_sim* s, double* out);
+/* Replaces the state (2*2^n doubles) - e.g. to resume from a dump. */
+KATE_API kate_status kate_sim_set_state(kate_sim* s, const double* in);
+
+/* Per-qubit <Z_q> = sum |a|^2 (1 - 2 bit_q), n doubles, FP64 reduction. */
+KATE_API kate_status kate_sim_expect_z(kate_sim* s, double* out);
+/* Probability of each computational basis state: 2^n doubles (n <= 30). */
+KATE_API kate_status kate_sim_probabilities(kate_sim* s, double* out);
+/* `shots` samples of the computational basis from |a|^2, seeded; out
+ * receives shots uint64 basis indices in the reference's qubit labels. */
+KATE_API kate_status kate_sim_sample(kate_sim* s, int shots, uint64_t seed, uint64_t* out);
+
+/* Runs init + every pass once on the simulator's stream with a CUDA event
+ * between launches and returns each pass's device time: ms[i] for pass i
+ * (capacity kate_sim_num_passes), *init_ms for the initialisation. */
+KATE_API kate_status kate_sim_profile_passes(kate_sim* s, float* ms, float* init_ms);
+/* Number of kernels one kate_sim_run_async launches. */
+KATE_API kate_status kate_sim_launches_per_run(kate_sim* s, int* out);
+
+/* Device pointer of the state and its layout: phys[q] receives the bit
+ * position currently holding qubit q (n ints). */
+KATE_API kate_status kate_sim_state_device(kate_sim* s, void** dptr, int* phys);
+KATE_API kate_status kate_sim_nqbits(kate_sim* s, int* out);
+
+/* Plan introspection: number of group passes, and pass i's tile qubits
+ * (capacity 16) and the number of gates it applies. */
+KATE_API kate_status kate_sim_num_passes(kate_sim* s, int* out);
+KATE_API kate_status kate_sim_get_pass(kate_sim* s, int i, int* tile_qbits, int* m, int* ngates);
+
+/* ---- group-pass plans (host only, no device needed) ----
+ * The single-GPU replacement for gateGrouping + allocate + the per-group
+ * launches (backendagnosticcode/Circuit.hpp:176-348,
+ * HIPcode/simulator.hpp:760-810): which qubits each HBM pass keeps on chip,
+ * which ops it applies, and how it permutes the tile on write. */
+#define KATE_PLAN_NO_REMAP 1u   /* keep the low physical bits fixed */
+#define KATE_PLAN_NO_FUSE1Q 2u  /* do not multiply single-qubit chains */
+KATE_API kate_status kate_plan_create(const kate_circuit* c, int max_tile, int coalesce, unsigned flags,
+                                      kate_plan** out);
+KATE_API kate_status kate_plan_destroy(kate_plan* p);
+KATE_API kate_status kate_plan_num_passes(const kate_plan* p, int* out);
+/* info[4] = {m, nops, op0, ncb}; tphys[16] physical bit of tile bit t;
+ * outsrc[16]: on store, output tile bit t takes input tile bit outsrc[t]. */
+KATE_API kate_status kate_plan_get_pass(const kate_plan* p, int i, int* info, uint8_t* tphys, uint8_t* outsrc);
+KATE_API kate_status kate_plan_num_ops(const kate_plan* p, int* out);
+/* ints[18] = {kind, k, tb[5], ftb[5], fpos[5], tmask}; *pmask; vals[2 + 2*1024]
+ * = phase (re, im) then the op's matrix or diagonal table (re, im pairs).
+ * kinds: 0 dense, 1 H, 2 controlled X, 3 controlled phase, 4 diagonal. */
+KATE_API kate_status kate_plan_get_op(const kate_plan* p, int i, int* ints, uint64_t* pmask, double* vals);
+/* phys[q]: physical bit of logical qubit q after the last pass;
+ * label_to_logical[x]: logical qubit held by program label x. */
+KATE_API kate_status kate_plan_final_layout(const kate_plan* p, int* phys, int* label_to_logical);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KATE_B200_H */

@@ -1,0 +1,352 @@
+"""Python mirror of Kate's circuit/simulator API over libkate_b200.so.
+
+The names and argument meanings follow the reference's C++ API (Line-fr/Kate):
+``Gate`` (backendagnosticcode/basic_host_types.hpp:190-296), ``Circuit``
+(backendagnosticcode/Circuit.hpp, QuantumCircuit.hpp), ``Simulator``
+(HIPcode/simulator.hpp:220-811), ``mergeGate`` (CPUcode/GateMerger.hpp:8-55)
+and ``proba_state`` (basic_host_types.hpp:319-336). Every call goes through
+the C ABI declared in include/kate_b200.h; nothing here computes amplitudes.
+Failures raise ``KateError`` (the reference prints and continues).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _lib
+
+Hadamard = 2
+CNOT = 3
+CRk = 4
+TOFFOLI = 5
+RX = 6
+RZ = 7
+DENSE = 0
+
+C128 = 0
+C64 = 1
+
+KATE_OK, KATE_EINVAL, KATE_ENOMEM, KATE_ECUDA, KATE_ETIMEDOUT, KATE_ESTATE = range(6)
+
+
+class KateError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"[kate status {status}] {msg}")
+        self.status = status
+
+
+def _check(st: int):
+    if st != KATE_OK:
+        raise KateError(st, _lib.last_error())
+
+
+_ip = ctypes.POINTER(ctypes.c_int)
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+def _iarr(v) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(v, dtype=np.int32))
+
+
+class Gate:
+    """Gate(identifier, qbits, optarg=0) or Gate(matrix, qbits) for a dense gate.
+
+    ``matrix`` is a 2^k x 2^k complex array, row-major; bit i of its local
+    index is ``qbits[i]``.
+    """
+
+    def __init__(self, what, qbits: Sequence[int], optarg: int = 0):
+        self.qbits = [int(q) for q in qbits]
+        if isinstance(what, (int, np.integer)):
+            self.identifier = int(what)
+            self.optarg = int(optarg)
+            self.densecontent = None
+        else:
+            m = np.ascontiguousarray(np.asarray(what, dtype=np.complex128))
+            self.identifier = DENSE
+            self.optarg = 0
+            self.densecontent = m
+
+    def as_tuple(self):
+        return (self.identifier, list(self.qbits), self.optarg, self.densecontent)
+
+    def __repr__(self):
+        return f"Gate(id={self.identifier}, qbits={self.qbits}, optarg={self.optarg})"
+
+
+class proba_state:
+    """Per-qubit (theta, phi) pairs, as in the reference."""
+
+    def __init__(self, val):
+        self.val = [(float(a), float(b)) for a, b in val]
+
+    def as_array(self) -> np.ndarray:
+        return np.array(self.val, dtype=np.float64).reshape(-1, 2)
+
+    def print(self):
+        for i, (t, p) in enumerate(self.val):
+            print(f"Qbit {i} : teta={t} , phi={p}")
+
+
+class Circuit:
+    """Kate::Circuit: gate list plus the compile passes."""
+
+    def __init__(self, nqbits: int, gates: Sequence = (), _handle=None):
+        self._lib = _lib.lib()
+        if _handle is not None:
+            self._h = _handle
+        else:
+            h = ctypes.c_void_p()
+            _check(self._lib.kate_circuit_create(int(nqbits), ctypes.byref(h)))
+            self._h = h
+        for g in gates:
+            self.appendGate(g)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            self._lib.kate_circuit_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def nqbits(self) -> int:
+        v = ctypes.c_int()
+        _check(self._lib.kate_circuit_nqbits(self._h, ctypes.byref(v)))
+        return v.value
+
+    def copy(self) -> "Circuit":
+        h = ctypes.c_void_p()
+        _check(self._lib.kate_circuit_clone(self._h, ctypes.byref(h)))
+        return Circuit(0, _handle=h)
+
+    def appendGate(self, gate):
+        if isinstance(gate, tuple):
+            gate = Gate(gate[3] if gate[0] == DENSE else gate[0], gate[1], gate[2])
+        q = _iarr(gate.qbits)
+        if gate.identifier == DENSE:
+            d = np.ascontiguousarray(gate.densecontent, dtype=np.complex128).view(np.float64).ravel()
+            _check(self._lib.kate_circuit_append_dense(self._h, d.ctypes.data_as(_dp), q.ctypes.data_as(_ip),
+                                                       len(gate.qbits)))
+        else:
+            _check(self._lib.kate_circuit_append_gate(self._h, gate.identifier, q.ctypes.data_as(_ip),
+                                                      len(gate.qbits), gate.optarg))
+
+    # --- passes (backendagnosticcode/Circuit.hpp) ---
+    def gateScheduling(self):
+        _check(self._lib.kate_circuit_schedule(self._h))
+
+    def gateFusion(self, qbitsizelimit: int = 5, merge_time_matters: float = 0.000001):
+        _check(self._lib.kate_circuit_fuse(self._h, int(qbitsizelimit), float(merge_time_matters)))
+
+    def gateGrouping(self, qbitgroupsize: int = 8):
+        _check(self._lib.kate_circuit_group(self._h, int(qbitgroupsize)))
+
+    def allocate(self, numberofgpulog2: int = 0, maxlocalqbitnumber: int = 300):
+        _check(self._lib.kate_circuit_allocate(self._h, int(numberofgpulog2), int(maxlocalqbitnumber)))
+
+    def compileDefault(self, numberofgpulog2: int = 0, maxlocalqbitnumber: int = 300):
+        _check(self._lib.kate_circuit_compile_default(self._h, int(numberofgpulog2), int(maxlocalqbitnumber)))
+
+    def compileOPT(self, qbit_matrix_merge_size_limit=5, merge_time_matters=0.000001, groupsize=10,
+                   numberofgpulog2=0, maxlocalqbitnumber=300):
+        _check(self._lib.kate_circuit_compile_opt(self._h, int(qbit_matrix_merge_size_limit),
+                                                  float(merge_time_matters), int(groupsize), int(numberofgpulog2),
+                                                  int(maxlocalqbitnumber)))
+
+    def exportqcx(self, filename: str):
+        _check(self._lib.kate_circuit_export_qcx(self._h, filename.encode()))
+
+    # --- introspection ---
+    def num_gates(self) -> int:
+        v = ctypes.c_int()
+        _check(self._lib.kate_circuit_num_gates(self._h, ctypes.byref(v)))
+        return v.value
+
+    @property
+    def gate_set_ordered(self) -> List[Tuple]:
+        out = []
+        q = np.zeros(64, dtype=np.int32)
+        d = np.zeros(2 * 4 ** 10, dtype=np.float64)
+        gid, nq, opt = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        for i in range(self.num_gates()):
+            _check(self._lib.kate_circuit_get_gate(self._h, i, ctypes.byref(gid), q.ctypes.data_as(_ip),
+                                                   ctypes.byref(nq), ctypes.byref(opt), d.ctypes.data_as(_dp)))
+            k = nq.value
+            dense = None
+            if gid.value == DENSE:
+                dim = 1 << k
+                dense = d[: 2 * dim * dim].view(np.complex128).reshape(dim, dim).copy()
+            out.append((gid.value, [int(x) for x in q[:k]], opt.value, dense))
+        return out
+
+    @property
+    def groups(self):
+        n = ctypes.c_int()
+        _check(self._lib.kate_circuit_num_groups(self._h, ctypes.byref(n)))
+        out = []
+        q = np.zeros(64, dtype=np.int32)
+        end, nq = ctypes.c_int(), ctypes.c_int()
+        for i in range(n.value):
+            _check(self._lib.kate_circuit_get_group(self._h, i, ctypes.byref(end), q.ctypes.data_as(_ip),
+                                                    ctypes.byref(nq)))
+            out.append((end.value, [int(x) for x in q[: nq.value]]))
+        return out
+
+    @property
+    def instructions(self):
+        n = ctypes.c_int()
+        _check(self._lib.kate_circuit_num_instructions(self._h, ctypes.byref(n)))
+        out = []
+        q = np.zeros(256, dtype=np.int32)
+        kind, nq = ctypes.c_int(), ctypes.c_int()
+        for i in range(n.value):
+            _check(self._lib.kate_circuit_get_instruction(self._h, i, ctypes.byref(kind), q.ctypes.data_as(_ip),
+                                                          ctypes.byref(nq)))
+            out.append((kind.value, [int(x) for x in q[: nq.value]]))
+        return out
+
+    def permutations(self):
+        n = self.nqbits
+        a = np.zeros(n, dtype=np.int32)
+        b = np.zeros(n, dtype=np.int32)
+        v = ctypes.c_int()
+        _check(self._lib.kate_circuit_get_permutations(self._h, a.ctypes.data_as(_ip), b.ctypes.data_as(_ip),
+                                                       ctypes.byref(v)))
+        return (list(a), list(b)) if v.value else (None, None)
+
+    def merge(self, begin: int, end: int) -> Gate:
+        """mergeGate of gates [begin, end) of this circuit."""
+        q = np.zeros(64, dtype=np.int32)
+        d = np.zeros(2 * 4 ** 10, dtype=np.float64)
+        k = ctypes.c_int()
+        _check(self._lib.kate_merge_gates(self._h, int(begin), int(end), q.ctypes.data_as(_ip), ctypes.byref(k),
+                                          d.ctypes.data_as(_dp)))
+        dim = 1 << k.value
+        return Gate(d[: 2 * dim * dim].view(np.complex128).reshape(dim, dim).copy(), [int(x) for x in q[: k.value]])
+
+
+def mergeGate(gates: Sequence[Gate]) -> Gate:
+    """CPUmergeGate / mergeGate (CPUcode/GateMerger.hpp:8-55): FP64 product
+    of the gates on the sorted union of their qubits."""
+    gs = [g if isinstance(g, Gate) else Gate(g[3] if g[0] == DENSE else g[0], g[1], g[2]) for g in gates]
+    n = 1 + max(q for g in gs for q in g.qbits)
+    c = Circuit(n, gs)
+    return c.merge(0, len(gs))
+
+
+class Simulator:
+    """Kate::Simulator on one B200 (HIPcode/simulator.hpp:220-811)."""
+
+    def __init__(self, circuit: Circuit, number_of_gpu: int = 1, precision: int = C128, device: int = 0):
+        self._lib = _lib.lib()
+        h = ctypes.c_void_p()
+        _check(self._lib.kate_sim_create(circuit.handle, int(precision), int(device), ctypes.byref(h)))
+        self._h = h
+        v = ctypes.c_int()
+        _check(self._lib.kate_sim_nqbits(self._h, ctypes.byref(v)))
+        self.nqbits = v.value
+        self.precision = precision
+
+    def __del__(self):
+        self.close()
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            self._lib.kate_sim_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def execute(self, arg=False, displaytime: bool = False) -> proba_state:
+        """execute(displaytime) or execute(proba_state_in, displaytime)."""
+        out = np.zeros(2 * self.nqbits, dtype=np.float64)
+        if isinstance(arg, proba_state):
+            pin = arg.as_array().ravel().copy()
+            _check(self._lib.kate_sim_execute_from(self._h, pin.ctypes.data_as(_dp), out.ctypes.data_as(_dp)))
+        else:
+            _check(self._lib.kate_sim_execute(self._h, out.ctypes.data_as(_dp)))
+        return proba_state(out.reshape(-1, 2))
+
+    def run_async(self, stream: int = 0):
+        _check(self._lib.kate_sim_run_async(self._h, ctypes.c_void_p(stream or None)))
+
+    def synchronize(self):
+        _check(self._lib.kate_sim_synchronize(self._h))
+
+    def proba(self) -> proba_state:
+        out = np.zeros(2 * self.nqbits, dtype=np.float64)
+        _check(self._lib.kate_sim_proba_state(self._h, out.ctypes.data_as(_dp)))
+        return proba_state(out.reshape(-1, 2))
+
+    def state(self, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """The state in the reference's amplitude order (complex128)."""
+        if out is None:
+            out = np.empty(1 << self.nqbits, dtype=np.complex128)
+        _check(self._lib.kate_sim_get_state(self._h, out.view(np.float64).ctypes.data_as(_dp)))
+        return out
+
+    def set_state(self, st: np.ndarray):
+        a = np.ascontiguousarray(st, dtype=np.complex128)
+        _check(self._lib.kate_sim_set_state(self._h, a.view(np.float64).ctypes.data_as(_dp)))
+
+    def expect_z(self) -> np.ndarray:
+        out = np.zeros(self.nqbits, dtype=np.float64)
+        _check(self._lib.kate_sim_expect_z(self._h, out.ctypes.data_as(_dp)))
+        return out
+
+    def probabilities(self) -> np.ndarray:
+        out = np.zeros(1 << self.nqbits, dtype=np.float64)
+        _check(self._lib.kate_sim_probabilities(self._h, out.ctypes.data_as(_dp)))
+        return out
+
+    def sample(self, shots: int, seed: int = 0) -> np.ndarray:
+        out = np.zeros(max(1, shots), dtype=np.uint64)
+        _check(self._lib.kate_sim_sample(self._h, int(shots), ctypes.c_uint64(seed),
+                                         out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))))
+        return out[:shots]
+
+    def state_device(self):
+        """(device pointer, physical bit of each qubit label)."""
+        p = ctypes.c_void_p()
+        phys = np.zeros(self.nqbits, dtype=np.int32)
+        _check(self._lib.kate_sim_state_device(self._h, ctypes.byref(p), phys.ctypes.data_as(_ip)))
+        return p.value, list(phys)
+
+    def profile_passes(self):
+        """(init_ms, [ms per pass]) from CUDA events between launches."""
+        n = ctypes.c_int()
+        _check(self._lib.kate_sim_num_passes(self._h, ctypes.byref(n)))
+        ms = (ctypes.c_float * max(1, n.value))()
+        init = ctypes.c_float()
+        _check(self._lib.kate_sim_profile_passes(self._h, ms, ctypes.byref(init)))
+        return init.value, [ms[i] for i in range(n.value)]
+
+    def launches_per_run(self) -> int:
+        v = ctypes.c_int()
+        _check(self._lib.kate_sim_launches_per_run(self._h, ctypes.byref(v)))
+        return v.value
+
+    def passes(self):
+        n = ctypes.c_int()
+        _check(self._lib.kate_sim_num_passes(self._h, ctypes.byref(n)))
+        out = []
+        q = np.zeros(16, dtype=np.int32)
+        m, ng = ctypes.c_int(), ctypes.c_int()
+        for i in range(n.value):
+            _check(self._lib.kate_sim_get_pass(self._h, i, q.ctypes.data_as(_ip), ctypes.byref(m), ctypes.byref(ng)))
+            out.append(([int(x) for x in q[: m.value]], ng.value))
+        return out
+
+
+__all__ = ["Gate", "Circuit", "Simulator", "mergeGate", "proba_state", "KateError", "Hadamard", "CNOT", "CRk",
+           "TOFFOLI", "RX", "RZ", "DENSE", "C128", "C64"]

@@ -1,0 +1,89 @@
+"""Loads libkate_b200.so (built in-tree by kate_b200/build.py) and declares
+the C ABI of include/kate_b200.h for ctypes. There is no fallback: if the
+library is missing the import fails loudly."""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libkate_b200.so")
+
+_lib = None
+
+_c = ctypes
+_i, _d, _vp = _c.c_int, _c.c_double, _c.c_void_p
+_ip, _dp = _c.POINTER(_c.c_int), _c.POINTER(_c.c_double)
+_u64, _u64p = _c.c_uint64, _c.POINTER(_c.c_uint64)
+_vpp = _c.POINTER(_c.c_void_p)
+
+# name -> argtypes (every function returns kate_status unless listed in _RET)
+SIGNATURES = {
+    "kate_last_error": [],
+    "kate_version": [],
+    "kate_circuit_create": [_i, _vpp],
+    "kate_circuit_destroy": [_vp],
+    "kate_circuit_clone": [_vp, _vpp],
+    "kate_circuit_nqbits": [_vp, _ip],
+    "kate_circuit_append_gate": [_vp, _i, _ip, _i, _i],
+    "kate_circuit_append_dense": [_vp, _dp, _ip, _i],
+    "kate_circuit_num_gates": [_vp, _ip],
+    "kate_circuit_get_gate": [_vp, _i, _ip, _ip, _ip, _ip, _dp],
+    "kate_circuit_schedule": [_vp],
+    "kate_circuit_fuse": [_vp, _i, _d],
+    "kate_circuit_group": [_vp, _i],
+    "kate_circuit_allocate": [_vp, _i, _i],
+    "kate_circuit_compile_default": [_vp, _i, _i],
+    "kate_circuit_compile_opt": [_vp, _i, _d, _i, _i, _i],
+    "kate_circuit_num_groups": [_vp, _ip],
+    "kate_circuit_get_group": [_vp, _i, _ip, _ip, _ip],
+    "kate_circuit_num_instructions": [_vp, _ip],
+    "kate_circuit_get_instruction": [_vp, _i, _ip, _ip, _ip],
+    "kate_circuit_get_permutations": [_vp, _ip, _ip, _ip],
+    "kate_merge_gates": [_vp, _i, _i, _ip, _ip, _dp],
+    "kate_circuit_export_qcx": [_vp, _c.c_char_p],
+    "kate_sim_create": [_vp, _i, _i, _vpp],
+    "kate_sim_destroy": [_vp],
+    "kate_sim_execute": [_vp, _dp],
+    "kate_sim_execute_from": [_vp, _dp, _dp],
+    "kate_sim_run_async": [_vp, _vp],
+    "kate_sim_synchronize": [_vp],
+    "kate_sim_proba_state": [_vp, _dp],
+    "kate_sim_get_state": [_vp, _dp],
+    "kate_sim_set_state": [_vp, _dp],
+    "kate_sim_expect_z": [_vp, _dp],
+    "kate_sim_probabilities": [_vp, _dp],
+    "kate_sim_sample": [_vp, _i, _u64, _u64p],
+    "kate_sim_state_device": [_vp, _vpp, _ip],
+    "kate_sim_nqbits": [_vp, _ip],
+    "kate_sim_profile_passes": [_vp, _c.POINTER(_c.c_float), _c.POINTER(_c.c_float)],
+    "kate_sim_launches_per_run": [_vp, _ip],
+    "kate_sim_num_passes": [_vp, _ip],
+    "kate_sim_get_pass": [_vp, _i, _ip, _ip, _ip],
+    "kate_plan_create": [_vp, _i, _i, _c.c_uint, _vpp],
+    "kate_plan_destroy": [_vp],
+    "kate_plan_num_passes": [_vp, _ip],
+    "kate_plan_get_pass": [_vp, _i, _ip, _c.POINTER(_c.c_uint8), _c.POINTER(_c.c_uint8)],
+    "kate_plan_num_ops": [_vp, _ip],
+    "kate_plan_get_op": [_vp, _i, _ip, _u64p, _dp],
+    "kate_plan_final_layout": [_vp, _ip, _ip],
+}
+_RET = {"kate_last_error": _c.c_char_p, "kate_version": _c.c_char_p}
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m kate_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, args in SIGNATURES.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = _RET.get(name, _i)
+        _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    return lib().kate_last_error().decode(errors="replace")

@@ -1,0 +1,522 @@
+// C ABI (include/kate_b200.h) over the C++ circuit, passes and simulator.
+#include "kate_b200.h"
+
+#include <cstring>
+#include <exception>
+#include <string>
+
+#include "circuit.hpp"
+#include "plan.hpp"
+#include "sim.hpp"
+
+struct kate_circuit {
+    kate::Program prog;
+};
+struct kate_sim {
+    kate::Simulator* sim = nullptr;
+};
+struct kate_plan {
+    kate::Plan plan;
+    std::vector<DevPass> passes;
+    std::vector<DevOp> ops;
+};
+
+namespace {
+thread_local std::string g_last_error;
+
+kate_status fail(kate_status s, const std::string& msg) {
+    g_last_error = msg;
+    return s;
+}
+
+kate_status from_msg(const std::string& msg, kate_status code = KATE_EINVAL) {
+    if (msg.empty()) return KATE_OK;
+    return fail(code, msg);
+}
+
+// Simulator messages from CUDA calls carry the call name; classify them.
+kate_status sim_status(const std::string& msg) {
+    if (msg.empty()) return KATE_OK;
+    if (msg.find("cudaMalloc") != std::string::npos || msg.find("MemoryAllocation") != std::string::npos)
+        return fail(KATE_ENOMEM, msg);
+    if (msg.find("no state") != std::string::npos) return fail(KATE_ESTATE, msg);
+    if (msg.find("cuda") != std::string::npos || msg.find("launch") != std::string::npos)
+        return fail(KATE_ECUDA, msg);
+    return fail(KATE_EINVAL, msg);
+}
+
+template <typename F>
+kate_status guarded(F&& f) {
+    try {
+        return f();
+    } catch (const std::bad_alloc&) {
+        return fail(KATE_ENOMEM, "host allocation failed");
+    } catch (const std::exception& e) {
+        return fail(KATE_EINVAL, e.what());
+    }
+}
+
+#define REQUIRE(cond, msg) \
+    if (!(cond)) return fail(KATE_EINVAL, msg)
+}  // namespace
+
+extern "C" {
+
+const char* kate_last_error(void) { return g_last_error.c_str(); }
+const char* kate_version(void) { return "kate_b200 0.1 (sm_100a)"; }
+
+kate_status kate_circuit_create(int nqbits, kate_circuit** out) {
+    return guarded([&] {
+        REQUIRE(out, "null output pointer");
+        REQUIRE(nqbits >= 1 && nqbits <= KATE_MAX_QUBITS, "nqbits must be in [1, 40]");
+        auto* c = new kate_circuit();
+        c->prog.nqbits = nqbits;
+        *out = c;
+        return KATE_OK;
+    });
+}
+
+kate_status kate_circuit_destroy(kate_circuit* c) {
+    delete c;
+    return KATE_OK;
+}
+
+kate_status kate_circuit_clone(const kate_circuit* c, kate_circuit** out) {
+    return guarded([&] {
+        REQUIRE(c && out, "null pointer");
+        *out = new kate_circuit(*c);
+        return KATE_OK;
+    });
+}
+
+kate_status kate_circuit_nqbits(const kate_circuit* c, int* out) {
+    REQUIRE(c && out, "null pointer");
+    *out = c->prog.nqbits;
+    return KATE_OK;
+}
+
+kate_status kate_circuit_append_gate(kate_circuit* c, int id, const int* qbits, int nq, int optarg) {
+    return guarded([&] {
+        REQUIRE(c, "null circuit");
+        REQUIRE(nq >= 0 && nq <= 64 && (nq == 0 || qbits), "bad qubit list");
+        if (id == kate::G_DENSE) return fail(KATE_EINVAL, "use kate_circuit_append_dense for dense gates");
+        kate::Gate g;
+        g.id = id;
+        g.qbits.assign(qbits, qbits + nq);
+        g.optarg = optarg;
+        std::string e = kate::validate_gate(c->prog, g);
+        if (!e.empty()) return fail(e.find("after gateGrouping") != std::string::npos ? KATE_ESTATE : KATE_EINVAL, e);
+        c->prog.gates.push_back(std::move(g));
+        return KATE_OK;
+    });
+}
+
+kate_status kate_circuit_append_dense(kate_circuit* c, const double* mat, const int* qbits, int nq) {
+    return guarded([&] {
+        REQUIRE(c && mat && qbits, "null pointer");
+        REQUIRE(nq >= 1 && nq <= 10, "dense gates take 1 to 10 qubits");
+        kate::Gate g;
+        g.id = kate::G_DENSE;
+        g.qbits.assign(qbits, qbits + nq);
+        size_t len = (size_t)1 << (2 * nq);
+        g.dense.resize(len);
+        for (size_t i = 0; i < len; i++) g.dense[i] = kate::Cx(mat[2 * i], mat[2 * i + 1]);
+        std::string e = kate::validate_gate(c->prog, g);
+        if (!e.empty()) return fail(e.find("after gateGrouping") != std::string::npos ? KATE_ESTATE : KATE_EINVAL, e);
+        c->prog.gates.push_back(std::move(g));
+        return KATE_OK;
+    });
+}
+
+kate_status kate_circuit_num_gates(const kate_circuit* c, int* out) {
+    REQUIRE(c && out, "null pointer");
+    *out = (int)c->prog.gates.size();
+    return KATE_OK;
+}
+
+kate_status kate_circuit_get_gate(const kate_circuit* c, int i, int* id, int* qbits, int* nq, int* optarg,
+                                  double* dense) {
+    REQUIRE(c && id && qbits && nq && optarg, "null pointer");
+    REQUIRE(i >= 0 && i < (int)c->prog.gates.size(), "gate index out of range");
+    const kate::Gate& g = c->prog.gates[i];
+    *id = g.id;
+    *nq = (int)g.qbits.size();
+    for (size_t k = 0; k < g.qbits.size(); k++) qbits[k] = g.qbits[k];
+    *optarg = g.optarg;
+    if (dense && g.id == kate::G_DENSE)
+        for (size_t k = 0; k < g.dense.size(); k++) {
+            dense[2 * k] = g.dense[k].re;
+            dense[2 * k + 1] = g.dense[k].im;
+        }
+    return KATE_OK;
+}
+
+kate_status kate_circuit_schedule(kate_circuit* c) {
+    return guarded([&] {
+        REQUIRE(c, "null circuit");
+        return from_msg(kate::pass_schedule(c->prog));
+    });
+}
+
+kate_status kate_circuit_fuse(kate_circuit* c, int k, double mtm) {
+    return guarded([&] {
+        REQUIRE(c, "null circuit");
+        REQUIRE(k >= 1, "qbitsizelimit must be >= 1");
+        kate::Program tmp = c->prog;
+        std::string e = kate::pass_fuse(tmp, k, mtm);
+        if (!e.empty()) return fail(KATE_EINVAL, e);
+        c->prog = std::move(tmp);
+        return KATE_OK;
+    });
+}
+
+kate_status kate_circuit_group(kate_circuit* c, int m) {
+    return guarded([&] {
+        REQUIRE(c, "null circuit");
+        REQUIRE(m >= 1, "qbitgroupsize must be >= 1");
+        return from_msg(kate::pass_group(c->prog, m));
+    });
+}
+
+kate_status kate_circuit_allocate(kate_circuit* c, int g, int maxlocal) {
+    return guarded([&] {
+        REQUIRE(c, "null circuit");
+        kate::Program tmp = c->prog;
+        std::string e = kate::pass_allocate(tmp, g, maxlocal);
+        if (!e.empty()) return fail(KATE_EINVAL, e);
+        c->prog = std::move(tmp);
+        return KATE_OK;
+    });
+}
+
+kate_status kate_circuit_compile_default(kate_circuit* c, int g, int maxlocal) {
+    return guarded([&] {
+        REQUIRE(c, "null circuit");
+        kate::Program tmp = c->prog;
+        std::string e = kate::pass_compile_default(tmp, g, maxlocal);
+        if (!e.empty()) return fail(KATE_EINVAL, e);
+        c->prog = std::move(tmp);
+        return KATE_OK;
+    });
+}
+
+kate_status kate_circuit_compile_opt(kate_circuit* c, int k, double mtm, int groupsize, int g, int maxlocal) {
+    return guarded([&] {
+        REQUIRE(c, "null circuit");
+        kate::Program tmp = c->prog;
+        std::string e = kate::pass_schedule(tmp);
+        if (e.empty()) e = kate::pass_fuse(tmp, k, mtm);
+        if (e.empty()) e = kate::pass_group(tmp, groupsize);
+        if (e.empty()) e = kate::pass_allocate(tmp, g, maxlocal);
+        if (!e.empty()) return fail(KATE_EINVAL, e);
+        c->prog = std::move(tmp);
+        return KATE_OK;
+    });
+}
+
+kate_status kate_circuit_num_groups(const kate_circuit* c, int* out) {
+    REQUIRE(c && out, "null pointer");
+    *out = (int)c->prog.groups.size();
+    return KATE_OK;
+}
+
+kate_status kate_circuit_get_group(const kate_circuit* c, int i, int* end, int* qbits, int* nq) {
+    REQUIRE(c && end && qbits && nq, "null pointer");
+    REQUIRE(i >= 0 && i < (int)c->prog.groups.size(), "group index out of range");
+    auto& g = c->prog.groups[i];
+    *end = g.first;
+    *nq = (int)g.second.size();
+    for (size_t k = 0; k < g.second.size(); k++) qbits[k] = g.second[k];
+    return KATE_OK;
+}
+
+kate_status kate_circuit_num_instructions(const kate_circuit* c, int* out) {
+    REQUIRE(c && out, "null pointer");
+    *out = (int)c->prog.instructions.size();
+    return KATE_OK;
+}
+
+kate_status kate_circuit_get_instruction(const kate_circuit* c, int i, int* kind, int* qbits, int* nq) {
+    REQUIRE(c && kind && qbits && nq, "null pointer");
+    REQUIRE(i >= 0 && i < (int)c->prog.instructions.size(), "instruction index out of range");
+    auto& ins = c->prog.instructions[i];
+    REQUIRE(ins.second.size() <= 256, "instruction too long for the 256-entry buffer");
+    *kind = ins.first;
+    *nq = (int)ins.second.size();
+    for (size_t k = 0; k < ins.second.size(); k++) qbits[k] = ins.second[k];
+    return KATE_OK;
+}
+
+kate_status kate_circuit_get_permutations(const kate_circuit* c, int* initial, int* final_inverse, int* valid) {
+    REQUIRE(c && valid, "null pointer");
+    const auto& p = c->prog;
+    *valid = (int)(p.initial_permutation.size() == (size_t)p.nqbits);
+    if (*valid) {
+        REQUIRE(initial && final_inverse, "null permutation buffer");
+        for (int i = 0; i < p.nqbits; i++) {
+            initial[i] = p.initial_permutation[i];
+            final_inverse[i] = p.final_inverse_permutation[i];
+        }
+    }
+    return KATE_OK;
+}
+
+kate_status kate_merge_gates(const kate_circuit* c, int begin, int end, int* out_qbits, int* k, double* out_mat) {
+    return guarded([&] {
+        REQUIRE(c && out_qbits && k && out_mat, "null pointer");
+        REQUIRE(begin >= 0 && end <= (int)c->prog.gates.size() && begin < end, "bad gate range");
+        std::vector<kate::Gate> block(c->prog.gates.begin() + begin, c->prog.gates.begin() + end);
+        kate::Gate g;
+        std::string e = kate::merge_gates(block, &g);
+        if (!e.empty()) return fail(KATE_EINVAL, e);
+        *k = (int)g.qbits.size();
+        for (int i = 0; i < *k; i++) out_qbits[i] = g.qbits[i];
+        for (size_t i = 0; i < g.dense.size(); i++) {
+            out_mat[2 * i] = g.dense[i].re;
+            out_mat[2 * i + 1] = g.dense[i].im;
+        }
+        return KATE_OK;
+    });
+}
+
+kate_status kate_circuit_export_qcx(const kate_circuit* c, const char* path) {
+    return guarded([&] {
+        REQUIRE(c && path, "null pointer");
+        return from_msg(kate::export_qcx(c->prog, path));
+    });
+}
+
+kate_status kate_sim_create(const kate_circuit* c, int precision, int device, kate_sim** out) {
+    return guarded([&] {
+        REQUIRE(c && out, "null pointer");
+        REQUIRE(precision == KATE_C128 || precision == KATE_C64, "unknown precision");
+        kate::Simulator* s = nullptr;
+        std::string e = kate::Simulator::create(c->prog, precision, device, &s);
+        if (!e.empty()) return sim_status(e);
+        auto* h = new kate_sim();
+        h->sim = s;
+        *out = h;
+        return KATE_OK;
+    });
+}
+
+kate_status kate_sim_destroy(kate_sim* s) {
+    if (s) {
+        delete s->sim;
+        delete s;
+    }
+    return KATE_OK;
+}
+
+kate_status kate_sim_execute(kate_sim* s, double* theta_phi) {
+    return guarded([&] {
+        REQUIRE(s, "null simulator");
+        std::string e = s->sim->run_async(nullptr, nullptr);
+        if (e.empty()) e = s->sim->synchronize();
+        if (e.empty() && theta_phi) e = s->sim->proba_state(theta_phi);
+        return sim_status(e);
+    });
+}
+
+kate_status kate_sim_execute_from(kate_sim* s, const double* in, double* out) {
+    return guarded([&] {
+        REQUIRE(s && in, "null pointer");
+        std::string e = s->sim->run_async(nullptr, in);
+        if (e.empty()) e = s->sim->synchronize();
+        if (e.empty() && out) e = s->sim->proba_state(out);
+        return sim_status(e);
+    });
+}
+
+kate_status kate_sim_run_async(kate_sim* s, void* stream) {
+    return guarded([&] {
+        REQUIRE(s, "null simulator");
+        return sim_status(s->sim->run_async(stream, nullptr));
+    });
+}
+
+kate_status kate_sim_synchronize(kate_sim* s) {
+    REQUIRE(s, "null simulator");
+    return sim_status(s->sim->synchronize());
+}
+
+kate_status kate_sim_proba_state(kate_sim* s, double* tp) {
+    return guarded([&] {
+        REQUIRE(s && tp, "null pointer");
+        return sim_status(s->sim->proba_state(tp));
+    });
+}
+
+kate_status kate_sim_get_state(kate_sim* s, double* out) {
+    return guarded([&] {
+        REQUIRE(s && out, "null pointer");
+        return sim_status(s->sim->get_state(out));
+    });
+}
+
+kate_status kate_sim_set_state(kate_sim* s, const double* in) {
+    return guarded([&] {
+        REQUIRE(s && in, "null pointer");
+        return sim_status(s->sim->set_state(in));
+    });
+}
+
+kate_status kate_sim_expect_z(kate_sim* s, double* out) {
+    return guarded([&] {
+        REQUIRE(s && out, "null pointer");
+        return sim_status(s->sim->expect_z(out));
+    });
+}
+
+kate_status kate_sim_probabilities(kate_sim* s, double* out) {
+    return guarded([&] {
+        REQUIRE(s && out, "null pointer");
+        return sim_status(s->sim->probabilities(out));
+    });
+}
+
+kate_status kate_sim_sample(kate_sim* s, int shots, uint64_t seed, uint64_t* out) {
+    return guarded([&] {
+        REQUIRE(s && (out || shots == 0), "null pointer");
+        return sim_status(s->sim->sample(shots, seed, out));
+    });
+}
+
+kate_status kate_sim_state_device(kate_sim* s, void** dptr, int* phys) {
+    REQUIRE(s && dptr && phys, "null pointer");
+    return sim_status(s->sim->state_device(dptr, phys));
+}
+
+kate_status kate_sim_profile_passes(kate_sim* s, float* ms, float* init_ms) {
+    return guarded([&] {
+        REQUIRE(s && ms, "null pointer");
+        return sim_status(s->sim->profile_passes(ms, init_ms));
+    });
+}
+
+kate_status kate_sim_launches_per_run(kate_sim* s, int* out) {
+    REQUIRE(s && out, "null pointer");
+    *out = s->sim->launches_per_run();
+    return KATE_OK;
+}
+
+kate_status kate_sim_nqbits(kate_sim* s, int* out) {
+    REQUIRE(s && out, "null pointer");
+    *out = s->sim->nqbits();
+    return KATE_OK;
+}
+
+kate_status kate_sim_num_passes(kate_sim* s, int* out) {
+    REQUIRE(s && out, "null pointer");
+    *out = (int)s->sim->plan().passes.size();
+    return KATE_OK;
+}
+
+kate_status kate_sim_get_pass(kate_sim* s, int i, int* tile_qbits, int* m, int* ngates) {
+    REQUIRE(s && tile_qbits && m && ngates, "null pointer");
+    const auto& P = s->sim->plan();
+    REQUIRE(i >= 0 && i < (int)P.passes.size(), "pass index out of range");
+    const auto& p = P.passes[i];
+    *m = (int)p.tile.size();
+    for (size_t k = 0; k < p.tile.size(); k++) tile_qbits[k] = p.tile[k];
+    *ngates = (int)p.gates.size();
+    return KATE_OK;
+}
+
+kate_status kate_plan_create(const kate_circuit* c, int max_tile, int coalesce, unsigned flags, kate_plan** out) {
+    return guarded([&] {
+        REQUIRE(c && out, "null pointer");
+        REQUIRE(max_tile >= 1 && max_tile <= KATE_MAX_TILE, "max_tile must be in [1, 14]");
+        REQUIRE(coalesce >= 0 && coalesce <= max_tile, "coalesce must be in [0, max_tile]");
+        kate::Program prog = c->prog;
+        if (prog.instructions.empty()) {
+            std::string e = kate::pass_compile_default(prog, 0, prog.nqbits);
+            if (!e.empty()) return fail(KATE_EINVAL, e);
+        }
+        kate::PlanOptions opt;
+        opt.max_tile = max_tile;
+        opt.coalesce = coalesce;
+        opt.remap = !(flags & KATE_PLAN_NO_REMAP);
+        opt.fuse_1q = !(flags & KATE_PLAN_NO_FUSE1Q);
+        auto* p = new kate_plan();
+        std::string e = kate::build_plan(prog, opt, &p->plan);
+        if (!e.empty()) {
+            delete p;
+            return fail(KATE_EINVAL, e);
+        }
+        for (auto& pp : p->plan.passes) {
+            p->passes.push_back(kate::to_devpass(prog.nqbits, pp, (int)p->ops.size()));
+            p->ops.insert(p->ops.end(), pp.ops.begin(), pp.ops.end());
+        }
+        *out = p;
+        return KATE_OK;
+    });
+}
+
+kate_status kate_plan_destroy(kate_plan* p) {
+    delete p;
+    return KATE_OK;
+}
+
+kate_status kate_plan_num_passes(const kate_plan* p, int* out) {
+    REQUIRE(p && out, "null pointer");
+    *out = (int)p->passes.size();
+    return KATE_OK;
+}
+
+kate_status kate_plan_get_pass(const kate_plan* p, int i, int* info, uint8_t* tphys, uint8_t* outsrc) {
+    REQUIRE(p && info && tphys && outsrc, "null pointer");
+    REQUIRE(i >= 0 && i < (int)p->passes.size(), "pass index out of range");
+    const DevPass& d = p->passes[i];
+    info[0] = d.m;
+    info[1] = d.nops;
+    info[2] = d.op0;
+    info[3] = d.ncb;
+    for (int t = 0; t < 16; t++) {
+        tphys[t] = d.tphys[t];
+        outsrc[t] = d.outsrc[t];
+    }
+    return KATE_OK;
+}
+
+kate_status kate_plan_num_ops(const kate_plan* p, int* out) {
+    REQUIRE(p && out, "null pointer");
+    *out = (int)p->ops.size();
+    return KATE_OK;
+}
+
+kate_status kate_plan_get_op(const kate_plan* p, int i, int* ints, uint64_t* pmask, double* vals) {
+    REQUIRE(p && ints && pmask && vals, "null pointer");
+    REQUIRE(i >= 0 && i < (int)p->ops.size(), "op index out of range");
+    const DevOp& o = p->ops[i];
+    ints[0] = o.kind;
+    ints[1] = o.k;
+    for (int j = 0; j < 5; j++) {
+        ints[2 + j] = o.tb[j];
+        ints[7 + j] = o.ftb[j];
+        ints[12 + j] = o.fpos[j];
+    }
+    ints[17] = (int)o.tmask;
+    *pmask = o.pmask;
+    vals[0] = o.ph_re;
+    vals[1] = o.ph_im;
+    size_t len = 0;
+    if (o.kind == OPK_DENSE) len = (size_t)1 << (2 * o.k);
+    else if (o.kind == OPK_DIAG) len = (size_t)1 << o.k;
+    for (size_t j = 0; j < len; j++) {
+        vals[2 + 2 * j] = p->plan.pool[o.mat + j].re;
+        vals[3 + 2 * j] = p->plan.pool[o.mat + j].im;
+    }
+    return KATE_OK;
+}
+
+kate_status kate_plan_final_layout(const kate_plan* p, int* phys, int* l2l) {
+    REQUIRE(p && phys && l2l, "null pointer");
+    for (int q = 0; q < p->plan.n; q++) {
+        phys[q] = p->plan.final_phys[q];
+        l2l[q] = p->plan.label_to_logical[q];
+    }
+    return KATE_OK;
+}
+
+}  // extern "C"

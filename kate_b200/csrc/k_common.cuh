@@ -1,0 +1,35 @@
+// Small device helpers shared by the kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace kate {
+
+#define KATE_SQRT2 1.4142135623730951
+#define KATE_SQRT2INV 0.7071067811865475
+
+// Inserts a zero bit at position b of v.
+__device__ __forceinline__ uint32_t ins0(uint32_t v, int b) {
+    return ((v >> b) << (b + 1)) | (v & ((1u << b) - 1u));
+}
+
+// (a.x*b.x - a.y*b.y, a.x*b.y + a.y*b.x): the reference's Complex product.
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// acc += a * b (complex), as four FMAs.
+__device__ __forceinline__ void cfma(double2& acc, double2 a, double2 b) {
+    acc.x = fma(a.x, b.x, acc.x);
+    acc.x = fma(-a.y, b.y, acc.x);
+    acc.y = fma(a.x, b.y, acc.y);
+    acc.y = fma(a.y, b.x, acc.y);
+}
+
+__device__ __forceinline__ double2 dadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+
+}  // namespace kate

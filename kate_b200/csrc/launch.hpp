@@ -1,0 +1,39 @@
+// Host-side launchers of the CUDA kernels (defined in the .cu files).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "device_types.h"
+
+namespace kate {
+
+// Product-state initialisation value table: v[b][p] is the factor for
+// physical bit p having value b.
+struct ProductInit {
+    double v[2][KATE_MAX_QUBITS][2];
+    int n;
+};
+
+// c128 state (double2 amplitudes)
+cudaError_t launch_set_basis0_c128(void* st, uint64_t dim, cudaStream_t s);
+cudaError_t launch_init_product_c128(void* st, int n, const ProductInit& P, cudaStream_t s);
+// One generic group pass (shared-memory tile, any op mix). Dense ops up to 5 qubits.
+cudaError_t launch_pass_generic_c128(void* st, int n, const DevPass& p, const DevOp* ops, const void* pool,
+                                     int grid, cudaStream_t s);
+int generic_pass_grid(int n, int m, int device);
+
+// Bit sums: per CTA, for every local bit, the sum over amplitudes with the
+// bit 0 and with the bit 1, plus the total. kind 0 sums amplitudes (double2
+// partials), kind 1 sums |a|^2 (double partials). Returns the grid shape.
+struct BitSumShape {
+    int grid;   // CTAs (2^g)
+    int g;      // coset bits handled by the grid
+    int nr;     // round bits handled per thread
+    int nout;   // partial values per CTA
+};
+BitSumShape bitsum_shape(int n);
+cudaError_t launch_bitsums_c128(const void* st, int n, int kind, void* partials, cudaStream_t s);
+cudaError_t launch_probs_c128(const void* st, uint64_t dim, double* out, cudaStream_t s);
+
+}  // namespace kate

@@ -1,0 +1,447 @@
+// Group-pass planner. See plan.hpp.
+#include "plan.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <set>
+
+namespace kate {
+
+namespace {
+
+constexpr double kPi = 3.1415926535897932384626433;
+
+bool is_diagonal(const std::vector<Cx>& m, int dim) {
+    for (int r = 0; r < dim; r++)
+        for (int c = 0; c < dim; c++)
+            if (r != c && (m[(size_t)r * dim + c].re != 0.0 || m[(size_t)r * dim + c].im != 0.0)) return false;
+    return true;
+}
+
+std::string classify(const Gate& g, const std::vector<int>& lab2log, int src, std::vector<PGate>& out) {
+    std::vector<int> q;
+    for (int x : g.qbits) q.push_back(lab2log[x]);
+    PGate p;
+    p.src = src;
+    switch (g.id) {
+    case G_H:
+        p.kind = OPK_H;
+        p.tq = {q[0]};
+        break;
+    case G_CNOT:
+        p.kind = OPK_X;
+        p.tq = {q[0]};
+        p.fq = {q[1]};
+        break;
+    case G_TOFFOLI:
+        p.kind = OPK_X;
+        p.tq = {q[2]};
+        p.fq = {q[0], q[1]};
+        break;
+    case G_CRK: {
+        p.kind = OPK_PHASE;
+        p.fq = {q[0], q[1]};
+        double t = ((double)2 * kPi) / (double)(1ull << g.optarg);
+        p.ph_re = std::cos(t);
+        p.ph_im = std::sin(t);
+        break;
+    }
+    case G_DENSE: {
+        int k = (int)q.size();
+        if (k > 5) return "dense gates above 5 qubits are not supported by the device path (fuse with k <= 5)";
+        int dim = 1 << k;
+        if (is_diagonal(g.dense, dim)) {
+            p.kind = OPK_DIAG;
+            p.fq = q;
+            for (int i = 0; i < dim; i++) p.table.push_back(g.dense[(size_t)i * dim + i]);
+        } else {
+            p.kind = OPK_DENSE;
+            p.tq = q;
+            p.table = g.dense;
+        }
+        break;
+    }
+    default:
+        return "";  // RX / RZ: no arithmetic, as in the reference
+    }
+    out.push_back(std::move(p));
+    return "";
+}
+
+// One-qubit chain fusion (the planner's own GateMerger step): an op acting
+// on a single qubit q (dense 2x2, diagonal, H) whose previous op touching q
+// is also a single-qubit op on q is multiplied into it in FP64. A layer of
+// RX then RZ on every qubit becomes one 2x2 per qubit (8 FMAs per amplitude
+// instead of two passes over the tile).
+bool single_qubit(const PGate& g, int* q) {
+    if ((g.kind == OPK_DENSE || g.kind == OPK_H) && g.tq.size() == 1 && g.fq.empty()) {
+        *q = g.tq[0];
+        return true;
+    }
+    if (g.kind == OPK_DIAG && g.fq.size() == 1 && g.tq.empty()) {
+        *q = g.fq[0];
+        return true;
+    }
+    return false;
+}
+
+void matrix_2x2(const PGate& g, Cx m[4]) {
+    if (g.kind == OPK_H) {
+        const double s = 0.7071067811865475;
+        m[0] = {s, 0};
+        m[1] = {s, 0};
+        m[2] = {s, 0};
+        m[3] = {-s, 0};
+    } else if (g.kind == OPK_DIAG) {
+        m[0] = g.table[0];
+        m[1] = {0, 0};
+        m[2] = {0, 0};
+        m[3] = g.table[1];
+    } else {
+        for (int i = 0; i < 4; i++) m[i] = g.table[i];
+    }
+}
+
+PGate make_1q(int q, const Cx m[4], int src) {
+    PGate p;
+    p.src = src;
+    if (m[1].re == 0.0 && m[1].im == 0.0 && m[2].re == 0.0 && m[2].im == 0.0) {
+        p.kind = OPK_DIAG;
+        p.fq = {q};
+        p.table = {m[0], m[3]};
+    } else {
+        p.kind = OPK_DENSE;
+        p.tq = {q};
+        p.table.assign(m, m + 4);
+    }
+    return p;
+}
+
+std::vector<PGate> fuse_single_qubit(std::vector<PGate>&& in, int n) {
+    std::vector<PGate> out;
+    out.reserve(in.size());
+    std::vector<int> last(n, -1);
+    for (auto& g : in) {
+        int q;
+        if (single_qubit(g, &q) && last[q] >= 0) {
+            int q2;
+            PGate& prev = out[last[q]];
+            if (single_qubit(prev, &q2) && q2 == q) {
+                Cx a[4], b[4], r[4];
+                matrix_2x2(g, a);
+                matrix_2x2(prev, b);
+                for (int i = 0; i < 2; i++)
+                    for (int j = 0; j < 2; j++) r[2 * i + j] = a[2 * i] * b[j] + a[2 * i + 1] * b[2 + j];
+                prev = make_1q(q, r, prev.src);
+                continue;
+            }
+        }
+        out.push_back(std::move(g));
+        for (int x : out.back().tq) last[x] = (int)out.size() - 1;
+        for (int x : out.back().fq) last[x] = (int)out.size() - 1;
+    }
+    return out;
+}
+
+struct Layout {
+    std::vector<int> phys;  // logical -> physical
+    std::vector<int> inv;   // physical -> logical
+    explicit Layout(int n) : phys(n), inv(n) {
+        std::iota(phys.begin(), phys.end(), 0);
+        std::iota(inv.begin(), inv.end(), 0);
+    }
+};
+
+// Greedy tile selection over `rem`: returns executed gate indices; `T` is
+// extended in place. If `order` is non-null it records the order in which
+// qubits joined T.
+std::vector<int> greedy_pass(const std::vector<PGate>& pg, const std::vector<int>& rem, int n, int m,
+                             std::vector<char>& inT, int& tsize, std::vector<int>* order, size_t scan_limit) {
+    std::vector<char> blocked(n, 0);
+    std::vector<int> exec;
+    size_t scanned = 0;
+    int nblocked = 0;
+    for (int gi : rem) {
+        if (++scanned > scan_limit || nblocked == n) break;
+        const PGate& g = pg[gi];
+        bool blk = false;
+        for (int q : g.tq) blk |= blocked[q] != 0;
+        for (int q : g.fq) blk |= blocked[q] != 0;
+        if (!blk) {
+            int need = 0;
+            for (int q : g.tq) need += !inT[q];
+            if (tsize + need <= m) {
+                for (int q : g.tq)
+                    if (!inT[q]) {
+                        inT[q] = 1;
+                        tsize++;
+                        if (order) order->push_back(q);
+                    }
+                exec.push_back(gi);
+                continue;
+            }
+        }
+        for (int q : g.tq) nblocked += !blocked[q], blocked[q] = 1;
+        for (int q : g.fq) nblocked += !blocked[q], blocked[q] = 1;
+    }
+    return exec;
+}
+
+}  // namespace
+
+DevPass to_devpass(int n, const PlannedPass& p, int op0) {
+    DevPass d{};
+    int m = (int)p.phys_in.size();
+    d.m = m;
+    d.nops = (int)p.ops.size();
+    d.op0 = op0;
+    d.ncb = n - m;
+    std::vector<char> inS(n, 0);
+    for (int t = 0; t < m; t++) {
+        d.tphys[t] = (uint8_t)p.phys_in[t];
+        inS[p.phys_in[t]] = 1;
+    }
+    for (int t = 0; t < m; t++) d.outsrc[p.out_tile[t]] = (uint8_t)t;
+    int j = 0;
+    for (int b = 0; b < n; b++)
+        if (!inS[b]) d.cphys[j++] = (uint8_t)b;
+    return d;
+}
+
+void lower_pass(const Plan& plan, PlannedPass& pass, const std::vector<int>& phys, std::vector<Cx>& pool) {
+    const int m = (int)pass.phys_in.size();
+    auto tile_bit = [&](int q) -> int {
+        int p = phys[q];
+        for (int t = 0; t < m; t++)
+            if (pass.phys_in[t] == p) return t;
+        return -1;
+    };
+    pass.ops.clear();
+    for (int gi : pass.gates) {
+        const PGate& g = plan.pgates[gi];
+        DevOp op{};
+        op.kind = g.kind;
+        op.k = (int)std::max(g.tq.size(), g.fq.size());
+        for (int i = 0; i < 5; i++) op.tb[i] = op.ftb[i] = op.fpos[i] = -1;
+        for (size_t i = 0; i < g.tq.size(); i++) op.tb[i] = tile_bit(g.tq[i]);
+        op.ph_re = g.ph_re;
+        op.ph_im = g.ph_im;
+        op.mat = -1;
+        if (g.kind == OPK_DENSE) op.k = (int)g.tq.size();
+        if (g.kind == OPK_X || g.kind == OPK_PHASE) {
+            for (int q : g.fq) {
+                int t = tile_bit(q);
+                if (t >= 0) op.tmask |= 1u << t;
+                else op.pmask |= 1ull << phys[q];
+            }
+        }
+        if (g.kind == OPK_DIAG) {
+            op.k = (int)g.fq.size();
+            for (size_t i = 0; i < g.fq.size(); i++) {
+                int t = tile_bit(g.fq[i]);
+                op.ftb[i] = t;
+                op.fpos[i] = t >= 0 ? -1 : phys[g.fq[i]];
+            }
+        }
+        if (!g.table.empty()) {
+            op.mat = (int64_t)pool.size();
+            pool.insert(pool.end(), g.table.begin(), g.table.end());
+        }
+        pass.ops.push_back(op);
+    }
+}
+
+std::vector<PlannedPass> plan_relayout(int n, const std::vector<int>& phys0, const std::vector<int>& target,
+                                       const PlanOptions& opt) {
+    std::vector<PlannedPass> out;
+    const int m = std::min(opt.max_tile, n);
+    const int c = std::min(opt.coalesce, m);
+    std::vector<int> phys(phys0), inv(n);
+    for (int q = 0; q < n; q++) inv[phys[q]] = q;
+    for (int guard = 0; guard < 4 * n + 8 && phys != target; guard++) {
+        std::vector<char> inS(n, 0);
+        std::vector<int> S;
+        auto add = [&](int p) {
+            if (!inS[p] && (int)S.size() < m) {
+                inS[p] = 1;
+                S.push_back(p);
+            }
+        };
+        for (int p = 0; p < c; p++) add(p);
+        // Follow displacement cycles from each wrong position while room remains.
+        for (int p = 0; p < n && (int)S.size() < m; p++) {
+            if (target[inv[p]] == p) continue;
+            int cur = p;
+            while ((int)S.size() < m) {
+                add(cur);
+                int nxt = target[inv[cur]];
+                if (inS[nxt]) break;
+                cur = nxt;
+            }
+        }
+        for (int p = 0; p < n && (int)S.size() < m; p++) add(p);
+        std::sort(S.begin(), S.end());
+        // Inside S: every qubit whose target lies in S goes there; the rest
+        // fill the remaining positions in order.
+        std::vector<int> newpos(n, -1);
+        std::vector<char> taken(n, 0);
+        for (int p : S) {
+            int q = inv[p];
+            if (inS[target[q]]) {
+                newpos[q] = target[q];
+                taken[target[q]] = 1;
+            }
+        }
+        size_t fill = 0;
+        for (int p : S) {
+            int q = inv[p];
+            if (newpos[q] >= 0) continue;
+            while (taken[S[fill]]) fill++;
+            newpos[q] = S[fill];
+            taken[S[fill]] = 1;
+        }
+        PlannedPass pp;
+        pp.phys_in = S;
+        pp.out_tile.assign(m, 0);
+        for (int t = 0; t < m; t++) {
+            int q = inv[S[t]];
+            pp.tile.push_back(q);
+            int np = newpos[q];
+            pp.out_tile[t] = (int)(std::lower_bound(S.begin(), S.end(), np) - S.begin());
+        }
+        for (int p : S) {
+            int q = inv[p];
+            phys[q] = newpos[q];
+        }
+        for (int q = 0; q < n; q++) inv[phys[q]] = q;
+        out.push_back(std::move(pp));
+    }
+    return out;
+}
+
+std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out) {
+    Plan& plan = *out;
+    const int n = prog.nqbits;
+    plan = Plan();
+    plan.n = n;
+    plan.initial_permutation = prog.initial_permutation;
+    plan.final_inverse_permutation = prog.final_inverse_permutation;
+    std::vector<int> lab2log(n);
+    std::iota(lab2log.begin(), lab2log.end(), 0);
+    // Walk the instruction stream: swaps relabel, computes emit gates.
+    size_t gi = 0;
+    int k = 0;
+    for (auto& ins : prog.instructions) {
+        if (ins.first == 0) {
+            for (size_t i = 0; i + 1 < ins.second.size(); i += 2) {
+                int a = ins.second[i], b = ins.second[i + 1];
+                if (a < 0 || b < 0 || a >= n || b >= n) return "swap instruction outside the circuit";
+                std::swap(lab2log[a], lab2log[b]);
+            }
+        } else {
+            if (gi >= prog.groups.size()) return "instruction stream has more compute steps than groups";
+            int end = prog.groups[gi].first;
+            for (; k < end; k++) {
+                std::string e = classify(prog.gates[k], lab2log, k, plan.pgates);
+                if (!e.empty()) return e;
+            }
+            gi++;
+        }
+    }
+    plan.label_to_logical = lab2log;
+    if (opt.fuse_1q) plan.pgates = fuse_single_qubit(std::move(plan.pgates), n);
+
+    const int m = std::min(opt.max_tile, n);
+    int maxT = 0;
+    for (auto& g : plan.pgates) maxT = std::max(maxT, (int)g.tq.size());
+    if (maxT > m) return "a gate has more target qubits than the tile";
+    // The c low physical bits are always tile bits; leave room for the
+    // widest gate's targets beside them so every pass can make progress.
+    const int c = std::max(0, std::min(opt.coalesce, m - maxT));
+    Layout L(n);
+    std::vector<int> rem(plan.pgates.size());
+    std::iota(rem.begin(), rem.end(), 0);
+    const size_t scan_limit = 1u << 20;
+    while (!rem.empty()) {
+        std::vector<char> inT(n, 0);
+        int tsize = 0;
+        for (int p = 0; p < c; p++) {
+            inT[L.inv[p]] = 1;
+            tsize++;
+        }
+        std::vector<int> exec = greedy_pass(plan.pgates, rem, n, m, inT, tsize, nullptr, scan_limit);
+        if (exec.empty()) return "planner made no progress";
+        for (int p = 0; p < n && tsize < m; p++)
+            if (!inT[L.inv[p]]) {
+                inT[L.inv[p]] = 1;
+                tsize++;
+            }
+        {
+            std::vector<int> nr;
+            nr.reserve(rem.size());
+            size_t e = 0;
+            for (int g : rem) {
+                if (e < exec.size() && exec[e] == g) e++;
+                else nr.push_back(g);
+            }
+            rem.swap(nr);
+        }
+        // Tile bits in ascending physical order.
+        std::vector<int> S;
+        for (int q = 0; q < n; q++)
+            if (inT[q]) S.push_back(L.phys[q]);
+        std::sort(S.begin(), S.end());
+        // Choose the qubits that the next pass wants at the low positions.
+        std::vector<int> newlow;
+        if (opt.remap && !rem.empty()) {
+            std::vector<char> inT2(n, 0);
+            int ts2 = 0;
+            std::vector<int> order;
+            greedy_pass(plan.pgates, rem, n, m, inT2, ts2, &order, scan_limit);
+            for (int q : order)
+                if (inT[q] && (int)newlow.size() < c) newlow.push_back(q);
+        }
+        for (int p = 0; p < c && (int)newlow.size() < c; p++) {
+            int q = L.inv[p];
+            if (std::find(newlow.begin(), newlow.end(), q) == newlow.end()) newlow.push_back(q);
+        }
+        // New layout: newlow qubits already in the low bits stay; arrivals
+        // take the freed low positions; displaced low qubits take the
+        // arrivals' old positions.
+        std::vector<int> nphys(L.phys);
+        std::vector<char> isnew(n, 0);
+        for (int q : newlow) isnew[q] = 1;
+        std::vector<int> freed, leaving;
+        for (int p = 0; p < c; p++)
+            if (!isnew[L.inv[p]]) {
+                freed.push_back(p);
+                leaving.push_back(L.inv[p]);
+            }
+        size_t fi = 0;
+        for (int q : newlow)
+            if (L.phys[q] >= c) {
+                int oldp = L.phys[q];
+                nphys[q] = freed[fi];
+                nphys[leaving[fi]] = oldp;
+                fi++;
+            }
+        PlannedPass pp;
+        pp.phys_in = S;
+        pp.gates = exec;
+        pp.out_tile.assign(m, 0);
+        for (int t = 0; t < m; t++) {
+            int q = L.inv[S[t]];
+            pp.tile.push_back(q);
+            pp.out_tile[t] = (int)(std::lower_bound(S.begin(), S.end(), nphys[q]) - S.begin());
+        }
+        lower_pass(plan, pp, L.phys, plan.pool);
+        plan.passes.push_back(std::move(pp));
+        L.phys = nphys;
+        for (int q = 0; q < n; q++) L.inv[L.phys[q]] = q;
+    }
+    plan.final_phys = L.phys;
+    return "";
+}
+
+}  // namespace kate

@@ -1,0 +1,84 @@
+// Group-pass planner: turns a compiled program into B200 group passes.
+//
+// A group pass reads every amplitude once and writes it once. It owns a
+// "tile" of m qubits: each CTA takes one coset of the tile (the 2^m
+// amplitudes that share all non-tile bits), stages it on chip, applies every
+// planned gate to it and writes it back. Gates are classified as
+//   - target qubits: must be tile qubits (dense, H, the X of CNOT/TOFFOLI);
+//   - free qubits: controls and diagonal qubits; they may lie outside the
+//     tile, where they are constant over a coset and are evaluated once per
+//     CTA from the coset's base address.
+// The planner packs gates greedily in program order (a gate is taken when
+// none of its qubits is blocked by an earlier skipped gate and its targets
+// fit the tile), which is the single-GPU replacement for the reference's
+// gateGrouping + per-group launches (backendagnosticcode/Circuit.hpp:176-206,
+// HIPcode/simulator.hpp:760-810).
+//
+// Qubit remap (the replacement for the reference's swap instructions,
+// HIPcode/simulator.hpp:639-759): the c lowest physical bits must be tile
+// bits so that every load/store touches 2^c contiguous amplitudes. Each pass
+// may write its tile back with its tile bits permuted, which moves c qubits
+// that the next pass needs into those low positions at no extra HBM cost.
+// Swap instructions of the compiled program become pure relabelings.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "circuit.hpp"
+#include "device_types.h"
+
+namespace kate {
+
+struct PlanOptions {
+    int max_tile = 12;   // m: tile qubits per pass
+    int coalesce = 4;    // c: low physical bits every tile must contain
+    bool remap = true;   // move next-needed qubits into the low bits on write
+    bool fuse_1q = true; // multiply chains of single-qubit ops on one qubit (FP64, host)
+};
+
+struct PlannedPass {
+    std::vector<int> tile;       // tile qubits (logical ids), ascending physical position
+    std::vector<int> phys_in;    // physical position of tile bit t (ascending)
+    std::vector<int> out_tile;   // input tile bit t is written to tile bit out_tile[t]
+    std::vector<int> gates;      // indices into Plan::pgates executed by this pass
+    std::vector<DevOp> ops;      // device ops, tile-relative
+};
+
+// A gate as the planner sees it (logical qubits).
+struct PGate {
+    int kind = 0;             // OPK_* from device_types.h
+    std::vector<int> tq;      // target qubits, in gate-bit order
+    std::vector<int> fq;      // free qubits (controls, or diagonal qubits in bit order)
+    std::vector<Cx> table;    // dense matrix (row-major) or diagonal table
+    double ph_re = 1.0, ph_im = 0.0;
+    int src = -1;             // index in the program's gate list
+};
+
+struct Plan {
+    int n = 0;
+    std::vector<PGate> pgates;
+    std::vector<PlannedPass> passes;
+    std::vector<int> final_phys;     // logical qubit -> physical bit after the last pass
+    std::vector<int> label_to_logical;  // program label x holds logical qubit label_to_logical[x] at the end
+    std::vector<int> initial_permutation, final_inverse_permutation;
+    std::vector<Cx> pool;            // dense matrices and diagonal tables of all ops
+};
+
+// Classifies gates, plans passes and lowers them to device ops. Dense gates
+// above 5 qubits are rejected (message returned).
+std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out);
+
+// Remap-only passes taking layout `phys` (logical -> physical) to `target`.
+std::vector<PlannedPass> plan_relayout(int n, const std::vector<int>& phys, const std::vector<int>& target,
+                                       const PlanOptions& opt);
+
+// Device descriptor of a pass whose ops start at op0.
+DevPass to_devpass(int n, const PlannedPass& p, int op0);
+
+// Lowers one pass's gates into device ops (tile-relative); matrices and
+// tables are appended to `pool` (complex doubles).
+void lower_pass(const Plan& plan, PlannedPass& pass, const std::vector<int>& phys, std::vector<Cx>& pool);
+
+}  // namespace kate

@@ -1,0 +1,365 @@
+// Device simulator. See sim.hpp.
+#include "sim.hpp"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <random>
+
+#include "launch.hpp"
+
+namespace kate {
+
+namespace {
+constexpr double kPi = 3.1415926535897932384626433;
+constexpr double kSqrt2 = 1.4142135623730951;
+
+std::string cuda_err(const char* what, cudaError_t e) {
+    return std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+}
+#define KCHECK(call)                                              \
+    do {                                                          \
+        cudaError_t e_ = (call);                                  \
+        if (e_ != cudaSuccess) return cuda_err(#call, e_);        \
+    } while (0)
+}  // namespace
+
+struct SimImpl {
+    int device = 0;
+    int n = 0;
+    int precision = 0;
+    Program prog;
+    Plan plan;
+    PlanOptions opt;
+    void* d_state = nullptr;
+    DevOp* d_ops = nullptr;
+    void* d_pool = nullptr;
+    void* d_part = nullptr;
+    size_t part_bytes = 0;
+    std::vector<DevPass> hpasses;
+    cudaStream_t stream = nullptr;
+    std::vector<int> phys;  // current layout: logical -> physical
+    bool has_state = false;
+    int grid = 0;
+
+    uint64_t dim() const { return 1ull << n; }
+    size_t amp_bytes() const { return precision == 0 ? 16 : 8; }
+
+    // Target layout for readback: label x at physical bit x.
+    std::vector<int> label_layout() const {
+        std::vector<int> t(n);
+        for (int x = 0; x < n; x++) t[plan.label_to_logical[x]] = x;
+        return t;
+    }
+    // Physical bit of program label x.
+    int phys_of_label(int x) const { return phys[plan.label_to_logical[x]]; }
+
+    std::string run_relayout(const std::vector<int>& target) {
+        if (phys == target) return "";
+        std::vector<PlannedPass> pp = plan_relayout(n, phys, target, opt);
+        for (auto& p : pp) {
+            DevPass d = to_devpass(n, p, 0);
+            int grid_r = generic_pass_grid(n, d.m, device);
+            KCHECK(launch_pass_generic_c128(d_state, n, d, d_ops, d_pool, grid_r, stream));
+        }
+        phys = target;
+        return "";
+    }
+
+    // Sums over amplitudes (kind 0) or probabilities (kind 1) for every
+    // physical bit; s0/s1 are 2 doubles per bit for kind 0, 1 for kind 1.
+    std::string bit_sums(int kind, std::vector<double>& s0, std::vector<double>& s1, double* total) {
+        BitSumShape sh = bitsum_shape(n);
+        const int w = kind == 0 ? 2 : 1;
+        std::vector<double> h((size_t)sh.grid * sh.nout * w);
+        KCHECK(launch_bitsums_c128(d_state, n, kind, d_part, stream));
+        KCHECK(cudaMemcpyAsync(h.data(), d_part, h.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        KCHECK(cudaStreamSynchronize(stream));
+        s0.assign((size_t)n * w, 0.0);
+        s1.assign((size_t)n * w, 0.0);
+        std::vector<double> tot(w, 0.0);
+        for (int c = 0; c < sh.grid; c++) {
+            const double* pc = h.data() + (size_t)c * sh.nout * w;
+            for (int k = 0; k < w; k++) tot[k] += pc[k];
+            for (int b = 0; b < n; b++) {
+                int slot;
+                if (b < 12) slot = b;
+                else if (b < 12 + sh.g) {
+                    bool one = (c >> (b - 12)) & 1;
+                    for (int k = 0; k < w; k++) (one ? s1 : s0)[(size_t)b * w + k] += pc[k];
+                    continue;
+                } else slot = 12 + (b - 12 - sh.g);
+                for (int k = 0; k < w; k++) {
+                    s0[(size_t)b * w + k] += pc[(size_t)(1 + 2 * slot) * w + k];
+                    s1[(size_t)b * w + k] += pc[(size_t)(2 + 2 * slot) * w + k];
+                }
+            }
+        }
+        if (total) for (int k = 0; k < w; k++) total[k] = tot[k];
+        return "";
+    }
+};
+
+std::string Simulator::create(const Program& prog_in, int precision, int device, Simulator** out) {
+    if (precision != 0) return "only KATE_C128 is available in this build of the simulator";
+    if (prog_in.nqbits < 1 || prog_in.nqbits > 34) return "the device simulator supports 1 to 34 qubits";
+    auto* impl = new SimImpl();
+    auto fail = [&](const std::string& e) {
+        auto* s = new Simulator();
+        s->d_ = impl;
+        delete s;
+        return e;
+    };
+    impl->device = device;
+    impl->n = prog_in.nqbits;
+    impl->precision = precision;
+    impl->prog = prog_in;
+    if (impl->prog.instructions.empty()) {
+        std::string e = pass_compile_default(impl->prog, 0, impl->prog.nqbits);
+        if (!e.empty()) return fail(e);
+    }
+    std::string e = build_plan(impl->prog, impl->opt, &impl->plan);
+    if (!e.empty()) return fail(e);
+
+    cudaError_t ce = cudaSetDevice(device);
+    if (ce != cudaSuccess) return fail(cuda_err("cudaSetDevice", ce));
+    ce = cudaStreamCreateWithFlags(&impl->stream, cudaStreamNonBlocking);
+    if (ce != cudaSuccess) return fail(cuda_err("cudaStreamCreate", ce));
+    // Upload ops and the matrix pool.
+    std::vector<DevOp> ops;
+    for (auto& p : impl->plan.passes) {
+        impl->hpasses.push_back(to_devpass(impl->n, p, (int)ops.size()));
+        ops.insert(ops.end(), p.ops.begin(), p.ops.end());
+    }
+    size_t ops_bytes = std::max<size_t>(1, ops.size()) * sizeof(DevOp);
+    size_t pool_bytes = std::max<size_t>(1, impl->plan.pool.size()) * sizeof(Cx);
+    ce = cudaMalloc(&impl->d_ops, ops_bytes);
+    if (ce != cudaSuccess) return fail(cuda_err("cudaMalloc(ops)", ce));
+    ce = cudaMalloc(&impl->d_pool, pool_bytes);
+    if (ce != cudaSuccess) return fail(cuda_err("cudaMalloc(pool)", ce));
+    if (!ops.empty()) cudaMemcpy(impl->d_ops, ops.data(), ops.size() * sizeof(DevOp), cudaMemcpyHostToDevice);
+    if (!impl->plan.pool.empty())
+        cudaMemcpy(impl->d_pool, impl->plan.pool.data(), impl->plan.pool.size() * sizeof(Cx), cudaMemcpyHostToDevice);
+    BitSumShape sh = bitsum_shape(impl->n);
+    impl->part_bytes = (size_t)sh.grid * sh.nout * 2 * sizeof(double);
+    ce = cudaMalloc(&impl->d_part, impl->part_bytes);
+    if (ce != cudaSuccess) return fail(cuda_err("cudaMalloc(partials)", ce));
+    ce = cudaMalloc(&impl->d_state, impl->dim() * impl->amp_bytes());
+    if (ce != cudaSuccess) return fail(cuda_err("cudaMalloc(state)", ce));
+    impl->grid = generic_pass_grid(impl->n, std::min(impl->opt.max_tile, impl->n), device);
+    impl->phys.resize(impl->n);
+    std::iota(impl->phys.begin(), impl->phys.end(), 0);
+    auto* s = new Simulator();
+    s->d_ = impl;
+    *out = s;
+    return "";
+}
+
+Simulator::~Simulator() {
+    if (!d_) return;
+    cudaSetDevice(d_->device);
+    if (d_->stream) cudaStreamSynchronize(d_->stream);
+    cudaFree(d_->d_state);
+    cudaFree(d_->d_ops);
+    cudaFree(d_->d_pool);
+    cudaFree(d_->d_part);
+    if (d_->stream) cudaStreamDestroy(d_->stream);
+    delete d_;
+}
+
+int Simulator::nqbits() const { return d_->n; }
+int Simulator::precision() const { return d_->precision; }
+const Plan& Simulator::plan() const { return d_->plan; }
+
+std::string Simulator::run_async(void* stream_in, const double* tp) {
+    SimImpl& S = *d_;
+    KCHECK(cudaSetDevice(S.device));
+    cudaStream_t st = stream_in ? (cudaStream_t)stream_in : S.stream;
+    if (tp) {
+        // execute(proba_state&): product state, qubit i placed at label
+        // initial_permutation[i] (CPUcode/simulator.hpp:139-162).
+        ProductInit P{};
+        P.n = S.n;
+        for (int i = 0; i < S.n; i++) {
+            double c0 = std::cos(tp[2 * i] * kPi / 2), s0 = std::sin(tp[2 * i] * kPi / 2);
+            double er = std::cos(tp[2 * i + 1]), ei = std::sin(tp[2 * i + 1]);
+            int lab = S.plan.initial_permutation.empty() ? i : S.plan.initial_permutation[i];
+            P.v[0][lab][0] = c0;
+            P.v[0][lab][1] = 0.0;
+            P.v[1][lab][0] = er * s0;
+            P.v[1][lab][1] = ei * s0;
+        }
+        KCHECK(launch_init_product_c128(S.d_state, S.n, P, st));
+    } else {
+        KCHECK(launch_set_basis0_c128(S.d_state, S.dim(), st));
+    }
+    for (auto& p : S.hpasses) KCHECK(launch_pass_generic_c128(S.d_state, S.n, p, S.d_ops, S.d_pool, S.grid, st));
+    S.phys = S.plan.final_phys;
+    S.has_state = true;
+    if (st != S.stream) {
+        // Order later library work on the simulator's stream after the caller's.
+        cudaEvent_t ev;
+        KCHECK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        KCHECK(cudaEventRecord(ev, st));
+        KCHECK(cudaStreamWaitEvent(S.stream, ev, 0));
+        cudaEventDestroy(ev);
+    }
+    return "";
+}
+
+std::string Simulator::synchronize() {
+    KCHECK(cudaSetDevice(d_->device));
+    KCHECK(cudaStreamSynchronize(d_->stream));
+    return "";
+}
+
+std::string Simulator::proba_state(double* out) {
+    SimImpl& S = *d_;
+    if (!S.has_state) return "no state: execute the simulator first";
+    KCHECK(cudaSetDevice(S.device));
+    std::vector<double> s0, s1;
+    std::string e = S.bit_sums(0, s0, s1, nullptr);
+    if (!e.empty()) return e;
+    // HIPcode/simulator.hpp:519-535 with the reference's Complex division,
+    // norm and angle (backendagnosticcode/basic_host_types.hpp:28-57).
+    const int n = S.n;
+    const double p = std::pow(kSqrt2, (double)n);
+    auto cdiv = [](double ar, double ai, double br, double bi, double& rr, double& ri) {
+        double d = br * br + bi * bi;
+        rr = (ar * br + ai * bi) / d;
+        ri = (br * ai - ar * bi) / d;
+    };
+    for (int x = 0; x < n; x++) {
+        int b = S.phys_of_label(x);
+        double v0r, v0i, v1r, v1i;
+        cdiv(s0[2 * b], s0[2 * b + 1], p, 0.0, v0r, v0i);
+        cdiv(s1[2 * b], s1[2 * b + 1], p, 0.0, v1r, v1i);
+        double n0 = std::sqrt(v0r * v0r + v0i * v0i), n1 = std::sqrt(v1r * v1r + v1i * v1i);
+        double teta, phi;
+        if (n0 < 0.0000000000001) {
+            teta = 1;
+            phi = 0;
+        } else if (n1 < 0.00000000000001) {
+            teta = 0;
+            phi = 0;
+        } else {
+            teta = std::atan(n1 / n0) / (kPi / 2);
+            double qr, qi;
+            cdiv(v1r, v1i, v0r, v0i, qr, qi);
+            phi = std::atan(qi / qr);
+        }
+        int o = S.plan.final_inverse_permutation.empty() ? x : S.plan.final_inverse_permutation[x];
+        out[2 * o] = teta;
+        out[2 * o + 1] = phi;
+    }
+    return "";
+}
+
+std::string Simulator::expect_z(double* out) {
+    SimImpl& S = *d_;
+    if (!S.has_state) return "no state: execute the simulator first";
+    KCHECK(cudaSetDevice(S.device));
+    std::vector<double> s0, s1;
+    std::string e = S.bit_sums(1, s0, s1, nullptr);
+    if (!e.empty()) return e;
+    for (int x = 0; x < S.n; x++) {
+        int b = S.phys_of_label(x);
+        out[x] = s0[b] - s1[b];
+    }
+    return "";
+}
+
+std::string Simulator::get_state(double* out) {
+    SimImpl& S = *d_;
+    if (!S.has_state) return "no state: execute the simulator first";
+    KCHECK(cudaSetDevice(S.device));
+    std::string e = S.run_relayout(S.label_layout());
+    if (!e.empty()) return e;
+    KCHECK(cudaMemcpyAsync(out, S.d_state, S.dim() * 16, cudaMemcpyDeviceToHost, S.stream));
+    KCHECK(cudaStreamSynchronize(S.stream));
+    return "";
+}
+
+std::string Simulator::set_state(const double* in) {
+    SimImpl& S = *d_;
+    KCHECK(cudaSetDevice(S.device));
+    KCHECK(cudaMemcpyAsync(S.d_state, in, S.dim() * 16, cudaMemcpyHostToDevice, S.stream));
+    KCHECK(cudaStreamSynchronize(S.stream));
+    S.phys = S.label_layout();
+    S.has_state = true;
+    return "";
+}
+
+std::string Simulator::probabilities(double* out) {
+    SimImpl& S = *d_;
+    if (!S.has_state) return "no state: execute the simulator first";
+    if (S.n > 30) return "probabilities are limited to 30 qubits";
+    KCHECK(cudaSetDevice(S.device));
+    std::string e = S.run_relayout(S.label_layout());
+    if (!e.empty()) return e;
+    double* d = nullptr;
+    KCHECK(cudaMallocAsync((void**)&d, S.dim() * sizeof(double), S.stream));
+    cudaError_t ce = launch_probs_c128(S.d_state, S.dim(), d, S.stream);
+    if (ce == cudaSuccess)
+        ce = cudaMemcpyAsync(out, d, S.dim() * sizeof(double), cudaMemcpyDeviceToHost, S.stream);
+    cudaFreeAsync(d, S.stream);
+    if (ce != cudaSuccess) return cuda_err("probabilities", ce);
+    KCHECK(cudaStreamSynchronize(S.stream));
+    return "";
+}
+
+std::string Simulator::sample(int shots, uint64_t seed, uint64_t* out) {
+    SimImpl& S = *d_;
+    if (shots < 0) return "shots must be >= 0";
+    if (S.n > 30) return "sampling is limited to 30 qubits";
+    std::vector<double> p(S.dim());
+    std::string e = probabilities(p.data());
+    if (!e.empty()) return e;
+    // Inverse-CDF sampling on sorted uniforms (splitmix64-seeded mt19937_64).
+    std::vector<double> cdf(p.size());
+    double acc = 0.0;
+    for (size_t i = 0; i < p.size(); i++) cdf[i] = (acc += p[i]);
+    std::mt19937_64 rng(seed);
+    std::uniform_real_distribution<double> U(0.0, 1.0);
+    for (int k = 0; k < shots; k++) {
+        double u = U(rng) * acc;
+        size_t idx = (size_t)(std::lower_bound(cdf.begin(), cdf.end(), u) - cdf.begin());
+        if (idx >= p.size()) idx = p.size() - 1;
+        out[k] = idx;
+    }
+    return "";
+}
+
+std::string Simulator::profile_passes(float* ms, float* init_ms) {
+    SimImpl& S = *d_;
+    KCHECK(cudaSetDevice(S.device));
+    std::vector<cudaEvent_t> ev(S.hpasses.size() + 2);
+    for (auto& e : ev) KCHECK(cudaEventCreate(&e));
+    KCHECK(cudaEventRecord(ev[0], S.stream));
+    KCHECK(launch_set_basis0_c128(S.d_state, S.dim(), S.stream));
+    KCHECK(cudaEventRecord(ev[1], S.stream));
+    for (size_t i = 0; i < S.hpasses.size(); i++) {
+        KCHECK(launch_pass_generic_c128(S.d_state, S.n, S.hpasses[i], S.d_ops, S.d_pool, S.grid, S.stream));
+        KCHECK(cudaEventRecord(ev[i + 2], S.stream));
+    }
+    KCHECK(cudaEventSynchronize(ev.back()));
+    if (init_ms) KCHECK(cudaEventElapsedTime(init_ms, ev[0], ev[1]));
+    for (size_t i = 0; i < S.hpasses.size(); i++) KCHECK(cudaEventElapsedTime(&ms[i], ev[i + 1], ev[i + 2]));
+    for (auto& e : ev) cudaEventDestroy(e);
+    S.phys = S.plan.final_phys;
+    S.has_state = true;
+    return "";
+}
+
+int Simulator::launches_per_run() const { return 1 + (int)d_->hpasses.size(); }
+
+std::string Simulator::state_device(void** dptr, int* phys) {
+    *dptr = d_->d_state;
+    for (int x = 0; x < d_->n; x++) phys[x] = d_->phys_of_label(x);
+    return "";
+}
+
+}  // namespace kate

@@ -1,0 +1,44 @@
+// Device simulator: owns the state vector and runs planned group passes.
+// Replaces the reference's GPU Simulator (HIPcode/simulator.hpp:220-811).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "circuit.hpp"
+#include "plan.hpp"
+
+namespace kate {
+
+struct SimImpl;
+
+class Simulator {
+public:
+    // Copies `prog` (compiling it with compileDefault(0) when it has no
+    // instructions), plans the passes and allocates the state on `device`.
+    static std::string create(const Program& prog, int precision, int device, Simulator** out);
+    ~Simulator();
+
+    std::string run_async(void* stream, const double* theta_phi_in);  // init + all passes, no sync
+    std::string synchronize();
+    std::string proba_state(double* theta_phi);                       // reference measurement
+    std::string get_state(double* out);                               // 2*2^n doubles, label order
+    std::string set_state(const double* in);
+    std::string expect_z(double* out);
+    std::string probabilities(double* out);
+    std::string sample(int shots, uint64_t seed, uint64_t* out);
+    std::string state_device(void** dptr, int* phys);
+    std::string profile_passes(float* ms, float* init_ms);
+    int launches_per_run() const;
+
+    int nqbits() const;
+    int precision() const;
+    const Plan& plan() const;
+    SimImpl* impl() { return d_; }
+
+private:
+    SimImpl* d_ = nullptr;
+};
+
+}  // namespace kate

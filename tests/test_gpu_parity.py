@@ -1,0 +1,99 @@
+"""Parity of the CUDA path with the oracle (Kate's CPU double-precision
+arithmetic), through the C ABI. Bar: max-abs amplitude error <= 1e-12."""
+import numpy as np
+import pytest
+
+import kate_b200 as K
+from kate_b200 import circuits
+from common import random_circuit
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+
+
+def run(n, gates, **kw):
+    sim = K.Simulator(K.Circuit(n, gates), 1, K.C128, 0)
+    res = sim.execute(**kw) if kw else sim.execute()
+    return sim, res
+
+
+def test_layered_n20_10_layers_matches_oracle(oracle):
+    n = 20
+    gates = circuits.layered(n, 10, seed=1234)
+    assert len(gates) == 590
+    sim, res = run(n, gates)
+    ref = oracle.simulate(n, gates)
+    assert np.abs(sim.state() - ref).max() <= TOL
+    assert np.abs(res.as_array() - oracle.measure(n, ref)).max() <= 1e-9
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 7, 9, 12, 13, 16])
+def test_random_circuits_all_gate_kinds(oracle, n):
+    rng = np.random.default_rng(100 + n)
+    gates = random_circuit(n, 120, rng)
+    sim, _ = run(n, gates)
+    assert np.abs(sim.state() - oracle.simulate(n, gates)).max() <= TOL
+
+
+def test_many_passes_with_remap_n22(oracle):
+    n = 22
+    rng = np.random.default_rng(7)
+    gates = circuits.layered(n, 3, seed=9) + random_circuit(n, 150, rng)
+    sim, _ = run(n, gates)
+    assert len(sim.passes()) > 3
+    assert np.abs(sim.state() - oracle.simulate(n, gates)).max() <= TOL
+
+
+def test_execute_from_product_state(oracle):
+    n = 14
+    rng = np.random.default_rng(3)
+    gates = random_circuit(n, 60, rng)
+    tp = np.stack([rng.uniform(0, 1, n), rng.uniform(-np.pi, np.pi, n)], axis=1)
+    sim = K.Simulator(K.Circuit(n, gates), 1, K.C128, 0)
+    res = sim.execute(K.proba_state(tp))
+    ref = oracle.simulate(n, gates, proba_in=tp)
+    assert np.abs(sim.state() - ref).max() <= TOL
+    assert np.abs(res.as_array() - oracle.measure(n, ref)).max() <= 1e-9
+
+
+def test_compiled_with_allocate_matches_reference(ref):
+    n = 12
+    rng = np.random.default_rng(11)
+    gates = random_circuit(n, 80, rng)
+    c = K.Circuit(n, gates)
+    c.gateScheduling()
+    c.gateFusion(4, 1e-6)
+    c.gateGrouping(8)
+    c.allocate(0)
+    rc = ref.circuit(n, gates)
+    rc.schedule(); rc.fuse(4, 1e-6); rc.group(8); rc.allocate(0)
+    rst, rpr, _ = rc.simulate()
+    sim = K.Simulator(c, 1, K.C128, 0)
+    pr = sim.execute()
+    assert np.abs(sim.state() - rst).max() <= TOL
+    assert np.abs(pr.as_array() - rpr).max() <= 1e-9
+
+
+def test_expect_z_and_probabilities(oracle):
+    n = 13
+    rng = np.random.default_rng(5)
+    gates = random_circuit(n, 50, rng)
+    sim, _ = run(n, gates)
+    st = oracle.simulate(n, gates)
+    p = np.abs(st) ** 2
+    z = np.array([p[((np.arange(1 << n) >> q) & 1) == 0].sum() - p[((np.arange(1 << n) >> q) & 1) == 1].sum()
+                  for q in range(n)])
+    assert np.abs(sim.expect_z() - z).max() <= 1e-12
+    assert np.abs(sim.probabilities() - p).max() <= 1e-12
+
+
+def test_sampling_follows_probabilities(oracle):
+    n = 6
+    rng = np.random.default_rng(2)
+    gates = random_circuit(n, 30, rng)
+    sim, _ = run(n, gates)
+    p = np.abs(oracle.simulate(n, gates)) ** 2
+    s = sim.sample(200000, seed=42)
+    hist = np.bincount(s.astype(np.int64), minlength=1 << n) / len(s)
+    assert np.abs(hist - p).max() < 0.01
+    assert np.array_equal(s[:100], sim.sample(100, seed=42)[:100])
