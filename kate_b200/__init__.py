@@ -131,6 +131,9 @@ class Circuit:
             gate = Gate(gate[3] if gate[0] == DENSE else gate[0], gate[1], gate[2])
         q = _iarr(gate.qbits)
         if gate.identifier == DENSE:
+            dim = 1 << len(gate.qbits)
+            if gate.densecontent is None or gate.densecontent.shape != (dim, dim):
+                raise KateError(KATE_EINVAL, "size mismatch: dense matrix dimension must be 2^k for k qubits")
             d = np.ascontiguousarray(gate.densecontent, dtype=np.complex128).view(np.float64).ravel()
             _check(self._lib.kate_circuit_append_dense(self._h, d.ctypes.data_as(_dp), q.ctypes.data_as(_ip),
                                                        len(gate.qbits)))

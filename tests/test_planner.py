@@ -1,0 +1,105 @@
+"""The group-pass planner, checked on the CPU: plans are executed by a numpy
+emulation of the kernel semantics (tests/plan_emulator.py) and compared with
+the oracle; structural invariants are checked directly."""
+import numpy as np
+import pytest
+
+import kate_b200 as K
+from kate_b200 import circuits
+from common import random_circuit
+from plan_emulator import PlanView
+
+NO_REMAP, NO_FUSE1Q = 1, 2
+
+
+def zero_state(n):
+    s = np.zeros(1 << n, dtype=np.complex128)
+    s[0] = 1
+    return s
+
+
+@pytest.mark.parametrize("seed", range(12))
+@pytest.mark.parametrize("opts", [(6, 2, 0), (8, 3, NO_REMAP), (5, 4, NO_FUSE1Q), (12, 4, 0), (4, 1, 0)])
+def test_emulated_plan_matches_oracle(oracle, seed, opts):
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(2, 12))
+    mt, co, fl = opts
+    mt = min(mt, n)
+    kinds = ("h", "cnot", "crk", "toff", "d1", "d2", "d3", "diag1", "diag2", "d5")
+    kinds = tuple(k for k in kinds if not (k == "d5" and mt < 5) and not (k == "d3" and mt < 3))
+    gates = random_circuit(n, int(rng.integers(1, 70)), rng, kinds=kinds)
+    pv = PlanView(K.Circuit(n, gates), mt, min(co, mt), fl)
+    out = pv.run(zero_state(n))
+    assert np.abs(out - oracle.simulate(n, gates)).max() <= 1e-12
+
+
+def test_layered_n20_plan_matches_oracle(oracle):
+    n = 20
+    gates = circuits.layered(n, 10, seed=1234)
+    pv = PlanView(K.Circuit(n, gates), 12, 4, 0)
+    assert np.abs(pv.run(zero_state(n)) - oracle.simulate(n, gates)).max() <= 1e-12
+
+
+def test_every_pass_keeps_the_low_bits_in_the_tile():
+    n = 24
+    pv = PlanView(K.Circuit(n, circuits.layered(n, 4)), 12, 4, 0)
+    for p in pv.passes:
+        assert p["tphys"][:4] == [0, 1, 2, 3]
+        assert sorted(p["outsrc"]) == list(range(p["m"]))
+        assert p["tphys"] == sorted(p["tphys"])
+    assert sorted(pv.final_phys) == list(range(n))
+
+
+def test_headline_plan_pass_count():
+    # 30 qubits, 20 layers of RX/RZ/CNOT ladder with 12-qubit tiles: about
+    # three passes per layer (each pass advances the ladder by ~11 qubits).
+    pv = PlanView(K.Circuit(30, circuits.layered(30, 20)), 12, 4, 0)
+    assert len(pv.passes) <= 62
+    ops = sum(p["nops"] for p in pv.passes)
+    assert ops == 20 * 30 + 20 * 29  # one fused 2x2 per qubit per layer + the CNOTs
+
+
+def test_single_qubit_chains_are_fused():
+    pv = PlanView(K.Circuit(4, circuits.layered(4, 1)), 4, 2, 0)
+    assert sum(p["nops"] for p in pv.passes) == 4 + 3
+    pv2 = PlanView(K.Circuit(4, circuits.layered(4, 1)), 4, 2, NO_FUSE1Q)
+    assert sum(p["nops"] for p in pv2.passes) == 8 + 3
+
+
+def test_diagonal_gates_may_sit_outside_the_tile(oracle):
+    # CRk and diagonal dense gates act as free qubits: one pass suffices even
+    # when they touch qubits outside a 4-qubit tile.
+    n = 10
+    gates = [(2, [q], 0, None) for q in range(4)] + [(4, [0, 9], 3, None), (4, [8, 7], 2, None),
+                                                      (0, [9], 0, np.diag([1, 1j]))]
+    pv = PlanView(K.Circuit(n, gates), 4, 2, 0)
+    assert len(pv.passes) == 1
+    assert np.abs(pv.run(zero_state(n)) - oracle.simulate(n, gates)).max() <= 1e-12
+
+
+def test_swap_instructions_become_relabelings(oracle, ref):
+    # allocate(g > 0) emits swap instructions (Circuit.hpp:207-348). On one
+    # GPU a swap of positions p1, p2 is a relabeling; its meaning is a SWAP
+    # gate on those positions in the program's label space.
+    n = 8
+    rng = np.random.default_rng(4)
+    gates = random_circuit(n, 40, rng, kinds=("h", "cnot", "d1", "d2", "crk"))
+    c = K.Circuit(n, gates)
+    c.gateGrouping(5)
+    c.allocate(2)
+    ins = c.instructions
+    assert any(k == 0 for k, _ in ins)
+    swap = np.eye(4)[[0, 2, 1, 3]].astype(np.complex128)
+    seq, gi, k0 = [], 0, 0
+    comp = c.gate_set_ordered
+    groups = c.groups
+    for kind, qs in ins:
+        if kind == 0:
+            for a, b in zip(qs[::2], qs[1::2]):
+                seq.append((0, [a, b], 0, swap))
+        else:
+            end = groups[gi][0]
+            seq += comp[k0:end]
+            k0, gi = end, gi + 1
+    pv = PlanView(c, 6, 2, 0)
+    assert np.abs(pv.run(zero_state(n)) - oracle.simulate(n, seq)).max() <= 1e-12
