@@ -219,6 +219,13 @@ KATE_API kate_status kate_plan_num_ops(const kate_plan* p, int* out);
  * = phase (re, im) then the op's matrix or diagonal table (re, im pairs).
  * kinds: 0 dense, 1 H, 2 controlled X, 3 controlled phase, 4 diagonal. */
 KATE_API kate_status kate_plan_get_op(const kate_plan* p, int i, int* ints, uint64_t* pmask, double* vals);
+/* Register-staged program of pass i (the PassProg struct of
+ * kate_b200/csrc/device_types.h, *size bytes, copied when cap allows);
+ * *has = 0 when the pass runs on the generic shared-memory kernel. */
+KATE_API kate_status kate_plan_get_program(const kate_plan* p, int i, void* out, size_t cap, size_t* size, int* has);
+KATE_API kate_status kate_plan_num_smem_ops(const kate_plan* p, int* out);
+/* Shared-memory op i of the register-staged programs, same format as kate_plan_get_op. */
+KATE_API kate_status kate_plan_get_smem_op(const kate_plan* p, int i, int* ints, uint64_t* pmask, double* vals);
 /* phys[q]: physical bit of logical qubit q after the last pass;
  * label_to_logical[x]: logical qubit held by program label x. */
 KATE_API kate_status kate_plan_final_layout(const kate_plan* p, int* phys, int* label_to_logical);

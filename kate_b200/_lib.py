@@ -67,6 +67,9 @@ SIGNATURES = {
     "kate_plan_num_ops": [_vp, _ip],
     "kate_plan_get_op": [_vp, _i, _ip, _u64p, _dp],
     "kate_plan_final_layout": [_vp, _ip, _ip],
+    "kate_plan_get_program": [_vp, _i, _vp, _c.c_size_t, _c.POINTER(_c.c_size_t), _ip],
+    "kate_plan_num_smem_ops": [_vp, _ip],
+    "kate_plan_get_smem_op": [_vp, _i, _ip, _u64p, _dp],
 }
 _RET = {"kate_last_error": _c.c_char_p, "kate_version": _c.c_char_p}
 

@@ -485,10 +485,8 @@ kate_status kate_plan_num_ops(const kate_plan* p, int* out) {
     return KATE_OK;
 }
 
-kate_status kate_plan_get_op(const kate_plan* p, int i, int* ints, uint64_t* pmask, double* vals) {
-    REQUIRE(p && ints && pmask && vals, "null pointer");
-    REQUIRE(i >= 0 && i < (int)p->ops.size(), "op index out of range");
-    const DevOp& o = p->ops[i];
+namespace {
+kate_status export_op(const kate::Plan& plan, const DevOp& o, int* ints, uint64_t* pmask, double* vals) {
     ints[0] = o.kind;
     ints[1] = o.k;
     for (int j = 0; j < 5; j++) {
@@ -504,10 +502,39 @@ kate_status kate_plan_get_op(const kate_plan* p, int i, int* ints, uint64_t* pma
     if (o.kind == OPK_DENSE) len = (size_t)1 << (2 * o.k);
     else if (o.kind == OPK_DIAG) len = (size_t)1 << o.k;
     for (size_t j = 0; j < len; j++) {
-        vals[2 + 2 * j] = p->plan.pool[o.mat + j].re;
-        vals[3 + 2 * j] = p->plan.pool[o.mat + j].im;
+        vals[2 + 2 * j] = plan.pool[o.mat + j].re;
+        vals[3 + 2 * j] = plan.pool[o.mat + j].im;
     }
     return KATE_OK;
+}
+}  // namespace
+
+kate_status kate_plan_get_op(const kate_plan* p, int i, int* ints, uint64_t* pmask, double* vals) {
+    REQUIRE(p && ints && pmask && vals, "null pointer");
+    REQUIRE(i >= 0 && i < (int)p->ops.size(), "op index out of range");
+    return export_op(p->plan, p->ops[i], ints, pmask, vals);
+}
+
+kate_status kate_plan_get_program(const kate_plan* p, int i, void* out, size_t cap, size_t* size, int* has) {
+    REQUIRE(p && size && has, "null pointer");
+    REQUIRE(i >= 0 && i < (int)p->plan.passes.size(), "pass index out of range");
+    *size = sizeof(PassProg);
+    const auto& pp = p->plan.passes[i];
+    *has = pp.prog ? 1 : 0;
+    if (pp.prog && out && cap >= sizeof(PassProg)) std::memcpy(out, pp.prog.get(), sizeof(PassProg));
+    return KATE_OK;
+}
+
+kate_status kate_plan_num_smem_ops(const kate_plan* p, int* out) {
+    REQUIRE(p && out, "null pointer");
+    *out = (int)p->plan.smem_ops.size();
+    return KATE_OK;
+}
+
+kate_status kate_plan_get_smem_op(const kate_plan* p, int i, int* ints, uint64_t* pmask, double* vals) {
+    REQUIRE(p && ints && pmask && vals, "null pointer");
+    REQUIRE(i >= 0 && i < (int)p->plan.smem_ops.size(), "op index out of range");
+    return export_op(p->plan, p->plan.smem_ops[i], ints, pmask, vals);
 }
 
 kate_status kate_plan_final_layout(const kate_plan* p, int* phys, int* l2l) {

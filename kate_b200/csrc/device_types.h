@@ -25,6 +25,64 @@ typedef struct {
     double ph_re, ph_im;
 } DevOp;
 
+// ---- Register-staged pass program (the tile kernel's instruction stream) ----
+// A pass is a sequence of stages. A register stage holds 16 amplitudes per
+// thread (256 threads x 16 = the 4096-amplitude tile): register-index bit i
+// is tile bit rb[i], thread-index bit i is tile bit tb[i]. Single-qubit ops
+// whose target is a register bit run on registers; controls and diagonal
+// bits may be register, thread or coset bits. Anything else runs as a
+// shared-memory op between register stages.
+#define SOP_STAGE 1  // store registers (if a stage is open), sync, load with rb/tb
+#define SOP_SMEM 2   // generic op on the shared-memory tile (DevOp index idx)
+#define SOP_U 3      // 2x2 on register bit a; matrix mats[idx .. idx+3] (row-major)
+#define SOP_H 4      // Hadamard on register bit a (the reference's arithmetic)
+#define SOP_X 5      // NOT on register bit a where controls creg/cthr/ccos are all 1
+#define SOP_PH 6     // multiply by mats[idx] where controls creg/cthr/ccos are all 1
+#define SOP_D1 7     // multiply by mats[idx + bit]; bit from register/thread/coset bit a (src)
+#define SOP_UR 8     // 2x2 with real entries on register bit a: mats[idx..idx+3].x (4 FP64 ops/amplitude)
+#define SOP_UX 9     // 2x2 [[a, ib], [ic, d]] (a, b, c, d real) on register bit a: 4 FP64 ops/amplitude
+#define SOP_DR 10    // diagonal over the register bits: multiply register j by mats[idx + j]
+
+#define SRC_REG 0
+#define SRC_THR 1
+#define SRC_COS 2
+
+#define KATE_TILE_BITS 12
+#define KATE_MAX_SOPS 160
+#define KATE_MAX_MATS 640
+#define KATE_MAX_STAGES 40
+
+typedef struct {
+    uint8_t kind;
+    uint8_t a;       // register bit (U/H/X; D1 SRC_REG), thread bit (D1 SRC_THR) or physical bit (D1 SRC_COS)
+    uint8_t src;     // D1 source
+    uint8_t creg;    // controls on register bits (register-index mask)
+    uint8_t cthr;    // controls on thread bits (thread-index mask)
+    uint8_t pad;
+    uint16_t idx;    // mats index (U, PH, D1, DR), DevOp index (SMEM) or stage index (STAGE)
+    uint64_t ccos;   // controls on coset bits (physical-bit mask)
+} SOp;               // 16 bytes: one shared-memory vector load per op
+
+typedef struct {
+    int32_t m, ncb, nops, nmats;
+    uint8_t tphys[16];
+    uint8_t outsrc[16];
+    uint8_t cphys[48];
+    SOp ops[KATE_MAX_SOPS];
+    double mats[KATE_MAX_MATS][2];
+    // Per stage (SOP_STAGE idx): byte offsets in the swizzled tile. The
+    // offset of thread t's register j is s0(t) ^ W(j) with
+    // s0(t) = stab[idx][t & 15] ^ stab[idx][16 + (t >> 4)] and W(j) the XOR
+    // of stab[idx][32 + i] over the set bits i of j.
+    uint16_t stab[KATE_MAX_STAGES][36];
+    // Per stage: tile bit of register-index bit i (rb) and of thread-index
+    // bit i (tb), the layout the tables above encode.
+    uint8_t srb[KATE_MAX_STAGES][4];
+    uint8_t stb[KATE_MAX_STAGES][8];
+    int32_t nstages;
+    int32_t sop0;    // first shared-memory op of this pass in the simulator's array (SMEM idx is relative)
+} PassProg;
+
 typedef struct {
     int32_t m;          // tile bits
     int32_t nops;

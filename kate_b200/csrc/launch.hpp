@@ -22,6 +22,12 @@ cudaError_t launch_init_product_c128(void* st, int n, const ProductInit& P, cuda
 cudaError_t launch_pass_generic_c128(void* st, int n, const DevPass& p, const DevOp* ops, const void* pool,
                                      int grid, cudaStream_t s);
 int generic_pass_grid(int n, int m, int device);
+// Register-staged tile kernel (12-qubit tiles, 256 threads x 16 amplitudes).
+// nbuf = 2: one CTA per SM with a prefetched second tile; nbuf = 1: two
+// CTAs per SM with one tile each.
+cudaError_t launch_tile_c128(void* st, const PassProg& prog, const DevOp* sops, const void* pool, int grid, int nbuf,
+                             cudaStream_t s);
+int tile_pass_grid(int n, int device, int nbuf);
 
 // Bit sums: per CTA, for every local bit, the sum over amplitudes with the
 // bit 0 and with the bit 1, plus the total. kind 0 sums amplitudes (double2

@@ -103,6 +103,14 @@ void matrix_2x2(const PGate& g, Cx m[4]) {
     }
 }
 
+// FP64 operations per amplitude of a 2x2 in the tile kernel (diagonals ~1:
+// they merge into the stage's register diagonal).
+int cost_2x2(const Cx m[4]) {
+    if (m[1].re == 0.0 && m[1].im == 0.0 && m[2].re == 0.0 && m[2].im == 0.0) return 1;
+    int k = classify_2x2(m);
+    return k == SOP_U ? 8 : 4;
+}
+
 PGate make_1q(int q, const Cx m[4], int src) {
     PGate p;
     p.src = src;
@@ -133,8 +141,14 @@ std::vector<PGate> fuse_single_qubit(std::vector<PGate>&& in, int n) {
                 matrix_2x2(prev, b);
                 for (int i = 0; i < 2; i++)
                     for (int j = 0; j < 2; j++) r[2 * i + j] = a[2 * i] * b[j] + a[2 * i + 1] * b[2 + j];
-                prev = make_1q(q, r, prev.src);
-                continue;
+                // Multiply only when the product is no dearer than the two
+                // ops apart: diagonals are nearly free (the tile kernel merges
+                // all register-bit diagonals of a stage into one multiply),
+                // real and RX-form 2x2s cost half a general one.
+                if (cost_2x2(r) <= cost_2x2(a) + cost_2x2(b)) {
+                    prev = make_1q(q, r, prev.src);
+                    continue;
+                }
             }
         }
         out.push_back(std::move(g));
@@ -371,6 +385,23 @@ std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out) {
             tsize++;
         }
         std::vector<int> exec = greedy_pass(plan.pgates, rem, n, m, inT, tsize, nullptr, scan_limit);
+        if ((int)exec.size() > opt.max_gates_per_pass) {
+            // Keep a prefix of the executable gates (a prefix of a
+            // dependency-closed set in program order is dependency-closed).
+            exec.resize(opt.max_gates_per_pass);
+            std::fill(inT.begin(), inT.end(), 0);
+            tsize = 0;
+            for (int p = 0; p < c; p++) {
+                inT[L.inv[p]] = 1;
+                tsize++;
+            }
+            for (int gi : exec)
+                for (int q : plan.pgates[gi].tq)
+                    if (!inT[q]) {
+                        inT[q] = 1;
+                        tsize++;
+                    }
+        }
         if (exec.empty()) return "planner made no progress";
         for (int p = 0; p < n && tsize < m; p++)
             if (!inT[L.inv[p]]) {
@@ -436,6 +467,12 @@ std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out) {
             pp.out_tile[t] = (int)(std::lower_bound(S.begin(), S.end(), nphys[q]) - S.begin());
         }
         lower_pass(plan, pp, L.phys, plan.pool);
+        pp.phys_before = L.phys;
+        if (opt.staged) {
+            auto prog = std::make_shared<PassProg>();
+            pp.prog_note = build_pass_program(plan, pp, n, plan.smem_ops, plan.pool, prog.get());
+            if (pp.prog_note.empty()) pp.prog = prog;
+        }
         plan.passes.push_back(std::move(pp));
         L.phys = nphys;
         for (int q = 0; q < n; q++) L.inv[L.phys[q]] = q;

@@ -23,6 +23,7 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -36,6 +37,8 @@ struct PlanOptions {
     int coalesce = 4;    // c: low physical bits every tile must contain
     bool remap = true;   // move next-needed qubits into the low bits on write
     bool fuse_1q = true; // multiply chains of single-qubit ops on one qubit (FP64, host)
+    bool staged = true;  // build register-staged programs for the tile kernel
+    int max_gates_per_pass = 96;  // keeps a pass program within the kernel parameter
 };
 
 struct PlannedPass {
@@ -43,7 +46,10 @@ struct PlannedPass {
     std::vector<int> phys_in;    // physical position of tile bit t (ascending)
     std::vector<int> out_tile;   // input tile bit t is written to tile bit out_tile[t]
     std::vector<int> gates;      // indices into Plan::pgates executed by this pass
-    std::vector<DevOp> ops;      // device ops, tile-relative
+    std::vector<DevOp> ops;      // device ops, tile-relative (generic kernel)
+    std::vector<int> phys_before;  // layout (logical -> physical) when the pass starts
+    std::shared_ptr<PassProg> prog;  // register-staged program (tile kernel), if it applies
+    std::string prog_note;           // why the generic kernel runs this pass, if it does
 };
 
 // A gate as the planner sees it (logical qubits).
@@ -64,6 +70,7 @@ struct Plan {
     std::vector<int> label_to_logical;  // program label x holds logical qubit label_to_logical[x] at the end
     std::vector<int> initial_permutation, final_inverse_permutation;
     std::vector<Cx> pool;            // dense matrices and diagonal tables of all ops
+    std::vector<DevOp> smem_ops;     // shared-memory ops referenced by register-staged programs
 };
 
 // Classifies gates, plans passes and lowers them to device ops. Dense gates
@@ -73,6 +80,14 @@ std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out);
 // Remap-only passes taking layout `phys` (logical -> physical) to `target`.
 std::vector<PlannedPass> plan_relayout(int n, const std::vector<int>& phys, const std::vector<int>& target,
                                        const PlanOptions& opt);
+
+// Register-staged program of a pass (12-qubit tiles). Non-register ops are
+// appended to smem_ops (their tables to pool). Returns "" on success.
+std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n, std::vector<DevOp>& smem_ops,
+                               std::vector<Cx>& pool, PassProg* out);
+
+// Register-op form of a 2x2 matrix: SOP_UR (real), SOP_UX ([[a, ib], [ic, d]]) or SOP_U.
+int classify_2x2(const Cx* m);
 
 // Device descriptor of a pass whose ops start at op0.
 DevPass to_devpass(int n, const PlannedPass& p, int op0);

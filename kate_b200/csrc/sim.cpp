@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <random>
@@ -36,6 +37,7 @@ struct SimImpl {
     PlanOptions opt;
     void* d_state = nullptr;
     DevOp* d_ops = nullptr;
+    DevOp* d_sops = nullptr;   // shared-memory ops of register-staged programs
     void* d_pool = nullptr;
     void* d_part = nullptr;
     size_t part_bytes = 0;
@@ -44,6 +46,15 @@ struct SimImpl {
     std::vector<int> phys;  // current layout: logical -> physical
     bool has_state = false;
     int grid = 0;
+    int tile_grid = 0;
+    int nbuf = 2;  // tile kernel buffering (1 or 2), see launch_tile_c128
+
+    // Launches pass i of the plan on stream st.
+    cudaError_t launch_pass(size_t i, cudaStream_t st) {
+        const PlannedPass& p = plan.passes[i];
+        if (p.prog) return launch_tile_c128(d_state, *p.prog, d_sops, d_pool, tile_grid, nbuf, st);
+        return launch_pass_generic_c128(d_state, n, hpasses[i], d_ops, d_pool, grid, st);
+    }
 
     uint64_t dim() const { return 1ull << n; }
     size_t amp_bytes() const { return precision == 0 ? 16 : 8; }
@@ -140,6 +151,11 @@ std::string Simulator::create(const Program& prog_in, int precision, int device,
     if (ce != cudaSuccess) return fail(cuda_err("cudaMalloc(ops)", ce));
     ce = cudaMalloc(&impl->d_pool, pool_bytes);
     if (ce != cudaSuccess) return fail(cuda_err("cudaMalloc(pool)", ce));
+    ce = cudaMalloc(&impl->d_sops, std::max<size_t>(1, impl->plan.smem_ops.size()) * sizeof(DevOp));
+    if (ce != cudaSuccess) return fail(cuda_err("cudaMalloc(smem ops)", ce));
+    if (!impl->plan.smem_ops.empty())
+        cudaMemcpy(impl->d_sops, impl->plan.smem_ops.data(), impl->plan.smem_ops.size() * sizeof(DevOp),
+                   cudaMemcpyHostToDevice);
     if (!ops.empty()) cudaMemcpy(impl->d_ops, ops.data(), ops.size() * sizeof(DevOp), cudaMemcpyHostToDevice);
     if (!impl->plan.pool.empty())
         cudaMemcpy(impl->d_pool, impl->plan.pool.data(), impl->plan.pool.size() * sizeof(Cx), cudaMemcpyHostToDevice);
@@ -150,6 +166,8 @@ std::string Simulator::create(const Program& prog_in, int precision, int device,
     ce = cudaMalloc(&impl->d_state, impl->dim() * impl->amp_bytes());
     if (ce != cudaSuccess) return fail(cuda_err("cudaMalloc(state)", ce));
     impl->grid = generic_pass_grid(impl->n, std::min(impl->opt.max_tile, impl->n), device);
+    if (const char* e = std::getenv("KATE_TILE_NBUF")) impl->nbuf = std::atoi(e) == 1 ? 1 : 2;
+    if (impl->n >= KATE_TILE_BITS) impl->tile_grid = tile_pass_grid(impl->n, device, impl->nbuf);
     impl->phys.resize(impl->n);
     std::iota(impl->phys.begin(), impl->phys.end(), 0);
     auto* s = new Simulator();
@@ -164,6 +182,7 @@ Simulator::~Simulator() {
     if (d_->stream) cudaStreamSynchronize(d_->stream);
     cudaFree(d_->d_state);
     cudaFree(d_->d_ops);
+    cudaFree(d_->d_sops);
     cudaFree(d_->d_pool);
     cudaFree(d_->d_part);
     if (d_->stream) cudaStreamDestroy(d_->stream);
@@ -196,7 +215,7 @@ std::string Simulator::run_async(void* stream_in, const double* tp) {
     } else {
         KCHECK(launch_set_basis0_c128(S.d_state, S.dim(), st));
     }
-    for (auto& p : S.hpasses) KCHECK(launch_pass_generic_c128(S.d_state, S.n, p, S.d_ops, S.d_pool, S.grid, st));
+    for (size_t i = 0; i < S.hpasses.size(); i++) KCHECK(S.launch_pass(i, st));
     S.phys = S.plan.final_phys;
     S.has_state = true;
     if (st != S.stream) {
@@ -342,7 +361,7 @@ std::string Simulator::profile_passes(float* ms, float* init_ms) {
     KCHECK(launch_set_basis0_c128(S.d_state, S.dim(), S.stream));
     KCHECK(cudaEventRecord(ev[1], S.stream));
     for (size_t i = 0; i < S.hpasses.size(); i++) {
-        KCHECK(launch_pass_generic_c128(S.d_state, S.n, S.hpasses[i], S.d_ops, S.d_pool, S.grid, S.stream));
+        KCHECK(S.launch_pass(i, S.stream));
         KCHECK(cudaEventRecord(ev[i + 2], S.stream));
     }
     KCHECK(cudaEventSynchronize(ev.back()));

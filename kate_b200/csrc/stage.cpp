@@ -1,0 +1,309 @@
+// Lowering of a planned pass into the register-staged program run by the
+// tile kernel (k_tile.cu). See device_types.h for the program format.
+//
+// The pass's ops are list-scheduled into stages. A stage fixes four tile
+// bits as register bits; ops whose target is one of them (2x2, H, X) or
+// that have no target (controlled phase, one-qubit diagonal) are applied to
+// registers. Ops are reordered only across ops that share no qubit, so the
+// result is unchanged. Each stage boundary costs one round trip of the tile
+// through shared memory, so the scheduler first takes ready ops whose target
+// is already a register bit, then grows the register set (up to four bits),
+// and closes the stage only when neither is possible.
+#include <algorithm>
+#include <cstring>
+
+#include "plan.hpp"
+
+namespace kate {
+
+namespace {
+
+struct LOp {
+    int kind = 0;        // SOP_*
+    int tgt = -1;        // target tile bit
+    uint32_t tctl = 0;   // control tile bits
+    uint64_t pctl = 0;   // control coset (physical) bits
+    int dtile = -1;      // D1: tile bit, or -1
+    int dphys = -1;      // D1: physical bit when outside the tile
+    Cx m[4];
+    int smem = -1;       // SMEM: index into smem_ops
+    std::vector<int> qs; // logical qubits (dependencies)
+};
+
+}  // namespace
+
+int classify_2x2(const Cx* m) {
+    bool real = true, rx = true;
+    for (int i = 0; i < 4; i++) real &= m[i].im == 0.0;
+    rx = m[0].im == 0.0 && m[3].im == 0.0 && m[1].re == 0.0 && m[2].re == 0.0;
+    return real ? SOP_UR : rx ? SOP_UX : SOP_U;
+}
+
+std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n, std::vector<DevOp>& smem_ops,
+                               std::vector<Cx>& pool, PassProg* out) {
+    const int m = (int)pass.phys_in.size();
+    if (m != KATE_TILE_BITS) return "register-staged kernel needs 12-qubit tiles";
+    const std::vector<int>& phys = pass.phys_before;
+    const int sop_begin = (int)smem_ops.size();
+    auto tile_bit = [&](int q) -> int {
+        int p = phys[q];
+        for (int t = 0; t < m; t++)
+            if (pass.phys_in[t] == p) return t;
+        return -1;
+    };
+    std::vector<LOp> L;
+    for (int gi : pass.gates) {
+        const PGate& g = plan.pgates[gi];
+        LOp o;
+        o.qs = g.tq;
+        o.qs.insert(o.qs.end(), g.fq.begin(), g.fq.end());
+        auto controls = [&]() {
+            for (int q : g.fq) {
+                int t = tile_bit(q);
+                if (t >= 0) o.tctl |= 1u << t;
+                else o.pctl |= 1ull << phys[q];
+            }
+        };
+        if (g.kind == OPK_DENSE && g.tq.size() == 1) {
+            o.kind = classify_2x2(g.table.data());
+            o.tgt = tile_bit(g.tq[0]);
+            for (int i = 0; i < 4; i++) o.m[i] = g.table[i];
+        } else if (g.kind == OPK_H) {
+            o.kind = SOP_H;
+            o.tgt = tile_bit(g.tq[0]);
+        } else if (g.kind == OPK_X) {
+            o.kind = SOP_X;
+            o.tgt = tile_bit(g.tq[0]);
+            controls();
+        } else if (g.kind == OPK_PHASE) {
+            o.kind = SOP_PH;
+            controls();
+            o.m[0] = Cx(g.ph_re, g.ph_im);
+        } else if (g.kind == OPK_DIAG && g.fq.size() == 1) {
+            o.kind = SOP_D1;
+            o.dtile = tile_bit(g.fq[0]);
+            if (o.dtile < 0) o.dphys = phys[g.fq[0]];
+            o.m[0] = g.table[0];
+            o.m[1] = g.table[1];
+        } else {
+            o.kind = SOP_SMEM;
+            PlannedPass one;
+            one.phys_in = pass.phys_in;
+            one.gates = {gi};
+            lower_pass(plan, one, phys, pool);
+            o.smem = (int)smem_ops.size();
+            smem_ops.push_back(one.ops[0]);
+        }
+        if ((o.kind == SOP_U || o.kind == SOP_UR || o.kind == SOP_UX || o.kind == SOP_H || o.kind == SOP_X) &&
+            o.tgt < 0)
+            return "internal: target outside the tile";
+        L.push_back(std::move(o));
+    }
+    const int N = (int)L.size();
+    // Dependencies: the previous op touching any of the same qubits.
+    std::vector<std::vector<int>> preds(N);
+    {
+        std::vector<int> last(n, -1);
+        for (int i = 0; i < N; i++) {
+            for (int q : L[i].qs)
+                if (last[q] >= 0) preds[i].push_back(last[q]);
+            for (int q : L[i].qs) last[q] = i;
+        }
+    }
+    std::vector<char> done(N, 0);
+    auto ready = [&](int i, const std::vector<char>& d) {
+        if (d[i]) return false;
+        for (int p : preds[i])
+            if (!d[p]) return false;
+        return true;
+    };
+    auto regable = [&](int i) { return L[i].kind != SOP_SMEM; };
+
+    std::memset(out, 0, sizeof(PassProg));
+    DevPass dp = to_devpass(n, pass, 0);
+    out->m = m;
+    out->ncb = dp.ncb;
+    std::memcpy(out->tphys, dp.tphys, 16);
+    std::memcpy(out->outsrc, dp.outsrc, 16);
+    std::memcpy(out->cphys, dp.cphys, 48);
+    out->sop0 = sop_begin;
+    std::vector<SOp> ops;
+    std::vector<Cx> mats;
+
+    int scheduled = 0;
+    while (scheduled < N) {
+        // Tentative register stage.
+        std::vector<char> d2(done);
+        std::vector<int> R, list;
+        for (;;) {
+            int pick = -1;
+            for (int i = 0; i < N && pick < 0; i++)
+                if (regable(i) && ready(i, d2) &&
+                    (L[i].tgt < 0 || std::find(R.begin(), R.end(), L[i].tgt) != R.end()))
+                    pick = i;
+            if (pick < 0 && R.size() < 4)
+                for (int i = 0; i < N && pick < 0; i++)
+                    if (regable(i) && ready(i, d2) && L[i].tgt >= 0) {
+                        pick = i;
+                        R.push_back(L[i].tgt);
+                    }
+            if (pick < 0) break;
+            d2[pick] = 1;
+            list.push_back(pick);
+        }
+        if (list.empty()) {
+            int first = -1;
+            for (int i = 0; i < N && first < 0; i++)
+                if (ready(i, done)) first = i;
+            if (first < 0 || regable(first)) return "internal: stage scheduler stalled";
+            SOp s{};
+            s.kind = SOP_SMEM;
+            s.idx = (uint16_t)(L[first].smem - out->sop0);
+            ops.push_back(s);
+            done[first] = 1;
+            scheduled++;
+            continue;
+        }
+        for (int t = 0; t < m && R.size() < 4; t++)
+            if (std::find(R.begin(), R.end(), t) == R.end()) R.push_back(t);
+        // Thread map: three low thread bits on tile bits of distinct residue
+        // mod 3 (conflict-free 16-byte accesses under the XOR swizzle of
+        // k_tile.cu), then the other non-register bits ascending.
+        std::vector<int> nonR, tb;
+        for (int t = 0; t < m; t++)
+            if (std::find(R.begin(), R.end(), t) == R.end()) nonR.push_back(t);
+        bool res_used[3] = {false, false, false};
+        for (int t : nonR)
+            if (tb.size() < 3 && !res_used[t % 3]) {
+                res_used[t % 3] = true;
+                tb.push_back(t);
+            }
+        for (int t : nonR)
+            if (std::find(tb.begin(), tb.end(), t) == tb.end()) tb.push_back(t);
+        SOp st{};
+        st.kind = SOP_STAGE;
+        if (out->nstages >= KATE_MAX_STAGES) return "pass program has too many stages";
+        st.idx = (uint16_t)out->nstages;
+        for (int i = 0; i < 4; i++) out->srb[out->nstages][i] = (uint8_t)R[i];
+        for (int i = 0; i < 8; i++) out->stb[out->nstages][i] = (uint8_t)tb[i];
+        {
+            auto swz = [](uint32_t i) { return i ^ (((i >> 3) ^ (i >> 6) ^ (i >> 9)) & 7u); };
+            uint16_t* tab = out->stab[out->nstages];
+            for (int v = 0; v < 16; v++) {
+                uint32_t lo = 0, hi = 0;
+                for (int i = 0; i < 4; i++) {
+                    if ((v >> i) & 1) lo |= 1u << tb[i];
+                    if ((v >> i) & 1) hi |= 1u << tb[4 + i];
+                }
+                tab[v] = (uint16_t)(swz(lo) << 4);
+                tab[16 + v] = (uint16_t)(swz(hi) << 4);
+            }
+            for (int i = 0; i < 4; i++) tab[32 + i] = (uint16_t)(swz(1u << R[i]) << 4);
+        }
+        out->nstages++;
+        ops.push_back(st);
+        auto regpos = [&](int t) { return (int)(std::find(R.begin(), R.end(), t) - R.begin()); };
+        auto thrpos = [&](int t) { return (int)(std::find(tb.begin(), tb.end(), t) - tb.begin()); };
+        auto ctl = [&](const LOp& o, SOp& s) {
+            for (int t = 0; t < m; t++)
+                if ((o.tctl >> t) & 1u) {
+                    int r = regpos(t);
+                    if (r < 4) s.creg |= (uint8_t)(1u << r);
+                    else s.cthr |= (uint8_t)(1u << thrpos(t));
+                }
+            s.ccos = o.pctl;
+        };
+        // Diagonals over register bits (one-qubit diagonals, phases whose
+        // controls are all register bits) are multiplied into one pending
+        // 16-entry table and emitted as a single op just before the first op
+        // that targets one of the bits it depends on (they commute with
+        // everything else), or at the end of the stage.
+        Cx dr[16];
+        uint32_t dr_support = 0;
+        auto dr_reset = [&]() {
+            for (auto& v : dr) v = Cx(1.0, 0.0);
+            dr_support = 0;
+        };
+        auto dr_flush = [&]() {
+            if (!dr_support) return;
+            SOp f{};
+            f.kind = SOP_DR;
+            f.idx = (uint16_t)mats.size();
+            mats.insert(mats.end(), dr, dr + 16);
+            ops.push_back(f);
+            dr_reset();
+        };
+        dr_reset();
+        for (int i : list) {
+            const LOp& o = L[i];
+            SOp s{};
+            s.kind = (uint8_t)o.kind;
+            if (o.tgt >= 0 && dr_support && ((dr_support >> regpos(o.tgt)) & 1u)) dr_flush();
+            switch (o.kind) {
+            case SOP_U:
+            case SOP_UR:
+            case SOP_UX:
+                s.a = (uint8_t)regpos(o.tgt);
+                s.idx = (uint16_t)mats.size();
+                mats.insert(mats.end(), o.m, o.m + 4);
+                break;
+            case SOP_H:
+                s.a = (uint8_t)regpos(o.tgt);
+                break;
+            case SOP_X:
+                s.a = (uint8_t)regpos(o.tgt);
+                ctl(o, s);
+                break;
+            case SOP_PH:
+                ctl(o, s);
+                if (s.cthr == 0 && s.ccos == 0) {
+                    for (int j = 0; j < 16; j++)
+                        if (((uint32_t)j & s.creg) == s.creg) dr[j] = dr[j] * o.m[0];
+                    dr_support |= s.creg ? s.creg : 1u;
+                    s.kind = 0;
+                    break;
+                }
+                s.idx = (uint16_t)mats.size();
+                mats.push_back(o.m[0]);
+                break;
+            case SOP_D1:
+                if (o.dtile >= 0) {
+                    int r = regpos(o.dtile);
+                    if (r < 4) {
+                        for (int j = 0; j < 16; j++) dr[j] = dr[j] * o.m[(j >> r) & 1];
+                        dr_support |= 1u << r;
+                        s.kind = 0;
+                        break;
+                    }
+                    s.src = SRC_THR;
+                    s.a = (uint8_t)thrpos(o.dtile);
+                } else {
+                    s.src = SRC_COS;
+                    s.a = (uint8_t)o.dphys;
+                }
+                s.idx = (uint16_t)mats.size();
+                mats.push_back(o.m[0]);
+                mats.push_back(o.m[1]);
+                break;
+            default:
+                return "internal: unexpected op in a register stage";
+            }
+            if (s.kind) ops.push_back(s);
+            done[i] = 1;
+            scheduled++;
+        }
+        dr_flush();
+    }
+    if ((int)ops.size() > KATE_MAX_SOPS || (int)mats.size() > KATE_MAX_MATS)
+        return "pass program too large for the kernel parameter";
+    out->nops = (int)ops.size();
+    out->nmats = (int)mats.size();
+    for (size_t i = 0; i < ops.size(); i++) out->ops[i] = ops[i];
+    for (size_t i = 0; i < mats.size(); i++) {
+        out->mats[i][0] = mats[i].re;
+        out->mats[i][1] = mats[i].im;
+    }
+    return "";
+}
+
+}  // namespace kate

@@ -27,6 +27,18 @@ def _deposit(vals: np.ndarray, positions) -> np.ndarray:
     return out
 
 
+SOP_DTYPE = np.dtype([("kind", "u1"), ("a", "u1"), ("src", "u1"), ("creg", "u1"), ("cthr", "u1"), ("pad", "u1"),
+                      ("idx", "<u2"), ("ccos", "<u8")])
+PROG_DTYPE = np.dtype([("m", "<i4"), ("ncb", "<i4"), ("nops", "<i4"), ("nmats", "<i4"), ("tphys", "u1", 16),
+                       ("outsrc", "u1", 16), ("cphys", "u1", 48), ("ops", SOP_DTYPE, 160), ("mats", "<f8", (640, 2)),
+                       ("stab", "<u2", (40, 36)), ("srb", "u1", (40, 4)), ("stb", "u1", (40, 8)),
+                       ("nstages", "<i4"), ("sop0", "<i4")])
+
+
+def _swz(i):
+    return i ^ (((i >> 3) ^ (i >> 6) ^ (i >> 9)) & 7)
+
+
 class PlanView:
     def __init__(self, circuit, max_tile=12, coalesce=4, flags=0):
         L = _lib.lib()
@@ -71,10 +83,144 @@ class PlanView:
         self.final_phys = [int(x) for x in phys]
         self.label_to_logical = [int(x) for x in l2l]
 
+        # register-staged programs
+        self.smem_ops = []
+        L.kate_plan_num_smem_ops(h, ctypes.byref(v))
+        for i in range(v.value):
+            self.smem_ops.append(self._read_op(L.kate_plan_get_smem_op, i))
+        self.programs = []
+        for i in range(len(self.passes)):
+            size, has = ctypes.c_size_t(), ctypes.c_int()
+            L.kate_plan_get_program(h, i, None, 0, ctypes.byref(size), ctypes.byref(has))
+            if not has.value:
+                self.programs.append(None)
+                continue
+            buf = np.zeros(size.value, dtype=np.uint8)
+            L.kate_plan_get_program(h, i, buf.ctypes.data_as(ctypes.c_void_p), size.value, ctypes.byref(size),
+                                    ctypes.byref(has))
+            self.programs.append(buf.view(PROG_DTYPE)[0])
+
+    def _read_op(self, fn, i):
+        ints = np.zeros(18, dtype=np.int32)
+        pm = ctypes.c_uint64()
+        vals = np.zeros(2 + 2 * 1024, dtype=np.float64)
+        fn(self.h, i, ints.ctypes.data_as(_ip), ctypes.byref(pm), vals.ctypes.data_as(_dp))
+        kind, k = int(ints[0]), int(ints[1])
+        op = dict(kind=kind, k=k, tb=[int(x) for x in ints[2:7]], ftb=[int(x) for x in ints[7:12]],
+                  fpos=[int(x) for x in ints[12:17]], tmask=int(ints[17]) & 0xFFFFFFFF, pmask=pm.value,
+                  phase=complex(vals[0], vals[1]))
+        if kind == 0:
+            d = 1 << k
+            op["mat"] = vals[2:2 + 2 * d * d].view(np.complex128).reshape(d, d).copy()
+        elif kind == 4:
+            op["tab"] = vals[2:2 + 2 * (1 << k)].view(np.complex128).copy()
+        return op
+
     def __del__(self):
         if getattr(self, "h", None) is not None and self.h.value:
             self.L.kate_plan_destroy(self.h)
             self.h = None
+
+    def run_staged(self, state: np.ndarray) -> np.ndarray:
+        """Executes passes that have a register-staged program with the tile
+        kernel's semantics (256 threads x 16 registers), the others with the
+        generic semantics."""
+        n = self.n
+        st = state.astype(np.complex128).copy()
+        t = np.arange(256, dtype=np.int64)
+        jj = np.arange(16, dtype=np.int64)
+        for p, prog in zip(self.passes, self.programs):
+            m = p["m"]
+            T = 1 << m
+            tphys = p["tphys"]
+            cphys = [b for b in range(n) if b not in tphys]
+            toff = _deposit(np.arange(T, dtype=np.int64), tphys)
+            bases = _deposit(np.arange(1 << (n - m), dtype=np.int64), cphys)
+            idx = bases[:, None] + toff[None, :]
+            tile = st[idx]
+            if prog is None:
+                for op in self.ops[p["op0"]:p["op0"] + p["nops"]]:
+                    self._apply(tile, bases, m, op)
+            else:
+                assert int(prog["m"]) == 12
+                mats = prog["mats"][:, 0] + 1j * prog["mats"][:, 1]
+                a = None
+                ridx = None
+                for k in range(int(prog["nops"])):
+                    op = prog["ops"][k]
+                    kind = int(op["kind"])
+                    if kind == 1:  # STAGE
+                        if a is not None:
+                            tile[:, ridx] = a
+                        si = int(op["idx"])
+                        ridx = _deposit(t, prog["stb"][si])[:, None] | _deposit(jj, prog["srb"][si])[None, :]
+                        # the kernel addresses registers through the precomputed swizzled tables
+                        tab = prog["stab"][si].astype(np.int64)
+                        s0 = tab[t & 15] ^ tab[16 + (t >> 4)]
+                        w = np.zeros(16, dtype=np.int64)
+                        for i in range(4):
+                            w ^= np.where((jj >> i) & 1 == 1, tab[32 + i], 0)
+                        assert np.array_equal(_swz((s0[:, None] ^ w[None, :]) >> 4), ridx)
+                        a = tile[:, ridx].copy()
+                    elif kind == 2:  # SMEM
+                        if a is not None:
+                            tile[:, ridx] = a
+                            a = None
+                        self._apply(tile, bases, m, self.smem_ops[int(prog["sop0"]) + int(op["idx"])])
+                    else:
+                        cthr = int(op["cthr"])
+                        ccos = int(op["ccos"])
+                        creg = int(op["creg"])
+                        cond = (((t & cthr) == cthr)[None, :]) & (((bases & ccos) == ccos)[:, None])
+                        B = int(op["a"])
+                        if kind == 10:  # DR: diagonal over the register bits
+                            a *= mats[int(op["idx"]):int(op["idx"]) + 16][None, None, :]
+                            continue
+                        if kind in (8, 9):  # real / RX-form 2x2: same arithmetic as U here
+                            kind = 3
+                        if kind in (3, 4, 5):
+                            lo = jj[((jj >> B) & 1) == 0]
+                            if kind == 5:
+                                lo = lo[(lo & creg) == creg]
+                            hi = lo | (1 << B)
+                            x, y = a[:, :, lo].copy(), a[:, :, hi].copy()
+                            if kind == 3:
+                                u = mats[int(op["idx"]):int(op["idx"]) + 4]
+                                a[:, :, lo] = u[0] * x + u[1] * y
+                                a[:, :, hi] = u[2] * x + u[3] * y
+                            elif kind == 4:
+                                s2 = 1 / np.sqrt(2)
+                                a[:, :, lo] = (x + y) * s2
+                                a[:, :, hi] = (x - y) * s2
+                            else:
+                                c3 = cond[:, :, None]
+                                a[:, :, lo] = np.where(c3, y, x)
+                                a[:, :, hi] = np.where(c3, x, y)
+                        elif kind == 6:
+                            sel = jj[(jj & creg) == creg]
+                            ph = mats[int(op["idx"])]
+                            a[:, :, sel] = np.where(cond[:, :, None], a[:, :, sel] * ph, a[:, :, sel])
+                        elif kind == 7:
+                            d0, d1 = mats[int(op["idx"])], mats[int(op["idx"]) + 1]
+                            src = int(op["src"])
+                            if src == 0:
+                                a *= np.where(((jj >> B) & 1) == 1, d1, d0)[None, None, :]
+                            elif src == 1:
+                                a *= np.where(((t >> B) & 1) == 1, d1, d0)[None, :, None]
+                            else:
+                                a *= np.where(((bases >> B) & 1) == 1, d1, d0)[:, None, None]
+                        else:
+                            raise ValueError(kind)
+                if a is not None:
+                    tile[:, ridx] = a
+            o = np.arange(T, dtype=np.int64)
+            src = np.zeros(T, dtype=np.int64)
+            for b in range(m):
+                src |= ((o >> b) & 1) << p["outsrc"][b]
+            st[idx] = tile[:, src]
+        x = np.arange(1 << n, dtype=np.int64)
+        phys_of_label = [self.final_phys[self.label_to_logical[b]] for b in range(n)]
+        return st[_deposit(x, phys_of_label)]
 
     def run(self, state: np.ndarray) -> np.ndarray:
         n = self.n
