@@ -42,6 +42,8 @@ typedef struct {
 #define SOP_UR 8     // 2x2 with real entries on register bit a: mats[idx..idx+3].x (4 FP64 ops/amplitude)
 #define SOP_UX 9     // 2x2 [[a, ib], [ic, d]] (a, b, c, d real) on register bit a: 4 FP64 ops/amplitude
 #define SOP_DR 10    // diagonal over the register bits: multiply register j by mats[idx + j]
+#define SOP_XF 11    // fold a NOT into the stage's store: store offset ^= idx where controls cthr/ccos are 1
+#define SOP_XL 12    // fold a NOT into the next stage's load: load offset ^= idx where controls cthr/ccos are 1
 
 #define SRC_REG 0
 #define SRC_THR 1
@@ -70,11 +72,17 @@ typedef struct {
     uint8_t cphys[48];
     SOp ops[KATE_MAX_SOPS];
     double mats[KATE_MAX_MATS][2];
-    // Per stage (SOP_STAGE idx): byte offsets in the swizzled tile. The
-    // offset of thread t's register j is s0(t) ^ W(j) with
-    // s0(t) = stab[idx][t & 15] ^ stab[idx][16 + (t >> 4)] and W(j) the XOR
-    // of stab[idx][32 + i] over the set bits i of j.
-    uint16_t stab[KATE_MAX_STAGES][36];
+    // Per stage (SOP_STAGE idx): byte offsets in the swizzled tile, with
+    // s0(t) = stab[idx][t & 15] ^ stab[idx][16 + (t >> 4)] the thread's
+    // base and W_k(j) the XOR of stab[idx][32 + 4k + i] over the set bits i
+    // of register index j:
+    //   load  register j from  s0(t) ^ L(t) ^ W_0(j)   (L: SOP_XL flips)
+    //   store register j to    s0(t) ^ S(t) ^ W_1(j)   (S: SOP_XF flips)
+    //   natural layout          s0(t) ^ W_2(j)
+    // NOTs and CNOTs on register bits at the start (end) of a stage commute
+    // into an affine map of the register index that the load (store)
+    // addressing applies, so they move no data.
+    uint16_t stab[KATE_MAX_STAGES][44];
     // Per stage: tile bit of register-index bit i (rb) and of thread-index
     // bit i (tb), the layout the tables above encode.
     uint8_t srb[KATE_MAX_STAGES][4];

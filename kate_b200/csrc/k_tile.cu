@@ -160,7 +160,7 @@ struct TileTables {
     uint64_t cb[3][256];   // coset base = cb[0][c & 255] | cb[1][(c >> 8) & 255] | cb[2][c >> 16]
     uint64_t goff[16];     // global offset of tile element t + 256 j is dT(t) + goff[j]
     uint32_t osw[16];      // swizzled byte offset of the source of output element t + 256 j: pTs(t) ^ osw[j]
-    uint16_t stab[KATE_MAX_STAGES][36];
+    uint16_t stab[KATE_MAX_STAGES][44];
 };
 
 template <int NBUF>
@@ -201,7 +201,7 @@ __global__ void __launch_bounds__(NT, 3 - NBUF)
             T.goff[t] = g;
             T.osw[t] = ops::swz(o) << 4;
         }
-        for (int i = t; i < P.nstages * 36; i += NT) (&T.stab[0][0])[i] = (&P.stab[0][0])[i];
+        for (int i = t; i < P.nstages * 44; i += NT) (&T.stab[0][0])[i] = (&P.stab[0][0])[i];
         for (int i = t; i < P.nops; i += NT) T.ops[i] = P.ops[i];
         for (int i = t; i < P.nmats; i += NT) T.mats[i] = make_double2(P.mats[i][0], P.mats[i][1]);
     }
@@ -247,32 +247,46 @@ __global__ void __launch_bounds__(NT, 3 - NBUF)
 
         double2 a[16];
         bool open = false;
-        uint32_t s0 = 0, w0 = 0, w1 = 0, w2 = 0, w3 = 0;
+        uint32_t s0s = 0;   // store offset base of the open stage (flipped by SOP_XF)
+        uint32_t lflip = 0; // load offset flips for the next stage (SOP_XL)
+        int si = 0;         // open stage's table
+        // Stores the open stage's registers through its store basis.
+        auto store_regs = [&]() {
+            const uint16_t* tab = T.stab[si];
+            const uint32_t v0 = tab[36], v1 = tab[37], v2 = tab[38], v3 = tab[39];
+#pragma unroll
+            for (int j = 0; j < 16; j++) sts(tb + reg_off(j, s0s, v0, v1, v2, v3), a[j]);
+        };
         for (int k = 0; k < P.nops; k++) {
             const SOp op = T.ops[k];
             switch (op.kind) {
             case SOP_STAGE: {
-                if (open) {
-#pragma unroll
-                    for (int j = 0; j < 16; j++) sts(tb + reg_off(j, s0, w0, w1, w2, w3), a[j]);
-                }
+                if (open) store_regs();
                 __syncthreads();
-                const uint16_t* tab = T.stab[op.idx];
-                s0 = (uint32_t)tab[t & 15u] ^ (uint32_t)tab[16 + (t >> 4)];
-                w0 = tab[32];
-                w1 = tab[33];
-                w2 = tab[34];
-                w3 = tab[35];
+                si = op.idx;
+                const uint16_t* tab = T.stab[si];
+                const uint32_t s0 = (uint32_t)tab[t & 15u] ^ (uint32_t)tab[16 + (t >> 4)];
+                const uint32_t w0 = tab[32], w1 = tab[33], w2 = tab[34], w3 = tab[35];
+                const uint32_t sl = s0 ^ lflip;
 #pragma unroll
-                for (int j = 0; j < 16; j++) a[j] = lds(tb + reg_off(j, s0, w0, w1, w2, w3));
+                for (int j = 0; j < 16; j++) a[j] = lds(tb + reg_off(j, sl, w0, w1, w2, w3));
+                s0s = s0;
+                lflip = 0;
                 open = true;
+                break;
+            }
+            case SOP_XF: {
+                if ((t & op.cthr) == op.cthr && (op.ccos == 0 || (coset_base(c) & op.ccos) == op.ccos)) s0s ^= op.idx;
+                break;
+            }
+            case SOP_XL: {
+                if ((t & op.cthr) == op.cthr && (op.ccos == 0 || (coset_base(c) & op.ccos) == op.ccos)) lflip ^= op.idx;
                 break;
             }
             case SOP_SMEM: {
                 if (!SM) break;
                 if (open) {
-#pragma unroll
-                    for (int j = 0; j < 16; j++) sts(tb + reg_off(j, s0, w0, w1, w2, w3), a[j]);
+                    store_regs();
                     open = false;
                 }
                 // The registers are dead until the next stage loads them.
@@ -372,10 +386,7 @@ __global__ void __launch_bounds__(NT, 3 - NBUF)
                 break;
             }
         }
-        if (open) {
-#pragma unroll
-            for (int j = 0; j < 16; j++) sts(tb + reg_off(j, s0, w0, w1, w2, w3), a[j]);
-        }
+        if (open) store_regs();
         __syncthreads();
         double2* dst = st + coset_base(c) + dT;
 #pragma unroll

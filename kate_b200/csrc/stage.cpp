@@ -180,30 +180,150 @@ std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n,
             }
         for (int t : nonR)
             if (std::find(tb.begin(), tb.end(), t) == tb.end()) tb.push_back(t);
-        SOp st{};
-        st.kind = SOP_STAGE;
-        if (out->nstages >= KATE_MAX_STAGES) return "pass program has too many stages";
-        st.idx = (uint16_t)out->nstages;
-        for (int i = 0; i < 4; i++) out->srb[out->nstages][i] = (uint8_t)R[i];
-        for (int i = 0; i < 8; i++) out->stb[out->nstages][i] = (uint8_t)tb[i];
-        {
-            auto swz = [](uint32_t i) { return i ^ (((i >> 3) ^ (i >> 6) ^ (i >> 9)) & 7u); };
-            uint16_t* tab = out->stab[out->nstages];
-            for (int v = 0; v < 16; v++) {
-                uint32_t lo = 0, hi = 0;
-                for (int i = 0; i < 4; i++) {
-                    if ((v >> i) & 1) lo |= 1u << tb[i];
-                    if ((v >> i) & 1) hi |= 1u << tb[4 + i];
-                }
-                tab[v] = (uint16_t)(swz(lo) << 4);
-                tab[16 + v] = (uint16_t)(swz(hi) << 4);
-            }
-            for (int i = 0; i < 4; i++) tab[32 + i] = (uint16_t)(swz(1u << R[i]) << 4);
-        }
-        out->nstages++;
-        ops.push_back(st);
         auto regpos = [&](int t) { return (int)(std::find(R.begin(), R.end(), t) - R.begin()); };
         auto thrpos = [&](int t) { return (int)(std::find(tb.begin(), tb.end(), t) - tb.begin()); };
+        auto in_R = [&](int t) { return std::find(R.begin(), R.end(), t) != R.end(); };
+        if (out->nstages >= KATE_MAX_STAGES) return "pass program has too many stages";
+        const int si = out->nstages++;
+        for (int i = 0; i < 4; i++) out->srb[si][i] = (uint8_t)R[i];
+        for (int i = 0; i < 8; i++) out->stb[si][i] = (uint8_t)tb[i];
+        uint16_t* stab = out->stab[si];
+        auto swz = [](uint32_t i) { return i ^ (((i >> 3) ^ (i >> 6) ^ (i >> 9)) & 7u); };
+        for (int v = 0; v < 16; v++) {
+            uint32_t lo = 0, hi = 0;
+            for (int i = 0; i < 4; i++) {
+                if ((v >> i) & 1) lo |= 1u << tb[i];
+                if ((v >> i) & 1) hi |= 1u << tb[4 + i];
+            }
+            stab[v] = (uint16_t)(swz(lo) << 4);
+            stab[16 + v] = (uint16_t)(swz(hi) << 4);
+        }
+        uint32_t wnat[4];
+        for (int i = 0; i < 4; i++) wnat[i] = swz(1u << R[i]) << 4;
+        auto W = [&](uint32_t x) {
+            uint32_t r = 0;
+            for (int k = 0; k < 4; k++)
+                if ((x >> k) & 1u) r ^= wnat[k];
+            return r;
+        };
+
+        // NOTs/CNOTs folded into addressing. An X is foldable when its
+        // controls are either one register bit or only thread/coset bits.
+        // It joins the load prefix when it commutes with every op kept in the
+        // stage before it, and the store suffix when it commutes with every
+        // kept op after it. Ops commute when neither's target is a qubit the
+        // other touches (controls and diagonals only read the Z basis).
+        auto touched = [&](const LOp& o) {
+            uint32_t m2 = o.tctl;
+            if (o.tgt >= 0) m2 |= 1u << o.tgt;
+            if (o.dtile >= 0) m2 |= 1u << o.dtile;
+            return m2;
+        };
+        auto commute = [&](const LOp& a, const LOp& b) {
+            return (a.tgt < 0 || !((touched(b) >> a.tgt) & 1u)) && (b.tgt < 0 || !((touched(a) >> b.tgt) & 1u));
+        };
+        auto reg_ctl = [&](const LOp& o) {
+            return o.pctl == 0 && __builtin_popcount(o.tctl) == 1 && in_R(__builtin_ctz(o.tctl));
+        };
+        auto lane_ctl = [&](const LOp& o) {
+            for (int t = 0; t < m; t++)
+                if (((o.tctl >> t) & 1u) && in_R(t)) return false;
+            return true;  // includes the uncontrolled NOT
+        };
+        auto foldable = [&](const LOp& o) { return o.kind == SOP_X && (reg_ctl(o) || lane_ctl(o)); };
+        std::vector<int> prefix, kept;
+        for (int i : list) {
+            bool ok = foldable(L[i]);
+            for (int k : kept)
+                if (ok && !commute(L[k], L[i])) ok = false;
+            (ok ? prefix : kept).push_back(i);
+        }
+        std::vector<int> suffix;
+        for (int ki = (int)kept.size() - 1; ki >= 0; ki--) {
+            const int i = kept[ki];
+            bool ok = foldable(L[i]);
+            for (size_t k2 = ki + 1; k2 < kept.size() && ok; k2++)
+                if (std::find(suffix.begin(), suffix.end(), kept[k2]) == suffix.end() &&
+                    !commute(L[i], L[kept[k2]]))
+                    ok = false;
+            if (ok) suffix.insert(suffix.begin(), i);
+        }
+        std::vector<int> body;
+        for (int i : kept)
+            if (std::find(suffix.begin(), suffix.end(), i) == suffix.end()) body.push_back(i);
+
+        // Affine map x -> M x ^ sum_k g_k u_k of a folded X sequence on the
+        // 4-bit register index: register CNOTs update M (and the lane vectors
+        // already accumulated), lane NOTs add u = e_B with their condition g.
+        struct Lane {
+            uint32_t u;
+            uint8_t cthr;
+            uint64_t ccos;
+        };
+        auto compose = [&](const std::vector<int>& seq, uint32_t col[4], std::vector<Lane>& lanes) {
+            for (int i = 0; i < 4; i++) col[i] = 1u << i;
+            for (int i : seq) {
+                const LOp& o = L[i];
+                const int B = regpos(o.tgt);
+                if (reg_ctl(o)) {
+                    const int C = regpos(__builtin_ctz(o.tctl));
+                    for (int k = 0; k < 4; k++) col[k] ^= ((col[k] >> C) & 1u) << B;
+                    for (auto& ln : lanes) ln.u ^= ((ln.u >> C) & 1u) << B;
+                } else {
+                    Lane ln{1u << B, 0, o.pctl};
+                    for (int t = 0; t < m; t++)
+                        if ((o.tctl >> t) & 1u) ln.cthr |= (uint8_t)(1u << thrpos(t));
+                    lanes.push_back(ln);
+                }
+            }
+        };
+        auto apply = [](const uint32_t col[4], uint32_t x) {
+            uint32_t r = 0;
+            for (int k = 0; k < 4; k++)
+                if ((x >> k) & 1u) r ^= col[k];
+            return r;
+        };
+        // Load fold: register j must receive the amplitude at pi^-1(j).
+        uint32_t pcol[4];
+        std::vector<Lane> plane;
+        compose(prefix, pcol, plane);
+        uint32_t inv[16];
+        for (uint32_t x = 0; x < 16; x++) inv[apply(pcol, x)] = x;
+        std::vector<SOp> xl;
+        for (auto& ln : plane) {
+            SOp f{};
+            f.kind = SOP_XL;
+            f.cthr = ln.cthr;
+            f.ccos = ln.ccos;
+            f.idx = (uint16_t)W(inv[ln.u]);
+            xl.push_back(f);
+        }
+        for (int i = 0; i < 4; i++) stab[32 + i] = (uint16_t)W(inv[1u << i]);
+        // Store fold: register j (natural index j) goes to pi(j).
+        uint32_t scol[4];
+        std::vector<Lane> slane;
+        compose(suffix, scol, slane);
+        std::vector<SOp> folds;
+        for (auto& ln : slane) {
+            SOp f{};
+            f.kind = SOP_XF;
+            f.cthr = ln.cthr;
+            f.ccos = ln.ccos;
+            f.idx = (uint16_t)W(ln.u);
+            folds.push_back(f);
+        }
+        for (int i = 0; i < 4; i++) stab[36 + i] = (uint16_t)W(scol[i]);
+        for (int i = 0; i < 4; i++) stab[40 + i] = (uint16_t)wnat[i];
+
+        ops.insert(ops.end(), xl.begin(), xl.end());
+        SOp st{};
+        st.kind = SOP_STAGE;
+        st.idx = (uint16_t)si;
+        ops.push_back(st);
+        for (int i : prefix) done[i] = 1;
+        for (int i : suffix) done[i] = 1;
+        scheduled += (int)(prefix.size() + suffix.size());
+        list = body;
         auto ctl = [&](const LOp& o, SOp& s) {
             for (int t = 0; t < m; t++)
                 if ((o.tctl >> t) & 1u) {
@@ -293,6 +413,7 @@ std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n,
             scheduled++;
         }
         dr_flush();
+        ops.insert(ops.end(), folds.begin(), folds.end());
     }
     if ((int)ops.size() > KATE_MAX_SOPS || (int)mats.size() > KATE_MAX_MATS)
         return "pass program too large for the kernel parameter";

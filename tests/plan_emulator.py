@@ -31,7 +31,7 @@ SOP_DTYPE = np.dtype([("kind", "u1"), ("a", "u1"), ("src", "u1"), ("creg", "u1")
                       ("idx", "<u2"), ("ccos", "<u8")])
 PROG_DTYPE = np.dtype([("m", "<i4"), ("ncb", "<i4"), ("nops", "<i4"), ("nmats", "<i4"), ("tphys", "u1", 16),
                        ("outsrc", "u1", 16), ("cphys", "u1", 48), ("ops", SOP_DTYPE, 160), ("mats", "<f8", (640, 2)),
-                       ("stab", "<u2", (40, 36)), ("srb", "u1", (40, 4)), ("stb", "u1", (40, 8)),
+                       ("stab", "<u2", (40, 44)), ("srb", "u1", (40, 4)), ("stb", "u1", (40, 8)),
                        ("nstages", "<i4"), ("sop0", "<i4")])
 
 
@@ -145,26 +145,52 @@ class PlanView:
                 assert int(prog["m"]) == 12
                 mats = prog["mats"][:, 0] + 1j * prog["mats"][:, 1]
                 a = None
-                ridx = None
+                sidx = None   # (C, 256, 16) store indices of the open stage
+                lflip = np.zeros((tile.shape[0], 256), dtype=np.int64)
+
+                def store():
+                    rows = np.arange(tile.shape[0])[:, None, None]
+                    tile[rows, sidx] = a
+
                 for k in range(int(prog["nops"])):
                     op = prog["ops"][k]
                     kind = int(op["kind"])
+                    if kind == 12:  # XL: flip the next stage's load offset
+                        cthr, ccos = int(op["cthr"]), int(op["ccos"])
+                        cond = (((t & cthr) == cthr)[None, :]) & (((bases & ccos) == ccos)[:, None])
+                        lflip = np.where(cond, lflip ^ int(op["idx"]), lflip)
+                        continue
                     if kind == 1:  # STAGE
                         if a is not None:
-                            tile[:, ridx] = a
+                            store()
                         si = int(op["idx"])
-                        ridx = _deposit(t, prog["stb"][si])[:, None] | _deposit(jj, prog["srb"][si])[None, :]
-                        # the kernel addresses registers through the precomputed swizzled tables
+                        nidx = _deposit(t, prog["stb"][si])[:, None] | _deposit(jj, prog["srb"][si])[None, :]
                         tab = prog["stab"][si].astype(np.int64)
                         s0 = tab[t & 15] ^ tab[16 + (t >> 4)]
-                        w = np.zeros(16, dtype=np.int64)
+                        wl = np.zeros(16, dtype=np.int64)
+                        ws = np.zeros(16, dtype=np.int64)
+                        wn = np.zeros(16, dtype=np.int64)
                         for i in range(4):
-                            w ^= np.where((jj >> i) & 1 == 1, tab[32 + i], 0)
-                        assert np.array_equal(_swz((s0[:, None] ^ w[None, :]) >> 4), ridx)
-                        a = tile[:, ridx].copy()
+                            bit = ((jj >> i) & 1) == 1
+                            wl ^= np.where(bit, tab[32 + i], 0)
+                            ws ^= np.where(bit, tab[36 + i], 0)
+                            wn ^= np.where(bit, tab[40 + i], 0)
+                        # the natural-layout table agrees with the stage's layout
+                        assert np.array_equal(_swz((s0[:, None] ^ wn[None, :]) >> 4), nidx)
+                        lidx = _swz(((s0[None, :] ^ lflip)[:, :, None] ^ wl[None, None, :]) >> 4)
+                        rows = np.arange(tile.shape[0])[:, None, None]
+                        a = tile[rows, lidx].copy()
+                        lflip = np.zeros((tile.shape[0], 256), dtype=np.int64)
+                        s0s = np.broadcast_to(s0[None, :], (tile.shape[0], 256)).copy()
+                        sidx = _swz((s0s[:, :, None] ^ ws[None, None, :]) >> 4)
+                    elif kind == 11:  # XF: flip the store offset
+                        cthr, ccos = int(op["cthr"]), int(op["ccos"])
+                        cond = (((t & cthr) == cthr)[None, :]) & (((bases & ccos) == ccos)[:, None])
+                        s0s = np.where(cond, s0s ^ int(op["idx"]), s0s)
+                        sidx = _swz((s0s[:, :, None] ^ ws[None, None, :]) >> 4)
                     elif kind == 2:  # SMEM
                         if a is not None:
-                            tile[:, ridx] = a
+                            store()
                             a = None
                         self._apply(tile, bases, m, self.smem_ops[int(prog["sop0"]) + int(op["idx"])])
                     else:
@@ -212,7 +238,7 @@ class PlanView:
                         else:
                             raise ValueError(kind)
                 if a is not None:
-                    tile[:, ridx] = a
+                    store()
             o = np.arange(T, dtype=np.int64)
             src = np.zeros(T, dtype=np.int64)
             for b in range(m):
