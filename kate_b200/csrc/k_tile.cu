@@ -158,7 +158,10 @@ struct TileTables {
     SOp ops[KATE_MAX_SOPS];        // the pass program, copied from the kernel parameter
     double2 mats[KATE_MAX_MATS];
     uint64_t cb[3][256];   // coset base = cb[0][c & 255] | cb[1][(c >> 8) & 255] | cb[2][c >> 16]
-    uint64_t goff[16];     // global offset of tile element t + 256 j is dT(t) + goff[j]
+    uint64_t goff[16];     // global offset of tile element t + 256 j is dT[t] + goff[j]
+    uint64_t dT[NT];       // per-thread constants, kept here rather than in registers
+    uint32_t tls[NT];      // swizzled byte offset of tile element t
+    uint32_t pTs[NT];      // swizzled byte offset of the source of output element t
     uint32_t osw[16];      // swizzled byte offset of the source of output element t + 256 j: pTs(t) ^ osw[j]
     uint16_t stab[KATE_MAX_STAGES][44];
 };
@@ -205,20 +208,24 @@ __global__ void __launch_bounds__(NT, 3 - NBUF)
         for (int i = t; i < P.nops; i += NT) T.ops[i] = P.ops[i];
         for (int i = t; i < P.nmats; i += NT) T.mats[i] = make_double2(P.mats[i][0], P.mats[i][1]);
     }
-    uint64_t dT = 0;
-#pragma unroll
-    for (int i = 0; i < 8; i++) dT |= (uint64_t)((t >> i) & 1u) << P.tphys[i];
-    uint32_t pT = 0;
-#pragma unroll
-    for (int i = 0; i < 8; i++) pT |= ((t >> i) & 1u) << P.outsrc[i];
-    const uint32_t pTs = ops::swz(pT) << 4;
-    const uint32_t tls = ops::swz(t) << 4;
+    {
+        uint64_t dT = 0;
+        uint32_t pT = 0;
+        for (int i = 0; i < 8; i++) {
+            dT |= (uint64_t)((t >> i) & 1u) << P.tphys[i];
+            pT |= ((t >> i) & 1u) << P.outsrc[i];
+        }
+        T.dT[t] = dT;
+        T.pTs[t] = ops::swz(pT) << 4;
+        T.tls[t] = ops::swz(t) << 4;
+    }
     const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(bufs);
     __syncthreads();
     const uint32_t ncos = 1u << P.ncb;
     auto coset_base = [&](uint32_t c) { return T.cb[0][c & 255u] | T.cb[1][(c >> 8) & 255u] | T.cb[2][c >> 16]; };
     auto load = [&](uint32_t c, uint32_t buf) {
-        const double2* src = st + coset_base(c) + dT;
+        const double2* src = st + (coset_base(c) + T.dT[t]);
+        const uint32_t tls = T.tls[t];
 #pragma unroll
         for (int j = 0; j < 16; j++) {
             const uint32_t d = buf + (tls ^ (swz_hi(j) << 4));
@@ -388,9 +395,16 @@ __global__ void __launch_bounds__(NT, 3 - NBUF)
         }
         if (open) store_regs();
         __syncthreads();
-        double2* dst = st + coset_base(c) + dT;
+        double2* dst = st + (coset_base(c) + T.dT[t]);
+        const uint32_t pTs = T.pTs[t];
+        // Four at a time: bounds the registers in flight (the op loop's
+        // amplitudes are dead here, but the allocator sizes for the peak).
 #pragma unroll
-        for (int j = 0; j < 16; j++) dst[T.goff[j]] = lds(tb + (pTs ^ T.osw[j]));
+        for (int j0 = 0; j0 < 16; j0 += 4) {
+#pragma unroll
+            for (int j = j0; j < j0 + 4; j++) dst[T.goff[j]] = lds(tb + (pTs ^ T.osw[j]));
+            asm volatile("" ::: "memory");
+        }
         // The buffer is refilled by the next load.
         __syncthreads();
     }

@@ -47,7 +47,7 @@ struct SimImpl {
     bool has_state = false;
     int grid = 0;
     int tile_grid = 0;
-    int nbuf = 2;  // tile kernel buffering (1 or 2), see launch_tile_c128
+    int nbuf = 1;  // tile kernel buffering (1: two CTAs per SM, 2: one CTA, prefetching)
 
     // Launches pass i of the plan on stream st.
     cudaError_t launch_pass(size_t i, cudaStream_t st) {
@@ -166,7 +166,7 @@ std::string Simulator::create(const Program& prog_in, int precision, int device,
     ce = cudaMalloc(&impl->d_state, impl->dim() * impl->amp_bytes());
     if (ce != cudaSuccess) return fail(cuda_err("cudaMalloc(state)", ce));
     impl->grid = generic_pass_grid(impl->n, std::min(impl->opt.max_tile, impl->n), device);
-    if (const char* e = std::getenv("KATE_TILE_NBUF")) impl->nbuf = std::atoi(e) == 1 ? 1 : 2;
+    if (const char* e = std::getenv("KATE_TILE_NBUF")) impl->nbuf = std::atoi(e) == 2 ? 2 : 1;
     if (impl->n >= KATE_TILE_BITS) impl->tile_grid = tile_pass_grid(impl->n, device, impl->nbuf);
     impl->phys.resize(impl->n);
     std::iota(impl->phys.begin(), impl->phys.end(), 0);
