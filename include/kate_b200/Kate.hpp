@@ -1,0 +1,235 @@
+// Kate.hpp - C++ facade of kate_b200 with the reference's class and method
+// names (Line-fr/Kate: Kate.hpp, backendagnosticcode/basic_host_types.hpp,
+// QuantumCircuit.hpp, Circuit.hpp, HIPcode/simulator.hpp), so that code
+// written against `#include "Kate.hpp"` compiles against this library
+// instead: replace the include with `#include <kate_b200/Kate.hpp>` and link
+// with -lkate_b200. Header-only; every call goes through the C ABI of
+// kate_b200.h.
+//
+// Like the reference, failures are printed to std::cout and execution
+// continues; Kate::last_status() returns the status of the last call.
+#ifndef KATE_B200_KATE_HPP
+#define KATE_B200_KATE_HPP
+
+#include <cmath>
+#include <iostream>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../kate_b200.h"
+
+#ifndef Hadamard
+#define Hadamard 2
+#define CNOT 3
+#define CRk 4
+#define TOFFOLI 5
+#define RX 6
+#define RZ 7
+#endif
+
+namespace Kate {
+
+inline kate_status& last_status() {
+    static thread_local kate_status s = KATE_OK;
+    return s;
+}
+
+inline bool check(kate_status s) {
+    last_status() = s;
+    if (s != KATE_OK) std::cout << "kate_b200: " << kate_last_error() << std::endl;
+    return s == KATE_OK;
+}
+
+class Complex {
+public:
+    double a = 0, b = 0;
+    Complex() = default;
+    Complex(double a_) : a(a_), b(0) {}
+    Complex(double a_, double b_) : a(a_), b(b_) {}
+    Complex operator+(Complex o) const { return Complex(a + o.a, b + o.b); }
+    Complex operator-(Complex o) const { return Complex(a - o.a, b - o.b); }
+    Complex operator*(Complex o) const { return Complex(a * o.a - b * o.b, a * o.b + b * o.a); }
+    Complex operator*(double d) const { return Complex(a * d, b * d); }
+    double norm() const { return std::sqrt(a * a + b * b); }
+    void print() const { std::cout << a << " + " << b << "i"; }
+};
+
+// Square row-major matrix (basic_host_types.hpp:86-186).
+template <typename T>
+class Matrix {
+public:
+    int n = 0;
+    std::vector<T> storage;
+    T* data = nullptr;
+    Matrix() = default;
+    explicit Matrix(int n_) : n(n_), storage((size_t)n_ * n_), data(storage.data()) {}
+    Matrix(const Matrix& o) : n(o.n), storage(o.storage), data(storage.data()) {}
+    Matrix& operator=(const Matrix& o) {
+        n = o.n;
+        storage = o.storage;
+        data = storage.data();
+        return *this;
+    }
+    T operator()(int r, int c) const { return data[(size_t)r * n + c]; }
+    void operator()(int r, int c, T v) { data[(size_t)r * n + c] = v; }
+    void fill(T v) {
+        for (auto& x : storage) x = v;
+    }
+};
+
+// Gate (basic_host_types.hpp:190-296).
+class Gate {
+public:
+    int identifier = -1;
+    int optarg = 0;
+    std::vector<int> qbits;
+    Matrix<Complex> densecontent;
+    Gate(int id, std::vector<int>& q, int opt = 0) : identifier(id), optarg(opt), qbits(q) {}
+    Gate(Matrix<Complex>& m, std::vector<int>& q) : identifier(0), qbits(q), densecontent(m) {}
+    void print() const {
+        std::cout << "Identifier : " << identifier << ", Qbits affected : ";
+        for (int q : qbits) std::cout << q << " ";
+        std::cout << std::endl;
+    }
+};
+
+// proba_state (basic_host_types.hpp:319-336).
+class proba_state {
+public:
+    std::vector<std::pair<double, double>> val;
+    explicit proba_state(int n) : val(n, {0.0, 0.0}) {}
+    explicit proba_state(std::vector<std::pair<double, double>>& v) : val(v) {}
+    void print() const {
+        for (size_t i = 0; i < val.size(); i++)
+            std::cout << "Qbit " << i << " : teta=" << val[i].first << " , phi=" << val[i].second << std::endl;
+    }
+};
+
+// Circuit (QuantumCircuit.hpp + Circuit.hpp).
+class Circuit {
+public:
+    int nqbits = 0;
+    explicit Circuit(int n) : nqbits(n) { check(kate_circuit_create(n, &h_)); }
+    Circuit(const Circuit& o) : nqbits(o.nqbits) { check(kate_circuit_clone(o.h_, &h_)); }
+    Circuit& operator=(const Circuit& o) {
+        if (this != &o) {
+            kate_circuit_destroy(h_);
+            nqbits = o.nqbits;
+            check(kate_circuit_clone(o.h_, &h_));
+        }
+        return *this;
+    }
+    ~Circuit() { kate_circuit_destroy(h_); }
+
+    void appendGate(const Gate& g) {
+        if (g.identifier == 0) {
+            std::vector<double> m(2 * g.densecontent.storage.size());
+            for (size_t i = 0; i < g.densecontent.storage.size(); i++) {
+                m[2 * i] = g.densecontent.storage[i].a;
+                m[2 * i + 1] = g.densecontent.storage[i].b;
+            }
+            check(kate_circuit_append_dense(h_, m.data(), g.qbits.data(), (int)g.qbits.size()));
+        } else {
+            check(kate_circuit_append_gate(h_, g.identifier, g.qbits.data(), (int)g.qbits.size(), g.optarg));
+        }
+    }
+    void gateScheduling() { check(kate_circuit_schedule(h_)); }
+    void gateFusion(int qbitsizelimit = 5, double merge_time_matters = 0.000001) {
+        check(kate_circuit_fuse(h_, qbitsizelimit, merge_time_matters));
+    }
+    void gateGrouping(int qbitgroupsize = 8) { check(kate_circuit_group(h_, qbitgroupsize)); }
+    void allocate(int numberofgpulog2 = 0, int maxlocalqbitnumber = 300) {
+        check(kate_circuit_allocate(h_, numberofgpulog2, maxlocalqbitnumber));
+    }
+    void compileDefault(int numberofgpulog2 = 0, int maxlocalqbitnumber = 300) {
+        check(kate_circuit_compile_default(h_, numberofgpulog2, maxlocalqbitnumber));
+    }
+    void compileOPT(int k = 5, double mtm = 0.000001, int groupsize = 10, int numberofgpulog2 = 0,
+                    int maxlocalqbitnumber = 300) {
+        check(kate_circuit_compile_opt(h_, k, mtm, groupsize, numberofgpulog2, maxlocalqbitnumber));
+    }
+    void exportqcx(const std::string& filename) { check(kate_circuit_export_qcx(h_, filename.c_str())); }
+    int gateCount() const {
+        int n = 0;
+        kate_circuit_num_gates(h_, &n);
+        return n;
+    }
+    const kate_circuit* handle() const { return h_; }
+
+private:
+    kate_circuit* h_ = nullptr;
+};
+using QuantumCircuit = Circuit;
+
+// mergeGate / CPUmergeGate (CPUcode/GateMerger.hpp:8-55).
+inline Gate mergeGate(std::vector<Gate> gates) {
+    int n = 0;
+    for (auto& g : gates)
+        for (int q : g.qbits) n = q + 1 > n ? q + 1 : n;
+    Circuit c(n);
+    for (auto& g : gates) c.appendGate(g);
+    std::vector<int> q(64);
+    int k = 0;
+    std::vector<double> m(2 * 1024 * 1024);
+    check(kate_merge_gates(c.handle(), 0, (int)gates.size(), q.data(), &k, m.data()));
+    q.resize(k);
+    Matrix<Complex> mat(1 << k);
+    for (size_t i = 0; i < mat.storage.size(); i++) mat.storage[i] = Complex(m[2 * i], m[2 * i + 1]);
+    return Gate(mat, q);
+}
+
+// Simulator (HIPcode/simulator.hpp:220-811) on one B200. number_of_gpu and
+// swapBufferSizeLog2 are accepted for source compatibility; one GPU is used.
+class Simulator {
+public:
+    Simulator(const Circuit& c, int number_of_gpu = 1, int swapBufferSizeLog2 = 24,
+              kate_precision precision = KATE_C128, int device = 0)
+        : n_(c.nqbits) {
+        (void)number_of_gpu;
+        (void)swapBufferSizeLog2;
+        check(kate_sim_create(c.handle(), precision, device, &s_));
+    }
+    Simulator(const Simulator&) = delete;
+    Simulator& operator=(const Simulator&) = delete;
+    ~Simulator() { kate_sim_destroy(s_); }
+
+    proba_state execute(bool displaytime = false) {
+        (void)displaytime;
+        std::vector<double> tp(2 * n_);
+        check(kate_sim_execute(s_, tp.data()));
+        return to_proba(tp);
+    }
+    proba_state execute(proba_state& in, bool displaytime = false) {
+        (void)displaytime;
+        std::vector<double> tin(2 * n_), tp(2 * n_);
+        for (int i = 0; i < n_ && i < (int)in.val.size(); i++) {
+            tin[2 * i] = in.val[i].first;
+            tin[2 * i + 1] = in.val[i].second;
+        }
+        check(kate_sim_execute_from(s_, tin.data(), tp.data()));
+        return to_proba(tp);
+    }
+    // The state in the reference's amplitude order.
+    std::vector<Complex> state() {
+        std::vector<double> d(2 * ((size_t)1 << n_));
+        check(kate_sim_get_state(s_, d.data()));
+        std::vector<Complex> r((size_t)1 << n_);
+        for (size_t i = 0; i < r.size(); i++) r[i] = Complex(d[2 * i], d[2 * i + 1]);
+        return r;
+    }
+    kate_sim* handle() { return s_; }
+
+private:
+    proba_state to_proba(const std::vector<double>& tp) {
+        std::vector<std::pair<double, double>> v(n_);
+        for (int i = 0; i < n_; i++) v[i] = {tp[2 * i], tp[2 * i + 1]};
+        return proba_state(v);
+    }
+    int n_;
+    kate_sim* s_ = nullptr;
+};
+
+}  // namespace Kate
+
+#endif  // KATE_B200_KATE_HPP
