@@ -230,6 +230,37 @@ KATE_API kate_status kate_plan_get_smem_op(const kate_plan* p, int i, int* ints,
  * label_to_logical[x]: logical qubit held by program label x. */
 KATE_API kate_status kate_plan_final_layout(const kate_plan* p, int* phys, int* label_to_logical);
 
+/* ---- measurement without allocation ----
+ * No counterpart in the reference: Kate allocates device memory on every
+ * measurement (HIPcode/simulator.hpp:483-543 calls hipMalloc/hipFree).
+ *
+ * For callers that must not allocate device memory once running: a serving
+ * loop that reserved the GPU's memory for resident state vectors, a caller
+ * bound to a fixed budget or a memory pool it does not own, a host-language
+ * binding that cannot manage device buffer lifetimes. Computes the
+ * reference's per-qubit (theta, phi) of a state vector the caller already
+ * holds on the current device: d_state is 2^nqbits complex128 amplitudes;
+ * phys_of_label[x] (nullable: identity) is the bit of the amplitude index
+ * holding program label x (kate_sim_state_device reports it);
+ * final_inverse_permutation (nullable: identity) maps labels to output
+ * qubits as in kate_sim_proba_state; theta_phi receives 2*nqbits doubles.
+ * Queued on `stream` (cudaStream_t as void*, NULL = default stream) and
+ * waited for before returning.
+ *
+ * It calls no cudaMalloc/cudaFree and no allocating library routine: its
+ * scratch is one fixed __device__ array of KATE_NOALLOC_SCRATCH_BYTES bytes
+ * that every GPU loading the library holds until the process exits, so
+ * nqbits is limited to KATE_NOALLOC_MAX_QUBITS (larger sizes return
+ * KATE_EINVAL). The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) for that device; make that first call
+ * before any stream capture. The array is shared by all calls and keeps the
+ * last call's contents (each call writes every slot it reads); calls that
+ * overlap on the GPU race on it, so the caller must serialise them. */
+#define KATE_NOALLOC_MAX_QUBITS 30
+#define KATE_NOALLOC_SCRATCH_BYTES 672704
+KATE_API kate_status kate_proba_state_noalloc(const void* d_state, int nqbits, const int* phys_of_label,
+                                              const int* final_inverse_permutation, double* theta_phi, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -70,6 +70,7 @@ SIGNATURES = {
     "kate_plan_get_program": [_vp, _i, _vp, _c.c_size_t, _c.POINTER(_c.c_size_t), _ip],
     "kate_plan_num_smem_ops": [_vp, _ip],
     "kate_plan_get_smem_op": [_vp, _i, _ip, _u64p, _dp],
+    "kate_proba_state_noalloc": [_vp, _i, _ip, _ip, _dp, _vp],
 }
 _RET = {"kate_last_error": _c.c_char_p, "kate_version": _c.c_char_p}
 

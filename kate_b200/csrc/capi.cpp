@@ -60,6 +60,10 @@ kate_status guarded(F&& f) {
     if (!(cond)) return fail(KATE_EINVAL, msg)
 }  // namespace
 
+namespace kate {
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace kate
+
 extern "C" {
 
 const char* kate_last_error(void) { return g_last_error.c_str(); }

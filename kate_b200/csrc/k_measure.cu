@@ -168,6 +168,12 @@ cudaError_t launch_bitsums_c128(const void* st, int n, int kind, void* partials,
     return cudaGetLastError();
 }
 
+cudaError_t launch_bitsums_c128_shape(const void* st, int n, int g, int nr, void* partials, cudaStream_t s) {
+    if (nr < 0 || nr > MAXR || g < 0) return cudaErrorInvalidValue;
+    k_bitsums<double2><<<1 << g, NT, 0, s>>>((const double2*)st, n, g, nr, (double2*)partials);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_probs_c128(const void* st, uint64_t dim, double* out, cudaStream_t s) {
     uint64_t blocks = (dim + 255) / 256;
     if (blocks > 148 * 16) blocks = 148 * 16;

@@ -40,6 +40,10 @@ struct BitSumShape {
 };
 BitSumShape bitsum_shape(int n);
 cudaError_t launch_bitsums_c128(const void* st, int n, int kind, void* partials, cudaStream_t s);
+// Amplitude bit sums with an explicit shape: 2^g CTAs, nr round bits per
+// thread (n = 12 + g + nr when n >= 12), partials of 1 + 2 * (12 + nr)
+// double2 per CTA.
+cudaError_t launch_bitsums_c128_shape(const void* st, int n, int g, int nr, void* partials, cudaStream_t s);
 cudaError_t launch_probs_c128(const void* st, uint64_t dim, double* out, cudaStream_t s);
 
 }  // namespace kate
