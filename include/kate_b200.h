@@ -207,6 +207,7 @@ KATE_API kate_status kate_sim_get_pass(kate_sim* s, int i, int* tile_qbits, int*
  * which ops it applies, and how it permutes the tile on write. */
 #define KATE_PLAN_NO_REMAP 1u   /* keep the low physical bits fixed */
 #define KATE_PLAN_NO_FUSE1Q 2u  /* do not multiply single-qubit chains */
+#define KATE_PLAN_C64 4u        /* complex64 plan: dense 5-qubit tensor-core blocks */
 KATE_API kate_status kate_plan_create(const kate_circuit* c, int max_tile, int coalesce, unsigned flags,
                                       kate_plan** out);
 KATE_API kate_status kate_plan_destroy(kate_plan* p);
@@ -224,6 +225,11 @@ KATE_API kate_status kate_plan_get_op(const kate_plan* p, int i, int* ints, uint
  * *has = 0 when the pass runs on the generic shared-memory kernel. */
 KATE_API kate_status kate_plan_get_program(const kate_plan* p, int i, void* out, size_t cap, size_t* size, int* has);
 KATE_API kate_status kate_plan_num_smem_ops(const kate_plan* p, int* out);
+/* Complex64 tensor-core block program of pass i (the BlockProg struct of
+ * kate_b200/csrc/device_types.h) and the pool of block operand images. */
+KATE_API kate_status kate_plan_get_block_program(const kate_plan* p, int i, void* out, size_t cap, size_t* size,
+                                                 int* has);
+KATE_API kate_status kate_plan_block_images(const kate_plan* p, void* out, size_t cap, size_t* size);
 /* Shared-memory op i of the register-staged programs, same format as kate_plan_get_op. */
 KATE_API kate_status kate_plan_get_smem_op(const kate_plan* p, int i, int* ints, uint64_t* pmask, double* vals);
 /* phys[q]: physical bit of logical qubit q after the last pass;

@@ -69,6 +69,8 @@ SIGNATURES = {
     "kate_plan_final_layout": [_vp, _ip, _ip],
     "kate_plan_get_program": [_vp, _i, _vp, _c.c_size_t, _c.POINTER(_c.c_size_t), _ip],
     "kate_plan_num_smem_ops": [_vp, _ip],
+    "kate_plan_get_block_program": [_vp, _i, _vp, _c.c_size_t, _c.POINTER(_c.c_size_t), _ip],
+    "kate_plan_block_images": [_vp, _vp, _c.c_size_t, _c.POINTER(_c.c_size_t)],
     "kate_plan_get_smem_op": [_vp, _i, _ip, _u64p, _dp],
     "kate_proba_state_noalloc": [_vp, _i, _ip, _ip, _dp, _vp],
 }

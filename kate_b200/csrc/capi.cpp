@@ -442,6 +442,7 @@ kate_status kate_plan_create(const kate_circuit* c, int max_tile, int coalesce, 
         opt.coalesce = coalesce;
         opt.remap = !(flags & KATE_PLAN_NO_REMAP);
         opt.fuse_1q = !(flags & KATE_PLAN_NO_FUSE1Q);
+        opt.c64 = (flags & KATE_PLAN_C64) != 0;
         auto* p = new kate_plan();
         std::string e = kate::build_plan(prog, opt, &p->plan);
         if (!e.empty()) {
@@ -526,6 +527,23 @@ kate_status kate_plan_get_program(const kate_plan* p, int i, void* out, size_t c
     const auto& pp = p->plan.passes[i];
     *has = pp.prog ? 1 : 0;
     if (pp.prog && out && cap >= sizeof(PassProg)) std::memcpy(out, pp.prog.get(), sizeof(PassProg));
+    return KATE_OK;
+}
+
+kate_status kate_plan_get_block_program(const kate_plan* p, int i, void* out, size_t cap, size_t* size, int* has) {
+    REQUIRE(p && size && has, "null pointer");
+    REQUIRE(i >= 0 && i < (int)p->plan.passes.size(), "pass index out of range");
+    *size = sizeof(BlockProg);
+    const auto& pp = p->plan.passes[i];
+    *has = pp.bprog ? 1 : 0;
+    if (pp.bprog && out && cap >= sizeof(BlockProg)) std::memcpy(out, pp.bprog.get(), sizeof(BlockProg));
+    return KATE_OK;
+}
+
+kate_status kate_plan_block_images(const kate_plan* p, void* out, size_t cap, size_t* size) {
+    REQUIRE(p && size, "null pointer");
+    *size = p->plan.bimg.size();
+    if (out && cap >= p->plan.bimg.size()) std::memcpy(out, p->plan.bimg.data(), p->plan.bimg.size());
     return KATE_OK;
 }
 

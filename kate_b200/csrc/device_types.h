@@ -100,3 +100,24 @@ typedef struct {
     uint8_t outsrc[16]; // on store, output tile bit t takes input tile bit outsrc[t]
     uint8_t cphys[48];  // physical bits of the coset index, ascending
 } DevPass;
+
+// ---- complex64 tensor-core pass program (k_block_c64.cu) ----
+// A pass applies up to KATE_C64_MAX_BLOCKS dense 5-qubit blocks to each
+// 4096-amplitude tile. Block b acts on tile bits btb[b][0..4] (ascending;
+// bit i of the block's local index is btb[b][i]); its 32x32 complex matrix
+// is stored as the real 64x64 matrix W (W[2r][2c] = Re U[r][c],
+// W[2r][2c+1] = -Im U[r][c], W[2r+1][2c] = Im U[r][c], W[2r+1][2c+1] =
+// Re U[r][c]) split into TF32 hi and lo parts, each laid out as the
+// K-major SWIZZLE_128B UMMA operand image (two K halves of 64 rows x 128 B):
+// KATE_BLOCK_IMG_BYTES per block at byte offset bimg[b] of the image pool.
+#define KATE_C64_MAX_BLOCKS 2
+#define KATE_BLOCK_IMG_BYTES 32768
+
+typedef struct {
+    int32_t m, ncb, nblocks, pad;
+    uint8_t tphys[16];
+    uint8_t outsrc[16];
+    uint8_t cphys[48];
+    uint8_t btb[KATE_C64_MAX_BLOCKS][8];
+    uint64_t bimg[KATE_C64_MAX_BLOCKS];
+} BlockProg;

@@ -19,7 +19,15 @@ namespace {
 constexpr int NT = 256;
 constexpr int MAXM = 12;
 
-__global__ void __launch_bounds__(NT) k_pass_generic(double2* __restrict__ st, const DevPass P,
+__device__ __forceinline__ double2 widen(double2 v) { return v; }
+__device__ __forceinline__ double2 widen(float2 v) { return make_double2(v.x, v.y); }
+__device__ __forceinline__ void narrow(double2* p, double2 v) { *p = v; }
+__device__ __forceinline__ void narrow(float2* p, double2 v) { *p = make_float2((float)v.x, (float)v.y); }
+
+// A (global amplitude type): double2 for complex128 states, float2 for
+// complex64; the shared-memory tile is double2 either way.
+template <typename A>
+__global__ void __launch_bounds__(NT) k_pass_generic(A* __restrict__ st, const DevPass P,
                                                      const DevOp* __restrict__ ops,
                                                      const double2* __restrict__ pool) {
     extern __shared__ double2 tile[];
@@ -32,7 +40,7 @@ __global__ void __launch_bounds__(NT) k_pass_generic(double2* __restrict__ st, c
         for (uint32_t i = threadIdx.x; i < T; i += NT) {
             uint64_t a = base;
             for (int b = 0; b < m; b++) a |= (uint64_t)((i >> b) & 1u) << P.tphys[b];
-            tile[ops::swz(i)] = st[a];
+            tile[ops::swz(i)] = widen(st[a]);
         }
         __syncthreads();
         for (int k = 0; k < P.nops; k++) {
@@ -48,15 +56,19 @@ __global__ void __launch_bounds__(NT) k_pass_generic(double2* __restrict__ st, c
                 a |= (uint64_t)bit << P.tphys[b];
                 i |= bit << P.outsrc[b];
             }
-            st[a] = tile[ops::swz(i)];
+            narrow(st + a, tile[ops::swz(i)]);
         }
         __syncthreads();
     }
 }
 
-__global__ void k_set_one(double2* st) { st[0] = make_double2(1.0, 0.0); }
+template <typename A>
+__global__ void k_set_one(A* st) {
+    narrow(st, make_double2(1.0, 0.0));
+}
 
-__global__ void k_init_product(double2* __restrict__ st, int n, const ProductInit P) {
+template <typename A>
+__global__ void k_init_product(A* __restrict__ st, int n, const ProductInit P) {
     const uint64_t dim = 1ull << n;
     for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < dim; x += (uint64_t)gridDim.x * blockDim.x) {
         double2 t = make_double2(1.0, 0.0);
@@ -64,36 +76,45 @@ __global__ void k_init_product(double2* __restrict__ st, int n, const ProductIni
             int b = (int)((x >> j) & 1ull);
             t = cmul(t, make_double2(P.v[b][j][0], P.v[b][j][1]));
         }
-        st[x] = t;
+        narrow(st + x, t);
     }
 }
 
 }  // namespace
 
-cudaError_t launch_set_basis0_c128(void* st, uint64_t dim, cudaStream_t s) {
-    cudaError_t e = cudaMemsetAsync(st, 0, dim * sizeof(double2), s);
+cudaError_t launch_set_basis0(void* st, uint64_t dim, int prec, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(st, 0, dim * (prec == 0 ? sizeof(double2) : sizeof(float2)), s);
     if (e != cudaSuccess) return e;
-    k_set_one<<<1, 1, 0, s>>>((double2*)st);
+    if (prec == 0) k_set_one<double2><<<1, 1, 0, s>>>((double2*)st);
+    else k_set_one<float2><<<1, 1, 0, s>>>((float2*)st);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_set_basis0_c128(void* st, uint64_t dim, cudaStream_t s) { return launch_set_basis0(st, dim, 0, s); }
+
+cudaError_t launch_init_product(void* st, int n, const ProductInit& P, int prec, cudaStream_t s) {
+    uint64_t dim = 1ull << n;
+    uint64_t blocks = (dim + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    if (prec == 0) k_init_product<double2><<<(unsigned)blocks, 256, 0, s>>>((double2*)st, n, P);
+    else k_init_product<float2><<<(unsigned)blocks, 256, 0, s>>>((float2*)st, n, P);
     return cudaGetLastError();
 }
 
 cudaError_t launch_init_product_c128(void* st, int n, const ProductInit& P, cudaStream_t s) {
-    uint64_t dim = 1ull << n;
-    uint64_t blocks = (dim + 255) / 256;
-    if (blocks > 148 * 16) blocks = 148 * 16;
-    k_init_product<<<(unsigned)blocks, 256, 0, s>>>((double2*)st, n, P);
-    return cudaGetLastError();
+    return launch_init_product(st, n, P, 0, s);
 }
 
 int generic_pass_grid(int n, int m, int device) {
     static int cached[64] = {0};
     if (device < 0 || device >= 64) device = 0;
     if (!cached[device]) {
-        cudaFuncSetAttribute(k_pass_generic, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (1 << MAXM) * (int)sizeof(double2));
+        const int smem = (1 << MAXM) * (int)sizeof(double2);
+        cudaFuncSetAttribute(k_pass_generic<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(k_pass_generic<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         int sms = 148, occ = 1;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pass_generic, NT, (1 << MAXM) * sizeof(double2));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pass_generic<double2>, NT, smem);
         if (occ < 1) occ = 1;
         cached[device] = sms * occ;
     }
@@ -101,13 +122,19 @@ int generic_pass_grid(int n, int m, int device) {
     return (int)(ncos < (uint64_t)cached[device] ? ncos : (uint64_t)cached[device]);
 }
 
+cudaError_t launch_pass_generic(void* st, int prec, const DevPass& p, const DevOp* ops, const void* pool, int grid,
+                                cudaStream_t s) {
+    if (p.m > MAXM) return cudaErrorInvalidValue;
+    size_t smem = ((size_t)1 << p.m) * sizeof(double2);
+    if (prec == 0) k_pass_generic<double2><<<grid, NT, smem, s>>>((double2*)st, p, ops, (const double2*)pool);
+    else k_pass_generic<float2><<<grid, NT, smem, s>>>((float2*)st, p, ops, (const double2*)pool);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_pass_generic_c128(void* st, int n, const DevPass& p, const DevOp* ops, const void* pool, int grid,
                                      cudaStream_t s) {
     (void)n;
-    if (p.m > MAXM) return cudaErrorInvalidValue;
-    size_t smem = ((size_t)1 << p.m) * sizeof(double2);
-    k_pass_generic<<<grid, NT, smem, s>>>((double2*)st, p, ops, (const double2*)pool);
-    return cudaGetLastError();
+    return launch_pass_generic(st, 0, p, ops, pool, grid, s);
 }
 
 }  // namespace kate

@@ -43,8 +43,15 @@ struct Acc<double> {
 // Output slots per CTA: 0 = total; 1 + 2*b = bit b is 0; 2 + 2*b = bit b is
 // 1, for local bits b = 0..11 then round bits 12..12+nr-1 (numbered in slot
 // order, not in index order).
-template <typename V>
-__global__ void __launch_bounds__(NT) k_bitsums(const double2* __restrict__ st, int n, int g, int nr,
+__device__ __forceinline__ double2 ld_amp(const double2* p) { return *p; }
+__device__ __forceinline__ double2 ld_amp(const float2* p) {
+    const float2 v = *p;
+    return make_double2(v.x, v.y);
+}
+
+// S: stored amplitude type (double2 or float2); sums are FP64 either way.
+template <typename V, typename S = double2>
+__global__ void __launch_bounds__(NT) k_bitsums(const S* __restrict__ st, int n, int g, int nr,
                                                 V* __restrict__ part) {
     using A = Acc<V>;
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
@@ -63,7 +70,7 @@ __global__ void __launch_bounds__(NT) k_bitsums(const double2* __restrict__ st, 
         for (int j = 0; j < 16; j++) {
             const uint32_t x = (uint32_t)t + ((uint32_t)j << 8);
             V v = A::zero();
-            if (x < lim) v = A::val(st[base + x]);
+            if (x < lim) v = A::val(ld_amp(st + base + x));
             tr = A::add(tr, v);
 #pragma unroll
             for (int i = 0; i < 4; i++) {
@@ -135,9 +142,10 @@ __global__ void __launch_bounds__(NT) k_bitsums(const double2* __restrict__ st, 
     }
 }
 
-__global__ void k_probs(const double2* __restrict__ st, uint64_t dim, double* __restrict__ out) {
+template <typename S>
+__global__ void k_probs(const S* __restrict__ st, uint64_t dim, double* __restrict__ out) {
     for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < dim; x += (uint64_t)gridDim.x * blockDim.x) {
-        double2 a = st[x];
+        const double2 a = ld_amp(st + x);
         out[x] = a.x * a.x + a.y * a.y;
     }
 }
@@ -177,7 +185,26 @@ cudaError_t launch_bitsums_c128_shape(const void* st, int n, int g, int nr, void
 cudaError_t launch_probs_c128(const void* st, uint64_t dim, double* out, cudaStream_t s) {
     uint64_t blocks = (dim + 255) / 256;
     if (blocks > 148 * 16) blocks = 148 * 16;
-    k_probs<<<(unsigned)blocks, 256, 0, s>>>((const double2*)st, dim, out);
+    k_probs<double2><<<(unsigned)blocks, 256, 0, s>>>((const double2*)st, dim, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bitsums(const void* st, int prec, int n, int kind, void* partials, cudaStream_t s) {
+    if (prec == 0) return launch_bitsums_c128(st, n, kind, partials, s);
+    BitSumShape sh = bitsum_shape(n);
+    if (sh.nr > MAXR) return cudaErrorInvalidValue;
+    if (kind == 0)
+        k_bitsums<double2, float2><<<sh.grid, NT, 0, s>>>((const float2*)st, n, sh.g, sh.nr, (double2*)partials);
+    else
+        k_bitsums<double, float2><<<sh.grid, NT, 0, s>>>((const float2*)st, n, sh.g, sh.nr, (double*)partials);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_probs(const void* st, int prec, uint64_t dim, double* out, cudaStream_t s) {
+    if (prec == 0) return launch_probs_c128(st, dim, out, s);
+    uint64_t blocks = (dim + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_probs<float2><<<(unsigned)blocks, 256, 0, s>>>((const float2*)st, dim, out);
     return cudaGetLastError();
 }
 

@@ -15,6 +15,14 @@ struct ProductInit {
     int n;
 };
 
+// prec: 0 = complex128 (double2 amplitudes), 1 = complex64 (float2).
+cudaError_t launch_set_basis0(void* st, uint64_t dim, int prec, cudaStream_t s);
+cudaError_t launch_init_product(void* st, int n, const ProductInit& P, int prec, cudaStream_t s);
+cudaError_t launch_pass_generic(void* st, int prec, const DevPass& p, const DevOp* ops, const void* pool, int grid,
+                                cudaStream_t s);
+cudaError_t launch_bitsums(const void* st, int prec, int n, int kind, void* partials, cudaStream_t s);
+cudaError_t launch_probs(const void* st, int prec, uint64_t dim, double* out, cudaStream_t s);
+
 // c128 state (double2 amplitudes)
 cudaError_t launch_set_basis0_c128(void* st, uint64_t dim, cudaStream_t s);
 cudaError_t launch_init_product_c128(void* st, int n, const ProductInit& P, cudaStream_t s);
@@ -28,6 +36,11 @@ int generic_pass_grid(int n, int m, int device);
 cudaError_t launch_tile_c128(void* st, const PassProg& prog, const DevOp* sops, const void* pool, int grid, int nbuf,
                              cudaStream_t s);
 int tile_pass_grid(int n, int device, int nbuf);
+
+// Complex64 pass of 5-qubit dense blocks on the tensor cores. err: device
+// int set to 1 if a bounded wait gave up.
+cudaError_t launch_block_c64(void* st, const BlockProg& prog, const void* bimg, int* err, int grid, cudaStream_t s);
+int block_c64_grid(int n, int device);
 
 // Bit sums: per CTA, for every local bit, the sum over amplitudes with the
 // bit 0 and with the bit 1, plus the total. kind 0 sums amplitudes (double2

@@ -171,7 +171,8 @@ struct Layout {
 // extended in place. If `order` is non-null it records the order in which
 // qubits joined T.
 std::vector<int> greedy_pass(const std::vector<PGate>& pg, const std::vector<int>& rem, int n, int m,
-                             std::vector<char>& inT, int& tsize, std::vector<int>* order, size_t scan_limit) {
+                             std::vector<char>& inT, int& tsize, std::vector<int>* order, size_t scan_limit,
+                             bool all_targets = false) {
     std::vector<char> blocked(n, 0);
     std::vector<int> exec;
     size_t scanned = 0;
@@ -183,15 +184,23 @@ std::vector<int> greedy_pass(const std::vector<PGate>& pg, const std::vector<int
         for (int q : g.tq) blk |= blocked[q] != 0;
         for (int q : g.fq) blk |= blocked[q] != 0;
         if (!blk) {
+            // Targets must be tile qubits; so must every qubit when
+            // all_targets is set (complex64 blocks).
             int need = 0;
             for (int q : g.tq) need += !inT[q];
+            if (all_targets)
+                for (int q : g.fq) need += !inT[q];
             if (tsize + need <= m) {
-                for (int q : g.tq)
+                auto take = [&](int q) {
                     if (!inT[q]) {
                         inT[q] = 1;
                         tsize++;
                         if (order) order->push_back(q);
                     }
+                };
+                for (int q : g.tq) take(q);
+                if (all_targets)
+                    for (int q : g.fq) take(q);
                 exec.push_back(gi);
                 continue;
             }
@@ -368,7 +377,7 @@ std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out) {
 
     const int m = std::min(opt.max_tile, n);
     int maxT = 0;
-    for (auto& g : plan.pgates) maxT = std::max(maxT, (int)g.tq.size());
+    for (auto& g : plan.pgates) maxT = std::max(maxT, (int)(g.tq.size() + (opt.c64 ? g.fq.size() : 0)));
     if (maxT > m) return "a gate has more target qubits than the tile";
     // The c low physical bits are always tile bits; leave room for the
     // widest gate's targets beside them so every pass can make progress.
@@ -384,23 +393,38 @@ std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out) {
             inT[L.inv[p]] = 1;
             tsize++;
         }
-        std::vector<int> exec = greedy_pass(plan.pgates, rem, n, m, inT, tsize, nullptr, scan_limit);
-        if ((int)exec.size() > opt.max_gates_per_pass) {
+        std::vector<int> exec = greedy_pass(plan.pgates, rem, n, m, inT, tsize, nullptr, scan_limit, opt.c64);
+        size_t keep = exec.size();
+        if ((int)keep > opt.max_gates_per_pass) keep = opt.max_gates_per_pass;
+        if (opt.c64 && m == KATE_TILE_BITS) {
+            std::vector<int> which = block_partition(plan.pgates, exec);
+            size_t k = 0;
+            while (k < which.size() && which[k] < KATE_C64_MAX_BLOCKS) k++;
+            keep = std::min(keep, k);
+        }
+        if (keep < exec.size()) {
             // Keep a prefix of the executable gates (a prefix of a
             // dependency-closed set in program order is dependency-closed).
-            exec.resize(opt.max_gates_per_pass);
+            exec.resize(keep);
             std::fill(inT.begin(), inT.end(), 0);
             tsize = 0;
             for (int p = 0; p < c; p++) {
                 inT[L.inv[p]] = 1;
                 tsize++;
             }
-            for (int gi : exec)
+            for (int gi : exec) {
                 for (int q : plan.pgates[gi].tq)
                     if (!inT[q]) {
                         inT[q] = 1;
                         tsize++;
                     }
+                if (opt.c64)
+                    for (int q : plan.pgates[gi].fq)
+                        if (!inT[q]) {
+                            inT[q] = 1;
+                            tsize++;
+                        }
+            }
         }
         if (exec.empty()) return "planner made no progress";
         for (int p = 0; p < n && tsize < m; p++)
@@ -429,7 +453,7 @@ std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out) {
             std::vector<char> inT2(n, 0);
             int ts2 = 0;
             std::vector<int> order;
-            greedy_pass(plan.pgates, rem, n, m, inT2, ts2, &order, scan_limit);
+            greedy_pass(plan.pgates, rem, n, m, inT2, ts2, &order, scan_limit, opt.c64);
             for (int q : order)
                 if (inT[q] && (int)newlow.size() < c) newlow.push_back(q);
         }
@@ -468,7 +492,14 @@ std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out) {
         }
         lower_pass(plan, pp, L.phys, plan.pool);
         pp.phys_before = L.phys;
-        if (opt.staged) {
+        if (opt.c64) {
+            if (m == KATE_TILE_BITS) {
+                auto bp = std::make_shared<BlockProg>();
+                pp.prog_note = build_block_program(plan, pp, n, plan.bimg, bp.get());
+                if (pp.prog_note.empty()) pp.bprog = bp;
+                else return "complex64 block lowering failed: " + pp.prog_note;
+            }
+        } else if (opt.staged) {
             auto prog = std::make_shared<PassProg>();
             pp.prog_note = build_pass_program(plan, pp, n, plan.smem_ops, plan.pool, prog.get());
             if (pp.prog_note.empty()) pp.prog = prog;

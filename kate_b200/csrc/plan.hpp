@@ -38,6 +38,7 @@ struct PlanOptions {
     bool remap = true;   // move next-needed qubits into the low bits on write
     bool fuse_1q = true; // multiply chains of single-qubit ops on one qubit (FP64, host)
     bool staged = true;  // build register-staged programs for the tile kernel
+    bool c64 = false;    // complex64 state: passes become dense 5-qubit tensor-core blocks
     int max_gates_per_pass = 96;  // keeps a pass program within the kernel parameter
 };
 
@@ -49,6 +50,7 @@ struct PlannedPass {
     std::vector<DevOp> ops;      // device ops, tile-relative (generic kernel)
     std::vector<int> phys_before;  // layout (logical -> physical) when the pass starts
     std::shared_ptr<PassProg> prog;  // register-staged program (tile kernel), if it applies
+    std::shared_ptr<BlockProg> bprog;  // complex64 tensor-core block program, if it applies
     std::string prog_note;           // why the generic kernel runs this pass, if it does
 };
 
@@ -71,6 +73,7 @@ struct Plan {
     std::vector<int> initial_permutation, final_inverse_permutation;
     std::vector<Cx> pool;            // dense matrices and diagonal tables of all ops
     std::vector<DevOp> smem_ops;     // shared-memory ops referenced by register-staged programs
+    std::vector<uint8_t> bimg;       // complex64 block operand images (KATE_BLOCK_IMG_BYTES each)
 };
 
 // Classifies gates, plans passes and lowers them to device ops. Dense gates
@@ -85,6 +88,14 @@ std::vector<PlannedPass> plan_relayout(int n, const std::vector<int>& phys, cons
 // appended to smem_ops (their tables to pool). Returns "" on success.
 std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n, std::vector<DevOp>& smem_ops,
                                std::vector<Cx>& pool, PassProg* out);
+
+// Complex64 block program of a pass (12-qubit tiles); operand images are
+// appended to `pool`. Returns "" on success.
+std::string build_block_program(const Plan& plan, const PlannedPass& pass, int n, std::vector<uint8_t>& pool,
+                                BlockProg* out);
+// Greedy partition of a pass's gates into blocks of at most five qubits:
+// the block number of each gate.
+std::vector<int> block_partition(const std::vector<PGate>& pg, const std::vector<int>& gates);
 
 // Register-op form of a 2x2 matrix: SOP_UR (real), SOP_UX ([[a, ib], [ic, d]]) or SOP_U.
 int classify_2x2(const Cx* m);

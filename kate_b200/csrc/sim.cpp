@@ -40,6 +40,8 @@ struct SimImpl {
     DevOp* d_sops = nullptr;   // shared-memory ops of register-staged programs
     void* d_pool = nullptr;
     void* d_part = nullptr;
+    void* d_bimg = nullptr;   // complex64 block operand images
+    int* d_err = nullptr;     // set by kernels whose bounded waits gave up
     size_t part_bytes = 0;
     std::vector<DevPass> hpasses;
     cudaStream_t stream = nullptr;
@@ -52,9 +54,11 @@ struct SimImpl {
     // Launches pass i of the plan on stream st.
     cudaError_t launch_pass(size_t i, cudaStream_t st) {
         const PlannedPass& p = plan.passes[i];
+        if (p.bprog) return launch_block_c64(d_state, *p.bprog, d_bimg, d_err, block_grid, st);
         if (p.prog) return launch_tile_c128(d_state, *p.prog, d_sops, d_pool, tile_grid, nbuf, st);
-        return launch_pass_generic_c128(d_state, n, hpasses[i], d_ops, d_pool, grid, st);
+        return launch_pass_generic(d_state, precision, hpasses[i], d_ops, d_pool, grid, st);
     }
+    int block_grid = 0;
 
     uint64_t dim() const { return 1ull << n; }
     size_t amp_bytes() const { return precision == 0 ? 16 : 8; }
@@ -74,7 +78,7 @@ struct SimImpl {
         for (auto& p : pp) {
             DevPass d = to_devpass(n, p, 0);
             int grid_r = generic_pass_grid(n, d.m, device);
-            KCHECK(launch_pass_generic_c128(d_state, n, d, d_ops, d_pool, grid_r, stream));
+            KCHECK(launch_pass_generic(d_state, precision, d, d_ops, d_pool, grid_r, stream));
         }
         phys = target;
         return "";
@@ -86,7 +90,7 @@ struct SimImpl {
         BitSumShape sh = bitsum_shape(n);
         const int w = kind == 0 ? 2 : 1;
         std::vector<double> h((size_t)sh.grid * sh.nout * w);
-        KCHECK(launch_bitsums_c128(d_state, n, kind, d_part, stream));
+        KCHECK(launch_bitsums(d_state, precision, n, kind, d_part, stream));
         KCHECK(cudaMemcpyAsync(h.data(), d_part, h.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
         KCHECK(cudaStreamSynchronize(stream));
         s0.assign((size_t)n * w, 0.0);
@@ -115,7 +119,7 @@ struct SimImpl {
 };
 
 std::string Simulator::create(const Program& prog_in, int precision, int device, Simulator** out) {
-    if (precision != 0) return "only KATE_C128 is available in this build of the simulator";
+    if (precision != 0 && precision != 1) return "unknown precision";
     if (prog_in.nqbits < 1 || prog_in.nqbits > 34) return "the device simulator supports 1 to 34 qubits";
     auto* impl = new SimImpl();
     auto fail = [&](const std::string& e) {
@@ -132,6 +136,7 @@ std::string Simulator::create(const Program& prog_in, int precision, int device,
         std::string e = pass_compile_default(impl->prog, 0, impl->prog.nqbits);
         if (!e.empty()) return fail(e);
     }
+    impl->opt.c64 = precision == 1;
     std::string e = build_plan(impl->prog, impl->opt, &impl->plan);
     if (!e.empty()) return fail(e);
 
@@ -159,6 +164,13 @@ std::string Simulator::create(const Program& prog_in, int precision, int device,
     if (!ops.empty()) cudaMemcpy(impl->d_ops, ops.data(), ops.size() * sizeof(DevOp), cudaMemcpyHostToDevice);
     if (!impl->plan.pool.empty())
         cudaMemcpy(impl->d_pool, impl->plan.pool.data(), impl->plan.pool.size() * sizeof(Cx), cudaMemcpyHostToDevice);
+    ce = cudaMalloc(&impl->d_bimg, std::max<size_t>(16, impl->plan.bimg.size()));
+    if (ce != cudaSuccess) return fail(cuda_err("cudaMalloc(block images)", ce));
+    if (!impl->plan.bimg.empty())
+        cudaMemcpy(impl->d_bimg, impl->plan.bimg.data(), impl->plan.bimg.size(), cudaMemcpyHostToDevice);
+    ce = cudaMalloc(&impl->d_err, sizeof(int));
+    if (ce != cudaSuccess) return fail(cuda_err("cudaMalloc(error flag)", ce));
+    cudaMemset(impl->d_err, 0, sizeof(int));
     BitSumShape sh = bitsum_shape(impl->n);
     impl->part_bytes = (size_t)sh.grid * sh.nout * 2 * sizeof(double);
     ce = cudaMalloc(&impl->d_part, impl->part_bytes);
@@ -167,7 +179,10 @@ std::string Simulator::create(const Program& prog_in, int precision, int device,
     if (ce != cudaSuccess) return fail(cuda_err("cudaMalloc(state)", ce));
     impl->grid = generic_pass_grid(impl->n, std::min(impl->opt.max_tile, impl->n), device);
     if (const char* e = std::getenv("KATE_TILE_NBUF")) impl->nbuf = std::atoi(e) == 2 ? 2 : 1;
-    if (impl->n >= KATE_TILE_BITS) impl->tile_grid = tile_pass_grid(impl->n, device, impl->nbuf);
+    if (impl->n >= KATE_TILE_BITS) {
+        if (precision == 0) impl->tile_grid = tile_pass_grid(impl->n, device, impl->nbuf);
+        else impl->block_grid = block_c64_grid(impl->n, device);
+    }
     impl->phys.resize(impl->n);
     std::iota(impl->phys.begin(), impl->phys.end(), 0);
     auto* s = new Simulator();
@@ -185,6 +200,8 @@ Simulator::~Simulator() {
     cudaFree(d_->d_sops);
     cudaFree(d_->d_pool);
     cudaFree(d_->d_part);
+    cudaFree(d_->d_bimg);
+    cudaFree(d_->d_err);
     if (d_->stream) cudaStreamDestroy(d_->stream);
     delete d_;
 }
@@ -211,9 +228,9 @@ std::string Simulator::run_async(void* stream_in, const double* tp) {
             P.v[1][lab][0] = er * s0;
             P.v[1][lab][1] = ei * s0;
         }
-        KCHECK(launch_init_product_c128(S.d_state, S.n, P, st));
+        KCHECK(launch_init_product(S.d_state, S.n, P, S.precision, st));
     } else {
-        KCHECK(launch_set_basis0_c128(S.d_state, S.dim(), st));
+        KCHECK(launch_set_basis0(S.d_state, S.dim(), S.precision, st));
     }
     for (size_t i = 0; i < S.hpasses.size(); i++) KCHECK(S.launch_pass(i, st));
     S.phys = S.plan.final_phys;
@@ -232,6 +249,12 @@ std::string Simulator::run_async(void* stream_in, const double* tp) {
 std::string Simulator::synchronize() {
     KCHECK(cudaSetDevice(d_->device));
     KCHECK(cudaStreamSynchronize(d_->stream));
+    int flag = 0;
+    KCHECK(cudaMemcpy(&flag, d_->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) {
+        cudaMemset(d_->d_err, 0, sizeof(int));
+        return "timed out: a bounded device wait gave up (tensor-core completion not observed)";
+    }
     return "";
 }
 
@@ -297,16 +320,31 @@ std::string Simulator::get_state(double* out) {
     KCHECK(cudaSetDevice(S.device));
     std::string e = S.run_relayout(S.label_layout());
     if (!e.empty()) return e;
-    KCHECK(cudaMemcpyAsync(out, S.d_state, S.dim() * 16, cudaMemcpyDeviceToHost, S.stream));
+    if (S.precision == 0) {
+        KCHECK(cudaMemcpyAsync(out, S.d_state, S.dim() * 16, cudaMemcpyDeviceToHost, S.stream));
+        KCHECK(cudaStreamSynchronize(S.stream));
+        return "";
+    }
+    // complex64: copy as floats, widen in place from the end of the buffer.
+    float* f = reinterpret_cast<float*>(out);
+    KCHECK(cudaMemcpyAsync(f, S.d_state, S.dim() * 8, cudaMemcpyDeviceToHost, S.stream));
     KCHECK(cudaStreamSynchronize(S.stream));
+    for (uint64_t i = 2 * S.dim(); i-- > 0;) out[i] = (double)f[i];
     return "";
 }
 
 std::string Simulator::set_state(const double* in) {
     SimImpl& S = *d_;
     KCHECK(cudaSetDevice(S.device));
-    KCHECK(cudaMemcpyAsync(S.d_state, in, S.dim() * 16, cudaMemcpyHostToDevice, S.stream));
-    KCHECK(cudaStreamSynchronize(S.stream));
+    if (S.precision == 0) {
+        KCHECK(cudaMemcpyAsync(S.d_state, in, S.dim() * 16, cudaMemcpyHostToDevice, S.stream));
+        KCHECK(cudaStreamSynchronize(S.stream));
+    } else {
+        std::vector<float> f(2 * S.dim());
+        for (size_t i = 0; i < f.size(); i++) f[i] = (float)in[i];
+        KCHECK(cudaMemcpyAsync(S.d_state, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice, S.stream));
+        KCHECK(cudaStreamSynchronize(S.stream));
+    }
     S.phys = S.label_layout();
     S.has_state = true;
     return "";
@@ -321,7 +359,7 @@ std::string Simulator::probabilities(double* out) {
     if (!e.empty()) return e;
     double* d = nullptr;
     KCHECK(cudaMallocAsync((void**)&d, S.dim() * sizeof(double), S.stream));
-    cudaError_t ce = launch_probs_c128(S.d_state, S.dim(), d, S.stream);
+    cudaError_t ce = launch_probs(S.d_state, S.precision, S.dim(), d, S.stream);
     if (ce == cudaSuccess)
         ce = cudaMemcpyAsync(out, d, S.dim() * sizeof(double), cudaMemcpyDeviceToHost, S.stream);
     cudaFreeAsync(d, S.stream);
@@ -358,7 +396,7 @@ std::string Simulator::profile_passes(float* ms, float* init_ms) {
     std::vector<cudaEvent_t> ev(S.hpasses.size() + 2);
     for (auto& e : ev) KCHECK(cudaEventCreate(&e));
     KCHECK(cudaEventRecord(ev[0], S.stream));
-    KCHECK(launch_set_basis0_c128(S.d_state, S.dim(), S.stream));
+    KCHECK(launch_set_basis0(S.d_state, S.dim(), S.precision, S.stream));
     KCHECK(cudaEventRecord(ev[1], S.stream));
     for (size_t i = 0; i < S.hpasses.size(); i++) {
         KCHECK(S.launch_pass(i, S.stream));

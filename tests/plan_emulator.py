@@ -35,6 +35,19 @@ PROG_DTYPE = np.dtype([("m", "<i4"), ("ncb", "<i4"), ("nops", "<i4"), ("nmats", 
                        ("nstages", "<i4"), ("sop0", "<i4")])
 
 
+BLOCK_DTYPE = np.dtype([("m", "<i4"), ("ncb", "<i4"), ("nblocks", "<i4"), ("pad", "<i4"), ("tphys", "u1", 16),
+                        ("outsrc", "u1", 16), ("cphys", "u1", 48), ("btb", "u1", (2, 8)), ("bimg", "<u8", 2)])
+
+
+def _sw128_offsets(rows):
+    """Byte offset of (row, k) in a K-major SWIZZLE_128B image, 64 columns."""
+    r = np.arange(rows)[:, None]
+    k = np.arange(64)[None, :]
+    khalf, kk = k >> 5, k & 31
+    chunk, w = kk >> 2, kk & 3
+    return khalf * rows * 128 + (r >> 3) * 1024 + (r & 7) * 128 + ((chunk ^ (r & 7)) << 4) + w * 4
+
+
 def _swz(i):
     return i ^ (((i >> 3) ^ (i >> 6) ^ (i >> 9)) & 7)
 
@@ -99,6 +112,69 @@ class PlanView:
             L.kate_plan_get_program(h, i, buf.ctypes.data_as(ctypes.c_void_p), size.value, ctypes.byref(size),
                                     ctypes.byref(has))
             self.programs.append(buf.view(PROG_DTYPE)[0])
+
+        # complex64 tensor-core block programs
+        self.block_programs = []
+        for i in range(len(self.passes)):
+            size, has = ctypes.c_size_t(), ctypes.c_int()
+            L.kate_plan_get_block_program(h, i, None, 0, ctypes.byref(size), ctypes.byref(has))
+            if not has.value:
+                self.block_programs.append(None)
+                continue
+            buf = np.zeros(size.value, dtype=np.uint8)
+            L.kate_plan_get_block_program(h, i, buf.ctypes.data_as(ctypes.c_void_p), size.value, ctypes.byref(size),
+                                          ctypes.byref(has))
+            self.block_programs.append(buf.view(BLOCK_DTYPE)[0])
+        size = ctypes.c_size_t()
+        L.kate_plan_block_images(h, None, 0, ctypes.byref(size))
+        self.bimg = np.zeros(max(size.value, 16), dtype=np.uint8)
+        L.kate_plan_block_images(h, self.bimg.ctypes.data_as(ctypes.c_void_p), self.bimg.size, ctypes.byref(size))
+
+    def block_matrix(self, off):
+        """The real 64x64 W = hi + lo read back from a block's operand images."""
+        o = _sw128_offsets(64)
+        hi = self.bimg[off:off + 16384].view(np.float32)
+        lo = self.bimg[off + 16384:off + 32768].view(np.float32)
+        return hi[o // 4].astype(np.float64) + lo[o // 4].astype(np.float64)
+
+    def run_blocks(self, state):
+        """Executes complex64 block programs (the others generically): each
+        block multiplies the 128 x 64 real rows of the tile by W^T read back
+        from the operand images, as the tensor-core kernel does."""
+        n = self.n
+        st = state.astype(np.complex128).copy()
+        for p, bp in zip(self.passes, self.block_programs):
+            m = p["m"]
+            T = 1 << m
+            tphys = p["tphys"]
+            cphys = [b for b in range(n) if b not in tphys]
+            toff = _deposit(np.arange(T, dtype=np.int64), tphys)
+            bases = _deposit(np.arange(1 << (n - m), dtype=np.int64), cphys)
+            idx = bases[:, None] + toff[None, :]
+            tile = st[idx]
+            if bp is None:
+                for op in self.ops[p["op0"]:p["op0"] + p["nops"]]:
+                    self._apply(tile, bases, m, op)
+            else:
+                for b in range(int(bp["nblocks"])):
+                    btb = [int(x) for x in bp["btb"][b][:5]]
+                    nb = [i for i in range(m) if i not in btb]
+                    rows = _deposit(np.arange(128, dtype=np.int64), nb)
+                    cols = _deposit(np.arange(32, dtype=np.int64), btb)
+                    sel = rows[:, None] | cols[None, :]          # (128, 32) tile indices
+                    x = tile[:, sel]                            # (C, 128, 32) complex
+                    xr = np.stack([x.real, x.imag], axis=-1).reshape(x.shape[0], 128, 64)
+                    W = self.block_matrix(int(bp["bimg"][b]))
+                    y = xr @ W.T
+                    tile[:, sel] = y[..., 0::2] + 1j * y[..., 1::2]
+            o = np.arange(T, dtype=np.int64)
+            src = np.zeros(T, dtype=np.int64)
+            for b in range(m):
+                src |= ((o >> b) & 1) << p["outsrc"][b]
+            st[idx] = tile[:, src]
+        x = np.arange(1 << n, dtype=np.int64)
+        phys_of_label = [self.final_phys[self.label_to_logical[b]] for b in range(n)]
+        return st[_deposit(x, phys_of_label)]
 
     def _read_op(self, fn, i):
         ints = np.zeros(18, dtype=np.int32)
