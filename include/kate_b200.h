@@ -74,6 +74,7 @@ typedef enum {
 typedef struct kate_circuit kate_circuit;
 typedef struct kate_sim kate_sim;
 typedef struct kate_plan kate_plan;
+typedef struct kate_batch kate_batch;
 
 /* Message of the last failed call on this thread ("" if none). */
 KATE_API const char* kate_last_error(void);
@@ -97,6 +98,13 @@ KATE_API kate_status kate_circuit_append_gate(kate_circuit* c, int id, const int
  * mat: 2*4^nq doubles, row-major, interleaved. 1 <= nq <= 10. */
 KATE_API kate_status kate_circuit_append_dense(kate_circuit* c, const double* mat, const int* qbits, int nq);
 
+/* Appends `count` gates at once (a loop of Circuit::appendGate,
+ * backendagnosticcode/Circuit.hpp:71-91): gate i has id ids[i], nqs[i]
+ * qubits taken in order from `qbits`, optarg optargs[i] (nullable: 0);
+ * dense gates take their 4^nq complex entries (re, im) in order from
+ * `dense`. All or nothing: on an error no gate is appended. */
+KATE_API kate_status kate_circuit_append_many(kate_circuit* c, int count, const int* ids, const int* nqs,
+                                              const int* qbits, const int* optargs, const double* dense);
 KATE_API kate_status kate_circuit_num_gates(const kate_circuit* c, int* out);
 /* Reads gate i. qbits receives *nq ints (capacity 64); dense (nullable)
  * receives 2*4^nq doubles for a dense gate. */
@@ -266,6 +274,55 @@ KATE_API kate_status kate_plan_final_layout(const kate_plan* p, int* phys, int* 
 #define KATE_NOALLOC_SCRATCH_BYTES 672704
 KATE_API kate_status kate_proba_state_noalloc(const void* d_state, int nqbits, const int* phys_of_label,
                                               const int* final_inverse_permutation, double* theta_phi, void* stream);
+
+/* ---- batches of independent circuits ----
+ * Replaces a caller's loop of `Simulator(circuit).execute()` over many
+ * independent circuits (CPUcode/simulator.hpp:120-200 per circuit; the GPU
+ * Simulator, HIPcode/simulator.hpp:220-811, plans, allocates and launches
+ * per circuit). A batch plans every circuit once, keeps all states in one
+ * device arena and runs them as one task queue in one persistent kernel,
+ * captured with its counter resets in one CUDA graph: a run is one graph
+ * launch. Output: <Z_q> for every qubit q of every circuit, in circuit
+ * order (circuit i's outputs follow those of circuits 0..i-1), indexed like
+ * kate_sim_expect_z (by program label). Circuits have 1 to
+ * KATE_BATCH_MAX_QUBITS qubits; those of at most 12 run entirely in one
+ * CTA's shared memory. */
+#define KATE_BATCH_MAX_QUBITS 24
+typedef struct {
+    int fusion;    /* gateFusion width applied to circuits without groups or instructions (1: none; 0: default) */
+    int max_gates; /* gates per pass program (0: default) */
+} kate_batch_tuning;
+typedef struct {
+    int chunk;                 /* cosets (4096-amplitude tiles) per pass task; 0: default */
+    int zchunks;               /* 65536-amplitude chunks per <Z> task; 0: default */
+    unsigned long long window_bytes; /* queue large circuits in windows of this many state bytes; 0: one window */
+    kate_batch_tuning tune[KATE_BATCH_MAX_QUBITS + 1]; /* by qubit count */
+} kate_batch_options;
+
+/* Defaults (no window, default tuning for every qubit count). */
+KATE_API kate_status kate_batch_options_default(kate_batch_options* opt);
+/* The autotuner: for each qubit count present in `circuits`, times
+ * candidate (fusion, max_gates) plans of a sample of those circuits on
+ * `device` and writes the fastest into opt->tune. */
+KATE_API kate_status kate_batch_autotune(const kate_circuit* const* circuits, int count, int precision, int device,
+                                         kate_batch_options* opt);
+/* opt: nullable (defaults). precision: KATE_C64 or KATE_C128. */
+KATE_API kate_status kate_batch_create(const kate_circuit* const* circuits, int count, int precision, int device,
+                                       const kate_batch_options* opt, kate_batch** out);
+KATE_API kate_status kate_batch_destroy(kate_batch* b);
+/* Enqueues one run (one graph launch) on `stream` (NULL: the batch's own). */
+KATE_API kate_status kate_batch_run_async(kate_batch* b, void* stream);
+/* Waits for the runs; KATE_ECUDA if a dependency wait in the kernel gave up. */
+KATE_API kate_status kate_batch_synchronize(kate_batch* b);
+/* Runs once and waits. */
+KATE_API kate_status kate_batch_run(kate_batch* b);
+/* Waits, then copies kate_batch_num_outputs doubles. */
+KATE_API kate_status kate_batch_expect_z(kate_batch* b, double* out);
+KATE_API kate_status kate_batch_num_outputs(const kate_batch* b, long long* out);
+/* info[0] tasks, info[1] pass programs, info[2] arena bytes, info[3] CTAs. */
+KATE_API kate_status kate_batch_info(const kate_batch* b, long long* info);
+/* Average device time of `runs` back-to-back runs (CUDA events). */
+KATE_API kate_status kate_batch_time(kate_batch* b, int runs, float* ms);
 
 #ifdef __cplusplus
 }

@@ -102,8 +102,9 @@ class Circuit:
             h = ctypes.c_void_p()
             _check(self._lib.kate_circuit_create(int(nqbits), ctypes.byref(h)))
             self._h = h
-        for g in gates:
-            self.appendGate(g)
+        gates = list(gates)
+        if gates:
+            self.appendGates(gates)
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -140,6 +141,37 @@ class Circuit:
         else:
             _check(self._lib.kate_circuit_append_gate(self._h, gate.identifier, q.ctypes.data_as(_ip),
                                                       len(gate.qbits), gate.optarg))
+
+    def appendGates(self, gates: Sequence):
+        """Appends many gates (Gate objects or (id, qbits, optarg, dense)
+        tuples) in one call; all or nothing."""
+        ids, nqs, qb, opt, dense = [], [], [], [], []
+        for g in gates:
+            if isinstance(g, Gate):
+                g = g.as_tuple()
+            gid, q, o, d = g
+            ids.append(int(gid))
+            nqs.append(len(q))
+            qb.extend(int(x) for x in q)
+            opt.append(int(o))
+            if gid == DENSE:
+                dim = 1 << len(q)
+                m = np.asarray(d, dtype=np.complex128) if d is not None else None
+                if m is None or m.shape != (dim, dim):
+                    raise KateError(KATE_EINVAL, "size mismatch: dense matrix dimension must be 2^k for k qubits")
+                dense.append(m.ravel())
+        self.appendFlat(ids, nqs, qb, opt, np.concatenate(dense) if dense else None)
+
+    def appendFlat(self, ids, nqs, qbits, optargs, dense=None):
+        """Appends gates given as flat arrays (kate_circuit_append_many):
+        ids[i], nqs[i] qubits taken in order from qbits, optargs[i]; dense
+        gates' 4^nq complex entries in order in ``dense``."""
+        ids_a, nqs_a, qb_a, opt_a = (_iarr(x) for x in (ids, nqs, qbits, optargs))
+        d = (np.ascontiguousarray(np.asarray(dense, dtype=np.complex128)).view(np.float64) if dense is not None
+             else np.zeros(2, dtype=np.float64))
+        _check(self._lib.kate_circuit_append_many(self._h, len(ids_a), ids_a.ctypes.data_as(_ip),
+                                                  nqs_a.ctypes.data_as(_ip), qb_a.ctypes.data_as(_ip),
+                                                  opt_a.ctypes.data_as(_ip), d.ctypes.data_as(_dp)))
 
     # --- passes (backendagnosticcode/Circuit.hpp) ---
     def gateScheduling(self):
@@ -353,3 +385,78 @@ class Simulator:
 
 __all__ = ["Gate", "Circuit", "Simulator", "mergeGate", "proba_state", "KateError", "Hadamard", "CNOT", "CRk",
            "TOFFOLI", "RX", "RZ", "DENSE", "C128", "C64"]
+
+
+class Batch:
+    """Many independent circuits in one persistent-kernel launch (one CUDA
+    graph). Outputs <Z_q> per qubit of every circuit.
+
+    ``options``: a ``_lib.BatchOptions`` (``None``: defaults); with
+    ``autotune=True`` the options are first tuned on the device for the qubit
+    counts present (``self.options`` holds the result).
+    """
+
+    def __init__(self, circuits: Sequence[Circuit], precision: int = C64, device: int = 0, options=None,
+                 autotune: bool = False):
+        self._lib = _lib.lib()
+        self._h = None
+        self.circuits = list(circuits)
+        self.nqbits = [c.nqbits for c in self.circuits]
+        arr = (ctypes.c_void_p * len(self.circuits))(*[c.handle.value for c in self.circuits])
+        if options is None:
+            options = _lib.BatchOptions()
+            _check(self._lib.kate_batch_options_default(ctypes.byref(options)))
+        if autotune:
+            _check(self._lib.kate_batch_autotune(arr, len(self.circuits), int(precision), int(device),
+                                                 ctypes.byref(options)))
+        self.options = options
+        h = ctypes.c_void_p()
+        _check(self._lib.kate_batch_create(arr, len(self.circuits), int(precision), int(device),
+                                           ctypes.byref(options), ctypes.byref(h)))
+        self._h = h
+        v = ctypes.c_longlong()
+        _check(self._lib.kate_batch_num_outputs(self._h, ctypes.byref(v)))
+        self.num_outputs = v.value
+
+    def __del__(self):
+        self.close()
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            self._lib.kate_batch_destroy(h)
+            self._h = None
+
+    def run_async(self, stream: int = 0):
+        _check(self._lib.kate_batch_run_async(self._h, ctypes.c_void_p(stream or None)))
+
+    def synchronize(self):
+        _check(self._lib.kate_batch_synchronize(self._h))
+
+    def run(self):
+        _check(self._lib.kate_batch_run(self._h))
+
+    def expect_z_flat(self, out: Optional[np.ndarray] = None) -> np.ndarray:
+        if out is None:
+            out = np.zeros(self.num_outputs, dtype=np.float64)
+        _check(self._lib.kate_batch_expect_z(self._h, out.ctypes.data_as(_dp)))
+        return out
+
+    def expect_z(self) -> List[np.ndarray]:
+        flat = self.expect_z_flat()
+        res, o = [], 0
+        for n in self.nqbits:
+            res.append(flat[o:o + n].copy())
+            o += n
+        return res
+
+    def info(self) -> dict:
+        v = (ctypes.c_longlong * 4)()
+        _check(self._lib.kate_batch_info(self._h, v))
+        return {"tasks": v[0], "programs": v[1], "arena_bytes": v[2], "ctas": v[3]}
+
+    def time(self, runs: int = 1) -> float:
+        ms = ctypes.c_float()
+        _check(self._lib.kate_batch_time(self._h, int(runs), ctypes.byref(ms)))
+        return ms.value
+

@@ -27,6 +27,7 @@ SIGNATURES = {
     "kate_circuit_nqbits": [_vp, _ip],
     "kate_circuit_append_gate": [_vp, _i, _ip, _i, _i],
     "kate_circuit_append_dense": [_vp, _dp, _ip, _i],
+    "kate_circuit_append_many": [_vp, _i, _ip, _ip, _ip, _ip, _dp],
     "kate_circuit_num_gates": [_vp, _ip],
     "kate_circuit_get_gate": [_vp, _i, _ip, _ip, _ip, _ip, _dp],
     "kate_circuit_schedule": [_vp],
@@ -73,7 +74,30 @@ SIGNATURES = {
     "kate_plan_block_images": [_vp, _vp, _c.c_size_t, _c.POINTER(_c.c_size_t)],
     "kate_plan_get_smem_op": [_vp, _i, _ip, _u64p, _dp],
     "kate_proba_state_noalloc": [_vp, _i, _ip, _ip, _dp, _vp],
+    "kate_batch_options_default": [_vp],
+    "kate_batch_autotune": [_vpp, _i, _i, _i, _vp],
+    "kate_batch_create": [_vpp, _i, _i, _i, _vp, _vpp],
+    "kate_batch_destroy": [_vp],
+    "kate_batch_run_async": [_vp, _vp],
+    "kate_batch_synchronize": [_vp],
+    "kate_batch_run": [_vp],
+    "kate_batch_expect_z": [_vp, _dp],
+    "kate_batch_num_outputs": [_vp, _c.POINTER(_c.c_longlong)],
+    "kate_batch_info": [_vp, _c.POINTER(_c.c_longlong)],
+    "kate_batch_time": [_vp, _i, _c.POINTER(_c.c_float)],
 }
+
+KATE_BATCH_MAX_QUBITS = 24
+
+
+class BatchTuning(_c.Structure):
+    _fields_ = [("fusion", _c.c_int), ("max_gates", _c.c_int)]
+
+
+class BatchOptions(_c.Structure):
+    """kate_batch_options (include/kate_b200.h)."""
+    _fields_ = [("chunk", _c.c_int), ("zchunks", _c.c_int), ("window_bytes", _c.c_ulonglong),
+                ("tune", BatchTuning * (KATE_BATCH_MAX_QUBITS + 1))]
 _RET = {"kate_last_error": _c.c_char_p, "kate_version": _c.c_char_p}
 
 

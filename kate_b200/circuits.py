@@ -96,16 +96,53 @@ def brickwork_su4(n: int, layers: int, seed: int = 1234) -> List[Tuple]:
     return gates
 
 
-def hea(n: int, depth: int, seed: int = 1234) -> List[Tuple]:
-    rng = SplitMix64(seed)
-    gates = []
+def splitmix_angles(seed: int, count: int) -> np.ndarray:
+    """The first `count` SplitMix64(seed).angle() values, vectorised."""
+    k = np.arange(1, count + 1, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        z = np.uint64(seed & MASK64) + k * np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    return 2.0 * math.pi * ((z >> np.uint64(11)).astype(np.float64) * (1.0 / (1 << 53)))
+
+
+def hea_flat(n: int, depth: int, seed: int = 1234):
+    """``hea`` as flat arrays (ids, nqs, qbits, optargs, dense) for
+    Circuit.appendFlat: per layer RY(theta_q) for every q, RZ(phi_q) for
+    every q, then CZ on (a, a+1), a = l % 2, l % 2 + 2, ..."""
+    ang = splitmix_angles(seed, 2 * n * depth).reshape(depth, 2, n)
+    ids, nqs, qb, dense = [], [], [], []
+    cz = CZ.ravel()
     for l in range(depth):
-        for q in range(n):
-            gates.append((0, [q], 0, ry(rng.angle())))
-        for q in range(n):
-            gates.append((0, [q], 0, rz(rng.angle())))
-        for a in range(l % 2, n - 1, 2):
-            gates.append((0, [a, a + 1], 0, CZ))
+        t = ang[l, 0] / 2
+        c, s_ = np.cos(t), np.sin(t)
+        ryd = np.stack([c, -s_, s_, c], axis=1).astype(np.complex128)
+        p = ang[l, 1] / 2
+        rzd = np.zeros((n, 4), dtype=np.complex128)
+        rzd[:, 0] = np.cos(-p) + 1j * np.sin(-p)
+        rzd[:, 3] = np.cos(p) + 1j * np.sin(p)
+        pairs = list(range(l % 2, n - 1, 2))
+        ids += [0] * (2 * n + len(pairs))
+        nqs += [1] * (2 * n) + [2] * len(pairs)
+        qb += list(range(n)) + list(range(n))
+        for a in pairs:
+            qb += [a, a + 1]
+        dense += [ryd.ravel(), rzd.ravel()] + [cz] * len(pairs)
+    nops = len(ids)
+    return (np.array(ids, np.int32), np.array(nqs, np.int32), np.array(qb, np.int32), np.zeros(nops, np.int32),
+            np.concatenate(dense))
+
+
+def hea(n: int, depth: int, seed: int = 1234) -> List[Tuple]:
+    ids, nqs, qb, _, dense = hea_flat(n, depth, seed)
+    gates, qo, do = [], 0, 0
+    for k in range(len(ids)):
+        q = [int(x) for x in qb[qo:qo + nqs[k]]]
+        dim = 1 << int(nqs[k])
+        gates.append((0, q, 0, dense[do:do + dim * dim].reshape(dim, dim).copy()))
+        qo += int(nqs[k])
+        do += dim * dim
     return gates
 
 

@@ -1,0 +1,535 @@
+// Batched execution. See batch.hpp and k_batch.cu.
+#include "batch.hpp"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstring>
+#include <map>
+#include <thread>
+
+#include "launch.hpp"
+#include "plan.hpp"
+
+namespace kate {
+
+namespace {
+
+std::string cuda_err(const char* what, cudaError_t e) {
+    return std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+}
+#define KCHECK(call)                                       \
+    do {                                                   \
+        cudaError_t e_ = (call);                           \
+        if (e_ != cudaSuccess) return cuda_err(#call, e_); \
+    } while (0)
+
+const BatchTune kDefaultTune{};
+
+// One circuit, planned and packed. Offsets are local to the circuit until
+// the packs are concatenated.
+struct CircPack {
+    std::string err;
+    int n_out = 0;   // the circuit's qubits: one <Z> output each
+    int n_sim = 0;   // qubits simulated (narrow circuits are padded to a full tile)
+    bool small = false;
+    std::vector<uint8_t> zbit;
+    std::vector<BatchProg> progs;
+    std::vector<uint8_t> blob;
+    std::vector<DevOp> sops;
+    std::vector<Cx> pool;
+    std::vector<std::pair<uint64_t, int>> generic;  // (blob offset, count) of DevOp arrays
+};
+
+uint64_t put_bytes(std::vector<uint8_t>& blob, const void* p, size_t bytes) {
+    const size_t off = (blob.size() + 15) & ~size_t(15);
+    blob.resize(off + bytes);
+    if (bytes) std::memcpy(blob.data() + off, p, bytes);
+    return off;
+}
+
+std::string pack_circuit(const Program& in, const BatchTune& tune, CircPack& out) {
+    Program p = in;
+    const int n = p.nqbits;
+    if (n < 1 || n > KATE_BATCH_MAX_QUBITS) return "batch circuits have 1 to 24 qubits";
+    out.n_out = n;
+    out.small = n <= KATE_BATCH_SMALL_MAX;
+    std::string e;
+    if (p.instructions.empty() && p.groups.empty() && tune.fusion >= 2) {
+        e = pass_schedule(p);
+        if (e.empty()) e = pass_fuse(p, tune.fusion, 1e-6);
+        if (!e.empty()) return e;
+    }
+    if (n < KATE_TILE_BITS) {
+        // Idle qubits n..11 fill the tile; they stay |0> and have no output.
+        p.nqbits = KATE_TILE_BITS;
+        if (!p.instructions.empty())
+            for (int q = n; q < KATE_TILE_BITS; q++) {
+                p.initial_permutation.push_back(q);
+                p.final_inverse_permutation.push_back(q);
+            }
+    }
+    if (p.instructions.empty()) {
+        e = pass_compile_default(p, 0, p.nqbits);
+        if (!e.empty()) return e;
+    }
+    out.n_sim = p.nqbits;
+    PlanOptions o;
+    o.max_tile = KATE_TILE_BITS;
+    o.coalesce = 4;
+    o.remap = !out.small;  // a resident tile is never written back, so it keeps its layout
+    o.fuse_1q = true;
+    o.staged = true;
+    o.c64 = false;
+    o.max_gates_per_pass = std::max(1, tune.max_gates);
+    Plan plan;
+    e = build_plan(p, o, &plan);
+    if (!e.empty()) return e;
+    for (int x = 0; x < n; x++) out.zbit.push_back((uint8_t)plan.final_phys[plan.label_to_logical[x]]);
+    out.pool = plan.pool;
+    out.sops = plan.smem_ops;
+    auto header = [&](const PlannedPass* pp, BatchProg& bp) {
+        if (pp) {
+            DevPass dp = to_devpass(out.n_sim, *pp, 0);
+            bp.m = dp.m;
+            bp.ncb = dp.ncb;
+            std::memcpy(bp.tphys, dp.tphys, 16);
+            std::memcpy(bp.outsrc, dp.outsrc, 16);
+            std::memcpy(bp.cphys, dp.cphys, 48);
+        } else {  // identity pass on the natural layout
+            bp.m = KATE_TILE_BITS;
+            bp.ncb = out.n_sim - KATE_TILE_BITS;
+            for (int t = 0; t < KATE_TILE_BITS; t++) bp.tphys[t] = bp.outsrc[t] = (uint8_t)t;
+            for (int b = 0; b < bp.ncb; b++) bp.cphys[b] = (uint8_t)(KATE_TILE_BITS + b);
+        }
+    };
+    for (const PlannedPass& pp : plan.passes) {
+        BatchProg bp{};
+        header(&pp, bp);
+        if (bp.m != KATE_TILE_BITS) return "internal: batch pass tile is not 12 qubits";
+        if (!out.small && bp.tphys[0] != 0) return "internal: batch pass tile does not hold physical bit 0";
+        if (pp.prog) {
+            const PassProg& P = *pp.prog;
+            bp.nops = P.nops;
+            bp.nmats = P.nmats;
+            bp.nstages = P.nstages;
+            bp.sop0 = P.sop0;
+            for (int k = 0; k < P.nops; k++)
+                if (P.ops[k].kind == SOP_SMEM) bp.flags |= BPROG_SMEM;
+            bp.ops_off = put_bytes(out.blob, P.ops, sizeof(SOp) * P.nops);
+            bp.mats_off = put_bytes(out.blob, P.mats, sizeof(double) * 2 * P.nmats);
+            bp.stab_off = put_bytes(out.blob, P.stab, sizeof(uint16_t) * 44 * P.nstages);
+        } else {
+            bp.nops = (int)pp.ops.size();
+            bp.nstages = -1;
+            bp.ops_off = put_bytes(out.blob, pp.ops.data(), sizeof(DevOp) * pp.ops.size());
+            out.generic.push_back({bp.ops_off, bp.nops});
+        }
+        out.progs.push_back(bp);
+    }
+    if (out.progs.empty() && !out.small) {
+        BatchProg bp{};
+        header(nullptr, bp);
+        out.progs.push_back(bp);
+    }
+    return "";
+}
+
+// Plans every circuit on host threads.
+std::vector<CircPack> pack_all(const std::vector<const Program*>& circuits, const BatchOptions& opt) {
+    std::vector<CircPack> packs(circuits.size());
+    std::atomic<size_t> next{0};
+    auto work = [&]() {
+        for (size_t i; (i = next.fetch_add(1)) < circuits.size();) {
+            const BatchTune& tu = opt.for_n(circuits[i]->nqbits);
+            try {
+                packs[i].err = pack_circuit(*circuits[i], tu, packs[i]);
+            } catch (const std::exception& ex) {
+                packs[i].err = ex.what();
+            }
+        }
+    };
+    unsigned nt = std::thread::hardware_concurrency();
+    nt = std::max(1u, std::min(nt, 32u));
+    if (circuits.size() < 8) nt = 1;
+    std::vector<std::thread> th;
+    for (unsigned k = 1; k < nt; k++) th.emplace_back(work);
+    work();
+    for (auto& x : th) x.join();
+    return packs;
+}
+
+}  // namespace
+
+const BatchTune& BatchOptions::for_n(int n) const {
+    if (n >= 0 && (size_t)n < tune.size() && tune[n].fusion >= 1 && tune[n].max_gates >= 1) return tune[n];
+    return kDefaultTune;
+}
+
+struct BatchImpl {
+    int device = 0;
+    int precision = 1;
+    int ncirc = 0;
+    int64_t nout = 0;
+    uint64_t arena_amps = 0;
+    int grid = 0;
+    std::vector<BatchTask> tasks;
+    std::vector<BatchCirc> circs;
+    std::vector<BatchProg> progs;
+    std::vector<uint8_t> blob;
+    std::vector<DevOp> sops;
+    std::vector<Cx> pool;
+    void* d_arena = nullptr;
+    BatchTask* d_tasks = nullptr;
+    BatchCirc* d_circs = nullptr;
+    BatchProg* d_progs = nullptr;
+    void* d_blob = nullptr;
+    DevOp* d_sops = nullptr;
+    void* d_pool = nullptr;
+    int* d_head = nullptr;
+    int* d_done = nullptr;
+    double* d_zout = nullptr;
+    int* d_err = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+
+    size_t amp_bytes() const { return precision == 0 ? 16 : 8; }
+
+    void release() {
+        cudaSetDevice(device);
+        if (stream) cudaStreamSynchronize(stream);
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        cudaFree(d_arena);
+        cudaFree(d_tasks);
+        cudaFree(d_circs);
+        cudaFree(d_progs);
+        cudaFree(d_blob);
+        cudaFree(d_sops);
+        cudaFree(d_pool);
+        cudaFree(d_head);
+        cudaFree(d_done);
+        cudaFree(d_zout);
+        cudaFree(d_err);
+        if (stream) cudaStreamDestroy(stream);
+        exec = nullptr;
+        graph = nullptr;
+        stream = nullptr;
+    }
+
+    template <typename T>
+    std::string upload(T** dptr, const std::vector<T>& v, const char* what) {
+        const size_t bytes = std::max<size_t>(16, v.size() * sizeof(T));
+        cudaError_t e = cudaMalloc((void**)dptr, bytes);
+        if (e != cudaSuccess) return cuda_err(what, e);
+        if (!v.empty()) {
+            e = cudaMemcpy(*dptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) return cuda_err(what, e);
+        }
+        return "";
+    }
+};
+
+std::string Batch::create(const std::vector<const Program*>& circuits, int precision, int device,
+                          const BatchOptions& opt, Batch** out) {
+    if (precision != 0 && precision != 1) return "unknown precision";
+    if (circuits.empty()) return "empty batch";
+    for (const Program* p : circuits)
+        if (!p) return "null circuit";
+    const int chunk = std::max(1, opt.chunk), zchunks = std::max(1, opt.zchunks);
+    std::vector<CircPack> packs = pack_all(circuits, opt);
+    for (size_t i = 0; i < packs.size(); i++)
+        if (!packs[i].err.empty()) return "circuit " + std::to_string(i) + ": " + packs[i].err;
+
+    auto* S = new BatchImpl();
+    auto fail = [&](const std::string& e) {
+        S->release();
+        delete S;
+        return e;
+    };
+    S->device = device;
+    S->precision = precision;
+    S->ncirc = (int)circuits.size();
+
+    // Concatenate the packs; lay the large states out in the arena.
+    std::vector<int> prog0(packs.size());
+    for (size_t i = 0; i < packs.size(); i++) {
+        CircPack& P = packs[i];
+        const uint64_t bbase = (S->blob.size() + 15) & ~uint64_t(15);
+        S->blob.resize(bbase);
+        S->blob.insert(S->blob.end(), P.blob.begin(), P.blob.end());
+        const int64_t pbase = (int64_t)S->pool.size();
+        const int sbase = (int)S->sops.size();
+        for (auto& g : P.generic) {
+            DevOp* ops = reinterpret_cast<DevOp*>(S->blob.data() + bbase + g.first);
+            for (int k = 0; k < g.second; k++) ops[k].mat += pbase;
+        }
+        for (DevOp d : P.sops) {
+            d.mat += pbase;
+            S->sops.push_back(d);
+        }
+        S->pool.insert(S->pool.end(), P.pool.begin(), P.pool.end());
+        prog0[i] = (int)S->progs.size();
+        for (BatchProg bp : P.progs) {
+            bp.ops_off += bbase;
+            bp.mats_off += bbase;
+            bp.stab_off += bbase;
+            bp.sop0 += sbase;
+            S->progs.push_back(bp);
+        }
+        BatchCirc bc{};
+        bc.n = P.n_out;
+        bc.zoff = (int32_t)S->nout;
+        S->nout += P.n_out;
+        for (int x = 0; x < P.n_out; x++) bc.zbit[x] = P.zbit[x];
+        if (!P.small) {
+            bc.off = S->arena_amps;
+            S->arena_amps += 1ull << P.n_sim;
+        }
+        S->circs.push_back(bc);
+        std::vector<uint8_t>().swap(P.blob);
+        std::vector<Cx>().swap(P.pool);
+        std::vector<DevOp>().swap(P.sops);
+    }
+    if (S->nout > INT32_MAX) return fail("too many outputs");
+    if (S->sops.size() > (size_t)INT32_MAX) return fail("too many shared-memory ops");
+
+    // Task queue. Large circuits, window by window, level by level; small
+    // circuits spread evenly between them (they depend on nothing, so they
+    // fill the waits at level boundaries).
+    std::vector<int> large, small;
+    for (size_t i = 0; i < packs.size(); i++) (packs[i].small ? small : large).push_back((int)i);
+    std::vector<BatchTask> ltasks;
+    {
+        size_t w0 = 0;
+        while (w0 < large.size()) {
+            size_t w1 = w0;
+            uint64_t bytes = 0;
+            do {
+                bytes += (1ull << packs[large[w1]].n_sim) * S->amp_bytes();
+                w1++;
+            } while (w1 < large.size() && (opt.window_bytes == 0 ||
+                                           bytes + (1ull << packs[large[w1]].n_sim) * S->amp_bytes() <= opt.window_bytes));
+            std::vector<int> need(large.size(), 0);
+            size_t maxlev = 0;
+            for (size_t k = w0; k < w1; k++) maxlev = std::max(maxlev, packs[large[k]].progs.size() + 1);
+            for (size_t lev = 0; lev < maxlev; lev++)
+                for (size_t k = w0; k < w1; k++) {
+                    const int ci = large[k];
+                    const CircPack& P = packs[ci];
+                    const size_t np = P.progs.size();
+                    if (lev > np) continue;
+                    const int before = need[k];
+                    if (lev < np) {
+                        const uint32_t ncos = 1u << (P.n_sim - KATE_TILE_BITS);
+                        for (uint32_t c0 = 0; c0 < ncos; c0 += chunk) {
+                            BatchTask t{};
+                            t.kind = BT_PASS;
+                            t.circ = ci;
+                            t.prog = prog0[ci] + (int)lev;
+                            t.c0 = c0;
+                            t.c1 = std::min<uint32_t>(ncos, c0 + chunk);
+                            t.need = before;
+                            t.first = lev == 0;
+                            ltasks.push_back(t);
+                            need[k]++;
+                        }
+                    } else {
+                        const uint32_t nch = (uint32_t)std::max<uint64_t>(1, (1ull << P.n_sim) >> 16);
+                        for (uint32_t c0 = 0; c0 < nch; c0 += zchunks) {
+                            BatchTask t{};
+                            t.kind = BT_ZRED;
+                            t.circ = ci;
+                            t.c0 = c0;
+                            t.c1 = std::min<uint32_t>(nch, c0 + zchunks);
+                            t.need = before;
+                            ltasks.push_back(t);
+                            need[k]++;
+                        }
+                    }
+                }
+            w0 = w1;
+        }
+    }
+    {
+        const size_t L = ltasks.size(), Sn = small.size();
+        size_t li = 0;
+        for (size_t s = 0; s < Sn; s++) {
+            // Large tasks due before small task s.
+            const size_t upto = L * s / Sn;
+            while (li < upto) S->tasks.push_back(ltasks[li++]);
+            BatchTask t{};
+            t.kind = BT_SMALL;
+            t.circ = small[s];
+            t.prog = prog0[small[s]];
+            t.nprog = (int)packs[small[s]].progs.size();
+            S->tasks.push_back(t);
+        }
+        while (li < L) S->tasks.push_back(ltasks[li++]);
+    }
+    if (S->tasks.size() > (size_t)INT32_MAX) return fail("too many tasks");
+
+    // Device side.
+    cudaError_t ce = cudaSetDevice(device);
+    if (ce != cudaSuccess) return fail(cuda_err("cudaSetDevice", ce));
+    ce = cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking);
+    if (ce != cudaSuccess) return fail(cuda_err("cudaStreamCreate", ce));
+    std::string e;
+    if ((e = S->upload(&S->d_tasks, S->tasks, "cudaMalloc(tasks)")) != "") return fail(e);
+    if ((e = S->upload(&S->d_circs, S->circs, "cudaMalloc(circuits)")) != "") return fail(e);
+    if ((e = S->upload(&S->d_progs, S->progs, "cudaMalloc(programs)")) != "") return fail(e);
+    if ((e = S->upload(&S->d_sops, S->sops, "cudaMalloc(smem ops)")) != "") return fail(e);
+    {
+        uint8_t* b = nullptr;
+        if ((e = S->upload(&b, S->blob, "cudaMalloc(program blob)")) != "") return fail(e);
+        S->d_blob = b;
+        Cx* p = nullptr;
+        if ((e = S->upload(&p, S->pool, "cudaMalloc(matrix pool)")) != "") return fail(e);
+        S->d_pool = p;
+    }
+    ce = cudaMalloc(&S->d_arena, std::max<uint64_t>(16, S->arena_amps * S->amp_bytes()));
+    if (ce != cudaSuccess) return fail(cuda_err("cudaMalloc(state arena)", ce));
+    ce = cudaMalloc((void**)&S->d_head, sizeof(int));
+    if (ce != cudaSuccess) return fail(cuda_err("cudaMalloc(queue head)", ce));
+    ce = cudaMalloc((void**)&S->d_done, sizeof(int) * S->ncirc);
+    if (ce != cudaSuccess) return fail(cuda_err("cudaMalloc(counters)", ce));
+    ce = cudaMalloc((void**)&S->d_zout, sizeof(double) * std::max<int64_t>(1, S->nout));
+    if (ce != cudaSuccess) return fail(cuda_err("cudaMalloc(outputs)", ce));
+    ce = cudaMalloc((void**)&S->d_err, sizeof(int));
+    if (ce != cudaSuccess) return fail(cuda_err("cudaMalloc(error flag)", ce));
+    ce = cudaMemset(S->d_err, 0, sizeof(int));
+    if (ce != cudaSuccess) return fail(cuda_err("cudaMemset(error flag)", ce));
+    S->grid = batch_grid(device, precision);
+    const int grid = (int)std::min<size_t>((size_t)S->grid, S->tasks.size());
+
+    // One graph: reset queue, counters and outputs, then the kernel.
+    ce = cudaStreamBeginCapture(S->stream, cudaStreamCaptureModeThreadLocal);
+    if (ce != cudaSuccess) return fail(cuda_err("cudaStreamBeginCapture", ce));
+    cudaMemsetAsync(S->d_head, 0, sizeof(int), S->stream);
+    cudaMemsetAsync(S->d_done, 0, sizeof(int) * S->ncirc, S->stream);
+    cudaMemsetAsync(S->d_zout, 0, sizeof(double) * std::max<int64_t>(1, S->nout), S->stream);
+    cudaError_t le = launch_batch(S->d_arena, precision, S->d_tasks, (int)S->tasks.size(), S->d_circs, S->d_progs,
+                                  S->d_blob, S->d_sops, S->d_pool, S->d_head, S->d_done, S->d_zout, S->d_err, grid,
+                                  S->stream);
+    ce = cudaStreamEndCapture(S->stream, &S->graph);
+    if (le != cudaSuccess) return fail(cuda_err("launch_batch", le));
+    if (ce != cudaSuccess) return fail(cuda_err("cudaStreamEndCapture", ce));
+    ce = cudaGraphInstantiate(&S->exec, S->graph, 0);
+    if (ce != cudaSuccess) return fail(cuda_err("cudaGraphInstantiate", ce));
+    // Host copies are no longer needed.
+    std::vector<uint8_t>().swap(S->blob);
+    std::vector<Cx>().swap(S->pool);
+    std::vector<DevOp>().swap(S->sops);
+    auto* b = new Batch();
+    b->d_ = S;
+    *out = b;
+    return "";
+}
+
+Batch::~Batch() {
+    if (!d_) return;
+    d_->release();
+    delete d_;
+}
+
+std::string Batch::run_async(void* stream) {
+    KCHECK(cudaSetDevice(d_->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : d_->stream;
+    KCHECK(cudaGraphLaunch(d_->exec, st));
+    if (st != d_->stream) {
+        cudaEvent_t ev;
+        KCHECK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        KCHECK(cudaEventRecord(ev, st));
+        KCHECK(cudaStreamWaitEvent(d_->stream, ev, 0));
+        cudaEventDestroy(ev);
+    }
+    return "";
+}
+
+std::string Batch::synchronize() {
+    KCHECK(cudaSetDevice(d_->device));
+    KCHECK(cudaStreamSynchronize(d_->stream));
+    int err = 0;
+    KCHECK(cudaMemcpy(&err, d_->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) {
+        cudaMemset(d_->d_err, 0, sizeof(int));
+        return "batch kernel: a dependency wait timed out; outputs are incomplete";
+    }
+    return "";
+}
+
+std::string Batch::expect_z(double* out) {
+    std::string e = synchronize();
+    if (!e.empty()) return e;
+    KCHECK(cudaMemcpy(out, d_->d_zout, sizeof(double) * d_->nout, cudaMemcpyDeviceToHost));
+    return "";
+}
+
+std::string Batch::time_runs(int runs, float* ms_avg) {
+    KCHECK(cudaSetDevice(d_->device));
+    cudaEvent_t a, b;
+    KCHECK(cudaEventCreate(&a));
+    KCHECK(cudaEventCreate(&b));
+    KCHECK(cudaEventRecord(a, d_->stream));
+    for (int r = 0; r < runs; r++) KCHECK(cudaGraphLaunch(d_->exec, d_->stream));
+    KCHECK(cudaEventRecord(b, d_->stream));
+    std::string e = synchronize();
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (!e.empty()) return e;
+    *ms_avg = ms / std::max(1, runs);
+    return "";
+}
+
+int64_t Batch::num_outputs() const { return d_->nout; }
+int64_t Batch::num_tasks() const { return (int64_t)d_->tasks.size(); }
+uint64_t Batch::arena_bytes() const { return d_->arena_amps * d_->amp_bytes(); }
+int Batch::grid() const { return d_->grid; }
+int64_t Batch::num_programs() const { return (int64_t)d_->progs.size(); }
+
+std::string batch_autotune(const std::vector<const Program*>& circuits, int precision, int device,
+                           BatchOptions* opt) {
+    if (opt->tune.size() < KATE_BATCH_MAX_QUBITS + 1) opt->tune.resize(KATE_BATCH_MAX_QUBITS + 1, BatchTune{0, 0});
+    std::map<int, std::vector<const Program*>> byn;
+    for (const Program* p : circuits)
+        if (p) byn[p->nqbits].push_back(p);
+    static const int kFusion[] = {1, 2, 3};
+    static const int kGates[] = {64, 96, 128};
+    for (auto& kv : byn) {
+        const int n = kv.first;
+        const int nsim = std::max(n, KATE_TILE_BITS);
+        // A sample of about 2^27 amplitudes of state (at most 512 circuits).
+        size_t cnt = (size_t)std::max<uint64_t>(1, (1ull << 27) >> nsim);
+        cnt = std::min<size_t>({cnt, kv.second.size(), 512});
+        std::vector<const Program*> sample(kv.second.begin(), kv.second.begin() + cnt);
+        float best = 0.f;
+        BatchTune bt = kDefaultTune;
+        bool found = false;
+        for (int f : kFusion)
+            for (int g : kGates) {
+                BatchOptions o = *opt;
+                o.tune[n] = BatchTune{f, g};
+                Batch* b = nullptr;
+                if (!Batch::create(sample, precision, device, o, &b).empty()) continue;
+                float ms = 0.f;
+                std::string e = b->time_runs(1, &ms);
+                if (e.empty()) e = b->time_runs(3, &ms);
+                delete b;
+                if (!e.empty()) return e;
+                if (!found || ms < best) {
+                    best = ms;
+                    bt = BatchTune{f, g};
+                    found = true;
+                }
+            }
+        if (!found) return "autotune: no candidate plan for " + std::to_string(n) + "-qubit circuits";
+        opt->tune[n] = bt;
+    }
+    return "";
+}
+
+}  // namespace kate

@@ -5,6 +5,7 @@
 #include <exception>
 #include <string>
 
+#include "batch.hpp"
 #include "circuit.hpp"
 #include "plan.hpp"
 #include "sim.hpp"
@@ -14,6 +15,9 @@ struct kate_circuit {
 };
 struct kate_sim {
     kate::Simulator* sim = nullptr;
+};
+struct kate_batch {
+    kate::Batch* b = nullptr;
 };
 struct kate_plan {
     kate::Plan plan;
@@ -128,6 +132,44 @@ kate_status kate_circuit_append_dense(kate_circuit* c, const double* mat, const 
         std::string e = kate::validate_gate(c->prog, g);
         if (!e.empty()) return fail(e.find("after gateGrouping") != std::string::npos ? KATE_ESTATE : KATE_EINVAL, e);
         c->prog.gates.push_back(std::move(g));
+        return KATE_OK;
+    });
+}
+
+kate_status kate_circuit_append_many(kate_circuit* c, int count, const int* ids, const int* nqs, const int* qbits,
+                                     const int* optargs, const double* dense) {
+    return guarded([&] {
+        REQUIRE(c && count >= 0, "null pointer");
+        if (count == 0) return KATE_OK;
+        REQUIRE(ids && nqs && qbits, "null pointer");
+        kate::Program tmp;
+        tmp.nqbits = c->prog.nqbits;
+        std::vector<kate::Gate> add;
+        add.reserve(count);
+        size_t qo = 0, dofs = 0;
+        for (int i = 0; i < count; i++) {
+            const int nq = nqs[i];
+            REQUIRE(nq >= 1 && nq <= 10, "gates take 1 to 10 qubits");
+            kate::Gate g;
+            g.id = ids[i];
+            g.qbits.assign(qbits + qo, qbits + qo + nq);
+            qo += nq;
+            g.optarg = optargs ? optargs[i] : 0;
+            if (g.id == kate::G_DENSE) {
+                REQUIRE(dense, "dense gates need matrix entries");
+                const size_t len = (size_t)1 << (2 * nq);
+                g.dense.resize(len);
+                for (size_t k = 0; k < len; k++) g.dense[k] = kate::Cx(dense[2 * (dofs + k)], dense[2 * (dofs + k) + 1]);
+                dofs += len;
+                g.optarg = 0;
+            }
+            std::string e = kate::validate_gate(c->prog, g);
+            if (!e.empty())
+                return fail(e.find("after gateGrouping") != std::string::npos ? KATE_ESTATE : KATE_EINVAL,
+                            "gate " + std::to_string(i) + ": " + e);
+            add.push_back(std::move(g));
+        }
+        for (auto& g : add) c->prog.gates.push_back(std::move(g));
         return KATE_OK;
     });
 }
@@ -566,6 +608,140 @@ kate_status kate_plan_final_layout(const kate_plan* p, int* phys, int* l2l) {
         l2l[q] = p->plan.label_to_logical[q];
     }
     return KATE_OK;
+}
+
+// ---- batches ----
+
+namespace {
+kate::BatchOptions to_options(const kate_batch_options* o) {
+    kate::BatchOptions r;
+    if (!o) return r;
+    if (o->chunk > 0) r.chunk = o->chunk;
+    if (o->zchunks > 0) r.zchunks = o->zchunks;
+    r.window_bytes = o->window_bytes;
+    r.tune.resize(KATE_BATCH_MAX_QUBITS + 1);
+    for (int n = 0; n <= KATE_BATCH_MAX_QUBITS; n++) {
+        r.tune[n].fusion = o->tune[n].fusion;
+        r.tune[n].max_gates = o->tune[n].max_gates;
+    }
+    return r;
+}
+
+std::vector<const kate::Program*> programs(const kate_circuit* const* c, int count) {
+    std::vector<const kate::Program*> v;
+    for (int i = 0; i < count; i++) v.push_back(c[i] ? &c[i]->prog : nullptr);
+    return v;
+}
+}  // namespace
+
+kate_status kate_batch_options_default(kate_batch_options* opt) {
+    REQUIRE(opt, "null pointer");
+    std::memset(opt, 0, sizeof(*opt));
+    kate::BatchOptions d;
+    opt->chunk = d.chunk;
+    opt->zchunks = d.zchunks;
+    return KATE_OK;
+}
+
+kate_status kate_batch_autotune(const kate_circuit* const* circuits, int count, int precision, int device,
+                                kate_batch_options* opt) {
+    return guarded([&] {
+        REQUIRE(circuits && opt && count > 0, "null pointer or empty batch");
+        REQUIRE(precision == KATE_C128 || precision == KATE_C64, "unknown precision");
+        for (int i = 0; i < count; i++) REQUIRE(circuits[i], "null circuit");
+        kate::BatchOptions o = to_options(opt);
+        std::string e = kate::batch_autotune(programs(circuits, count), precision, device, &o);
+        if (!e.empty()) return sim_status(e);
+        for (int n = 0; n <= KATE_BATCH_MAX_QUBITS; n++) {
+            opt->tune[n].fusion = o.tune[n].fusion;
+            opt->tune[n].max_gates = o.tune[n].max_gates;
+        }
+        return KATE_OK;
+    });
+}
+
+kate_status kate_batch_create(const kate_circuit* const* circuits, int count, int precision, int device,
+                              const kate_batch_options* opt, kate_batch** out) {
+    return guarded([&] {
+        REQUIRE(circuits && out && count > 0, "null pointer or empty batch");
+        REQUIRE(precision == KATE_C128 || precision == KATE_C64, "unknown precision");
+        for (int i = 0; i < count; i++) REQUIRE(circuits[i], "null circuit");
+        kate::Batch* b = nullptr;
+        std::string e = kate::Batch::create(programs(circuits, count), precision, device, to_options(opt), &b);
+        if (!e.empty()) return sim_status(e);
+        auto* h = new kate_batch();
+        h->b = b;
+        *out = h;
+        return KATE_OK;
+    });
+}
+
+kate_status kate_batch_destroy(kate_batch* b) {
+    if (b) {
+        delete b->b;
+        delete b;
+    }
+    return KATE_OK;
+}
+
+kate_status kate_batch_run_async(kate_batch* b, void* stream) {
+    return guarded([&] {
+        REQUIRE(b, "null batch");
+        return sim_status(b->b->run_async(stream));
+    });
+}
+
+kate_status kate_batch_synchronize(kate_batch* b) {
+    return guarded([&] {
+        REQUIRE(b, "null batch");
+        std::string e = b->b->synchronize();
+        if (!e.empty()) return fail(KATE_ECUDA, e);
+        return KATE_OK;
+    });
+}
+
+kate_status kate_batch_run(kate_batch* b) {
+    return guarded([&] {
+        REQUIRE(b, "null batch");
+        std::string e = b->b->run_async(nullptr);
+        if (!e.empty()) return sim_status(e);
+        e = b->b->synchronize();
+        if (!e.empty()) return fail(KATE_ECUDA, e);
+        return KATE_OK;
+    });
+}
+
+kate_status kate_batch_expect_z(kate_batch* b, double* out) {
+    return guarded([&] {
+        REQUIRE(b && out, "null pointer");
+        std::string e = b->b->expect_z(out);
+        if (!e.empty()) return fail(KATE_ECUDA, e);
+        return KATE_OK;
+    });
+}
+
+kate_status kate_batch_num_outputs(const kate_batch* b, long long* out) {
+    REQUIRE(b && out, "null pointer");
+    *out = (long long)b->b->num_outputs();
+    return KATE_OK;
+}
+
+kate_status kate_batch_info(const kate_batch* b, long long* info) {
+    REQUIRE(b && info, "null pointer");
+    info[0] = (long long)b->b->num_tasks();
+    info[1] = (long long)b->b->num_programs();
+    info[2] = (long long)b->b->arena_bytes();
+    info[3] = (long long)b->b->grid();
+    return KATE_OK;
+}
+
+kate_status kate_batch_time(kate_batch* b, int runs, float* ms) {
+    return guarded([&] {
+        REQUIRE(b && ms && runs > 0, "null pointer or no runs");
+        std::string e = b->b->time_runs(runs, ms);
+        if (!e.empty()) return fail(KATE_ECUDA, e);
+        return KATE_OK;
+    });
 }
 
 }  // extern "C"

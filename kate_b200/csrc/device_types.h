@@ -121,3 +121,51 @@ typedef struct {
     uint8_t btb[KATE_C64_MAX_BLOCKS][8];
     uint64_t bimg[KATE_C64_MAX_BLOCKS];
 } BlockProg;
+
+// ---- batched execution (k_batch.cu) ----
+// A batch is a task list run by one persistent kernel. SMALL tasks simulate
+// a whole circuit of at most KATE_BATCH_SMALL_MAX qubits (narrower circuits
+// are padded with idle qubits) in one CTA's shared memory: |0...0>, every
+// pass program back to back on the same tile, then <Z_q>. PASS tasks run one
+// group pass over a range of cosets of a larger circuit's state; ZRED tasks
+// add a range of a finished state's amplitudes into its <Z_q> outputs. Tasks
+// are queued level by level (pass index) per circuit, and a task waits until
+// `need` tasks of its circuit have finished, so it only ever waits on tasks
+// taken from the queue before it.
+#define KATE_BATCH_SMALL_MAX 12
+#define KATE_BATCH_MAX_QUBITS 24
+#define BT_SMALL 0
+#define BT_PASS 1
+#define BT_ZRED 2
+
+typedef struct {
+    int32_t kind;
+    int32_t circ;
+    int32_t prog;     // BT_PASS: program index; BT_SMALL: first program index
+    int32_t nprog;    // BT_SMALL: programs run back to back
+    uint32_t c0, c1;  // BT_PASS: coset range; BT_ZRED: range of 2^16-amplitude chunks
+    int32_t need;     // finished tasks of this circuit required before starting
+    int32_t first;    // BT_PASS: the input is |0...0> (nothing is loaded)
+} BatchTask;
+
+typedef struct {
+    uint64_t off;     // state offset in the arena (amplitudes)
+    int32_t n;        // <Z> outputs (the circuit's qubits)
+    int32_t zoff;     // first <Z> output of this circuit
+    uint8_t zbit[40]; // output q reads bit zbit[q] of the tile (SMALL) or state (otherwise)
+} BatchCirc;
+
+// A pass program in the batch's program blob: a register-staged program
+// (nstages >= 0: SOp ops, double[2] matrices, stage tables) or, when none
+// could be built, a generic one (nstages < 0: DevOp ops run on the shared
+// tile one by one). Offsets are in bytes from the blob's start.
+#define BPROG_SMEM 1  // BatchProg.flags: the staged program has SOP_SMEM ops
+
+typedef struct {
+    int32_t m, ncb, nops, nmats, nstages, sop0;  // sop0: first shared-memory op in the batch's array
+    int32_t flags, pad;
+    uint8_t tphys[16];
+    uint8_t outsrc[16];
+    uint8_t cphys[48];
+    uint64_t ops_off, mats_off, stab_off;
+} BatchProg;

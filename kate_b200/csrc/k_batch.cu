@@ -1,0 +1,313 @@
+// Persistent batch kernel: many independent circuits in one launch.
+//
+// CTAs take tasks from a global queue (one atomicAdd per task). A task
+// first waits, with a time-bounded spin, until the tasks of its circuit that
+// it depends on have finished (per-circuit counters), then runs:
+//   BT_SMALL  the whole circuit in shared memory: |0...0>, every pass
+//             program back to back on the same tile, <Z_q>; the state never
+//             touches HBM;
+//   BT_PASS   one group pass program over a range of cosets: 16-byte
+//             cp.async loads (L2 only: other SMs wrote the state earlier in
+//             this launch), the register-staged program, stores that bypass
+//             L1. The first pass of a circuit starts from |0...0> in shared
+//             memory instead of loading;
+//   BT_ZRED   <Z_q> partial sums over a range of amplitudes, added to the
+//             circuit's outputs with FP64 atomics.
+// Finished tasks bump their circuit's counter after a memory fence. Tasks
+// are queued level by level per circuit, so a task waits only on tasks
+// dequeued before it: every CTA that holds a task can finish it, whatever
+// the number of resident CTAs.
+// C2 is the amplitude type: float2 (complex64, FP32 arithmetic) or double2
+// (complex128, FP64 arithmetic). <Z> sums are FP64.
+#include <cuda_runtime.h>
+
+#include "k_stage.cuh"
+#include "launch.hpp"
+
+namespace kate {
+
+namespace {
+
+using namespace stage;
+
+constexpr unsigned long long WAIT_NS = 5000000000ull;  // a dependency wait gives up after 5 s
+
+__device__ __forceinline__ unsigned long long now_ns() {
+    unsigned long long v;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(v));
+    return v;
+}
+
+__device__ __forceinline__ double2 ldst(const double2* p) { return __ldcg(p); }
+__device__ __forceinline__ double2 ldst(const float2* p) {
+    const float2 v = __ldcg(p);
+    return make_double2(v.x, v.y);
+}
+
+// Block-wide sums of per-thread values v[0..nb): result in red[NB * 8 + b].
+template <int NB>
+__device__ void block_sums(const double (&v)[NB], int nb, double* red) {
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+#pragma unroll
+    for (int b = 0; b < NB; b++) {
+        if (b >= nb) break;
+        double x = v[b];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) red[warp * NB + b] = x;
+    }
+    __syncthreads();
+    if (t < nb) {
+        double s = 0.0;
+        for (int w = 0; w < NT / 32; w++) s += red[w * NB + t];
+        red[NB * (NT / 32) + t] = s;
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ ProgView view(const BatchProg& P, const unsigned char* blob) {
+    ProgView v;
+    v.m = P.m;
+    v.ncb = P.ncb;
+    v.nops = P.nstages >= 0 ? P.nops : 0;  // generic programs run from global memory
+    v.nmats = P.nstages >= 0 ? P.nmats : 0;
+    v.nstages = P.nstages >= 0 ? P.nstages : 0;
+    v.sop0 = P.sop0;
+    v.tphys = P.tphys;
+    v.outsrc = P.outsrc;
+    v.cphys = P.cphys;
+    v.ops = reinterpret_cast<const SOp*>(blob + P.ops_off);
+    v.mats = reinterpret_cast<const double(*)[2]>(blob + P.mats_off);
+    v.stab = reinterpret_cast<const uint16_t(*)[44]>(blob + P.stab_off);
+    return v;
+}
+
+// Dynamic shared memory of the batch kernel: the tile, then its tables.
+extern __shared__ __align__(16) unsigned char batch_smem_raw[];
+
+// The register-staged program as a call of its own, so that its registers
+// are allocated apart from the task loop's. The tile and tables are taken
+// from the shared-memory symbol (shared-window addressing).
+template <typename C2, bool SM>
+__device__ __noinline__ void run_staged(int nops, uint64_t cbase, const DevOp* __restrict__ sops, int sop0,
+                                        const double2* __restrict__ pool) {
+    C2* tile = reinterpret_cast<C2*>(batch_smem_raw);
+    const TileTables<C2>& T = *reinterpret_cast<const TileTables<C2>*>(batch_smem_raw + TS * sizeof(C2));
+    const uint32_t tb = (uint32_t)__cvta_generic_to_shared(tile);
+    run_program<C2, SM>(T, nops, tb, tile, cbase, sops, sop0, pool, threadIdx.x);
+}
+
+// Runs program P (tables already in T) on the tile, for coset base cbase.
+template <typename C2>
+__device__ __forceinline__ void run_any(const TileTables<C2>& T, const BatchProg& P, const unsigned char* blob,
+                                        uint32_t tb, C2* tile, uint64_t cbase, const DevOp* __restrict__ sops,
+                                        const double2* __restrict__ pool, uint32_t t) {
+    if (P.nstages >= 0) {
+        if (P.flags & BPROG_SMEM) run_staged<C2, true>(P.nops, cbase, sops, P.sop0, pool);
+        else run_staged<C2, false>(P.nops, cbase, sops, P.sop0, pool);
+    } else {
+        const DevOp* gops = reinterpret_cast<const DevOp*>(blob + P.ops_off);
+        for (int k = 0; k < P.nops; k++) {
+            const DevOp op = gops[k];
+            ops::apply_op<C2>(tile, TB, cbase, op, pool, (int)t, NT);
+            __syncthreads();
+        }
+    }
+}
+
+// <Z_q> of a resident tile: output q reads tile bit zbit[q].
+template <typename C2>
+__device__ __noinline__ void small_z(const C2* tile, int nz, const uint8_t* zbit, double* red, double* out) {
+    const uint32_t t = threadIdx.x;
+    double z[KATE_BATCH_SMALL_MAX];
+#pragma unroll
+    for (int q = 0; q < KATE_BATCH_SMALL_MAX; q++) z[q] = 0.0;
+    for (uint32_t i = t; i < (uint32_t)TS; i += NT) {
+        const C2 a = tile[ops::tsw<C2>(i)];
+        const double p = (double)a.x * a.x + (double)a.y * a.y;
+#pragma unroll
+        for (int q = 0; q < KATE_BATCH_SMALL_MAX; q++)
+            if (q < nz) z[q] += ((i >> zbit[q]) & 1u) ? -p : p;
+    }
+    block_sums<KATE_BATCH_SMALL_MAX>(z, nz, red);
+    if ((int)t < nz) out[t] = red[KATE_BATCH_SMALL_MAX * (NT / 32) + t];
+}
+
+// <Z_q> partial sums of an n-qubit state over 2^16-amplitude chunks
+// [ch0, ch1), added to out[q] (q reads physical bit zbit[q]). Thread t takes
+// amplitudes chunk * 2^16 + t + 256 k: physical bits 0..7 come from t, 8..15
+// from k, the rest from the chunk.
+template <typename C2>
+__device__ __noinline__ void zred(const C2* st, int n, uint32_t ch0, uint32_t ch1, const uint8_t* zbit, double* red,
+                                  double* out) {
+    const uint32_t t = threadIdx.x;
+    double z[KATE_BATCH_MAX_QUBITS];
+#pragma unroll
+    for (int q = 0; q < KATE_BATCH_MAX_QUBITS; q++) z[q] = 0.0;
+    for (uint32_t ch = ch0; ch < ch1; ch++) {
+        double tot = 0.0, kb[8];
+#pragma unroll
+        for (int b = 0; b < 8; b++) kb[b] = 0.0;
+        const uint64_t x0 = (uint64_t)ch << 16;
+        for (uint32_t k = 0; k < 256; k++) {
+            const uint64_t x = x0 + t + ((uint64_t)k << 8);
+            if (x >> n) break;
+            const double2 a = ldst(st + x);
+            const double p = a.x * a.x + a.y * a.y;
+            tot += p;
+#pragma unroll
+            for (int b = 0; b < 8; b++) kb[b] += ((k >> b) & 1u) ? -p : p;
+        }
+#pragma unroll
+        for (int b = 0; b < KATE_BATCH_MAX_QUBITS; b++) {
+            if (b < 8) z[b] += ((t >> b) & 1u) ? -tot : tot;
+            else if (b < 16) z[b] += kb[b - 8];
+            else z[b] += ((ch >> (b - 16)) & 1u) ? -tot : tot;
+        }
+    }
+    block_sums<KATE_BATCH_MAX_QUBITS>(z, n, red);
+    if ((int)t < n) atomicAdd(out + t, red[KATE_BATCH_MAX_QUBITS * (NT / 32) + zbit[t]]);
+}
+
+template <typename C2>
+__device__ __forceinline__ void init_basis0(C2* tile, bool one, uint32_t t) {
+#pragma unroll 4
+    for (uint32_t i = t; i < (uint32_t)TS; i += NT) tile[i] = Amp<C2>::mk(0, 0);
+    if (one && t == 0) tile[0] = Amp<C2>::mk(1, 0);  // element 0 sits at offset 0
+}
+
+// complex64: two CTAs per SM (128 registers); complex128 programs need more.
+template <typename C2>
+__global__ void __launch_bounds__(NT, sizeof(C2) == 8 ? 2 : 1)
+    k_batch(C2* __restrict__ arena, const BatchTask* __restrict__ tasks, int ntasks, const BatchCirc* __restrict__ circs,
+            const BatchProg* __restrict__ progs, const unsigned char* __restrict__ blob, const DevOp* __restrict__ sops,
+            const double2* __restrict__ pool, int* __restrict__ head, int* __restrict__ done,
+            double* __restrict__ zout, int* __restrict__ err) {
+    C2* tile = reinterpret_cast<C2*>(batch_smem_raw);
+    TileTables<C2>& T = *reinterpret_cast<TileTables<C2>*>(batch_smem_raw + TS * sizeof(C2));
+    __shared__ int s_task;
+    __shared__ int s_abort;
+    __shared__ uint8_t s_zbit[40];
+    __shared__ double red[KATE_BATCH_MAX_QUBITS * (NT / 32) + KATE_BATCH_MAX_QUBITS];
+    const uint32_t t = threadIdx.x;
+    const uint32_t tb = (uint32_t)__cvta_generic_to_shared(tile);
+    for (;;) {
+        if (t == 0) {
+            // After a failed wait anywhere, every CTA stops at its next task.
+            s_task = *((volatile int*)err) ? ntasks : atomicAdd(head, 1);
+            s_abort = 0;
+        }
+        __syncthreads();
+        const int ti = s_task;
+        if (ti >= ntasks) break;
+        const BatchTask K = tasks[ti];
+        if (t == 0 && K.need > 0) {
+            const unsigned long long t0 = now_ns();
+            while (*((volatile int*)(done + K.circ)) < K.need) {
+                if (now_ns() - t0 > WAIT_NS || *((volatile int*)err)) {
+                    s_abort = 1;
+                    atomicExch(err, 1);
+                    break;
+                }
+                __nanosleep(256);
+            }
+            __threadfence();
+        }
+        if (t < 40) s_zbit[t] = circs[K.circ].zbit[t];
+        __syncthreads();
+        if (s_abort) break;
+        const int nz = circs[K.circ].n;
+        const int zoff = circs[K.circ].zoff;
+
+        if (K.kind != BT_ZRED) {
+            // SMALL: step s runs program prog + s on the resident tile.
+            // PASS: step s runs program prog on coset c0 + s.
+            const bool small = K.kind == BT_SMALL;
+            const int nsteps = small ? K.nprog : (int)(K.c1 - K.c0);
+            C2* st = arena + circs[K.circ].off;
+            if (small) {
+                init_basis0(tile, true, t);
+            } else {
+                const ProgView v = view(progs[K.prog], blob);
+                setup_program(T, v, t);
+                setup_io(T, v, t);
+            }
+            for (int s = 0; s < nsteps; s++) {
+                const BatchProg& P = progs[small ? K.prog + s : K.prog];
+                const uint32_t c = K.c0 + (uint32_t)s;
+                uint64_t cbase = 0;
+                __syncthreads();
+                if (small) {
+                    setup_program(T, view(P, blob), t);
+                } else {
+                    cbase = coset_base(T, c);
+                    if (K.first) {
+                        init_basis0(tile, cbase == 0, t);
+                    } else {
+                        load_async(T, st, c, tb, t);
+                        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+                    }
+                }
+                __syncthreads();
+                run_any(T, P, blob, tb, tile, cbase, sops, pool, t);
+                if (!small) {
+                    __syncthreads();
+                    store_tile<C2, true>(T, st, c, tb, t);
+                }
+            }
+            __syncthreads();
+            if (small) small_z(tile, nz, s_zbit, red, zout + zoff);
+        } else {
+            zred(arena + circs[K.circ].off, nz, K.c0, K.c1, s_zbit, red, zout + zoff);
+        }
+        __syncthreads();
+        if (t == 0) {
+            __threadfence();
+            atomicAdd(done + K.circ, 1);
+        }
+    }
+}
+
+template <typename C2>
+constexpr size_t batch_smem() {
+    return (size_t)TS * sizeof(C2) + sizeof(TileTables<C2>);
+}
+
+}  // namespace
+
+int batch_grid(int device, int prec) {
+    static int cached[64][2] = {{0}};
+    if (device < 0 || device >= 64) device = 0;
+    const int pi = prec == 1 ? 1 : 0;
+    if (!cached[device][pi]) {
+        int sms = 148, occ = 1;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        if (pi == 1) {
+            cudaFuncSetAttribute(k_batch<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)batch_smem<float2>());
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<float2>, NT, batch_smem<float2>());
+        } else {
+            cudaFuncSetAttribute(k_batch<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)batch_smem<double2>());
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<double2>, NT, batch_smem<double2>());
+        }
+        if (occ < 1) occ = 1;
+        cached[device][pi] = sms * occ;
+    }
+    return cached[device][pi];
+}
+
+cudaError_t launch_batch(void* arena, int prec, const BatchTask* tasks, int ntasks, const BatchCirc* circs,
+                         const BatchProg* progs, const void* blob, const DevOp* sops, const void* pool, int* head,
+                         int* done, double* zout, int* err, int grid, cudaStream_t s) {
+    const unsigned char* b = (const unsigned char*)blob;
+    const double2* pl = (const double2*)pool;
+    if (prec == 1)
+        k_batch<float2><<<grid, NT, batch_smem<float2>(), s>>>((float2*)arena, tasks, ntasks, circs, progs, b, sops, pl,
+                                                               head, done, zout, err);
+    else
+        k_batch<double2><<<grid, NT, batch_smem<double2>(), s>>>((double2*)arena, tasks, ntasks, circs, progs, b, sops,
+                                                                 pl, head, done, zout, err);
+    return cudaGetLastError();
+}
+
+}  // namespace kate

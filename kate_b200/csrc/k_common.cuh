@@ -30,6 +30,22 @@ __device__ __forceinline__ void cfma(double2& acc, double2 a, double2 b) {
     acc.y = fma(a.y, b.x, acc.y);
 }
 
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) { return cmulf(a, b); }
+__device__ __forceinline__ void cfma(float2& acc, float2 a, float2 b) {
+    acc.x = fmaf(a.x, b.x, acc.x);
+    acc.x = fmaf(-a.y, b.y, acc.x);
+    acc.y = fmaf(a.x, b.y, acc.y);
+    acc.y = fmaf(a.y, b.x, acc.y);
+}
+
+// A complex double from the matrix pool, as the tile's element type.
+template <typename C2>
+__device__ __forceinline__ C2 from_pool(double2 v);
+template <>
+__device__ __forceinline__ double2 from_pool<double2>(double2 v) { return v; }
+template <>
+__device__ __forceinline__ float2 from_pool<float2>(double2 v) { return make_float2((float)v.x, (float)v.y); }
+
 __device__ __forceinline__ double2 dadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 
 }  // namespace kate

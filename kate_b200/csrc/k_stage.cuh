@@ -1,0 +1,489 @@
+// Register-staged pass programs on one 4096-amplitude coset tile (see
+// PassProg in device_types.h), for both amplitude types:
+//   double2  complex128, FP64 arithmetic: 16-byte elements;
+//   float2   complex64, FP32 arithmetic: 8-byte elements.
+// Used by the tile kernel (k_tile.cu) and the batch kernel (k_batch.cu).
+//
+// Shared-memory byte offsets are tsw(e) << SH for element e: swz(e) << 4
+// for complex128, swz2(e) << 3 for complex64 (see k_ops.cuh). The host
+// writes stage tables and SOP_XF / SOP_XL flips as complex128 offsets,
+// swz(x) << 4 for tile-index vectors x; the complex64 setup maps each to
+// swz2(x) << 3 (x = swz(v >> 4), swz being its own inverse). All maps are
+// linear over GF(2), so XOR combinations of table entries map alike.
+#pragma once
+
+#include "k_common.cuh"
+#include "k_ops.cuh"
+
+namespace kate {
+namespace stage {
+namespace {
+
+constexpr int NT = 256;
+constexpr int TB = KATE_TILE_BITS;
+constexpr int TS = 1 << TB;
+static_assert(NT * 16 == TS, "16 amplitudes per thread");
+
+template <typename C2>
+struct Amp;
+template <>
+struct Amp<double2> {
+    using R = double;
+    static constexpr int SH = 4;   // log2 bytes per element
+    static constexpr int NCP = 16; // 16-byte copies per thread per tile
+    __device__ __forceinline__ static R fm(R a, R b, R c) { return fma(a, b, c); }
+    __device__ __forceinline__ static double2 mk(R x, R y) { return make_double2(x, y); }
+    __device__ __forceinline__ static double2 lds(uint32_t addr) {
+        double2 v;
+        asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"(addr));
+        return v;
+    }
+    __device__ __forceinline__ static void sts(uint32_t addr, double2 v) {
+        asm volatile("st.shared.v2.f64 [%0], {%1, %2};" ::"r"(addr), "d"(v.x), "d"(v.y) : "memory");
+    }
+};
+template <>
+struct Amp<float2> {
+    using R = float;
+    static constexpr int SH = 3;
+    static constexpr int NCP = 8;  // each 16-byte copy moves an adjacent pair of amplitudes
+    __device__ __forceinline__ static R fm(R a, R b, R c) { return fmaf(a, b, c); }
+    __device__ __forceinline__ static float2 mk(R x, R y) { return make_float2(x, y); }
+    __device__ __forceinline__ static float2 lds(uint32_t addr) {
+        float2 v;
+        asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr));
+        return v;
+    }
+    __device__ __forceinline__ static void sts(uint32_t addr, float2 v) {
+        asm volatile("st.shared.v2.f32 [%0], {%1, %2};" ::"r"(addr), "f"(v.x), "f"(v.y) : "memory");
+    }
+};
+
+// r = u0 * x + u1 * y (complex): 8 FMA-class ops.
+template <typename C2>
+__device__ __forceinline__ C2 row2(C2 u0, C2 u1, C2 x, C2 y) {
+    using A = Amp<C2>;
+    C2 r;
+    r.x = u0.x * x.x;
+    r.x = A::fm(-u0.y, x.y, r.x);
+    r.x = A::fm(u1.x, y.x, r.x);
+    r.x = A::fm(-u1.y, y.y, r.x);
+    r.y = u0.x * x.y;
+    r.y = A::fm(u0.y, x.x, r.y);
+    r.y = A::fm(u1.x, y.y, r.y);
+    r.y = A::fm(u1.y, y.x, r.y);
+    return r;
+}
+
+template <int B, typename C2>
+__device__ __forceinline__ void reg_u(C2 (&a)[16], C2 u00, C2 u01, C2 u10, C2 u11) {
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+        if ((j >> B) & 1) continue;
+        const int k = j | (1 << B);
+        const C2 x = a[j], y = a[k];
+        a[j] = row2(u00, u01, x, y);
+        a[k] = row2(u10, u11, x, y);
+    }
+}
+
+template <int B, typename C2>
+__device__ __forceinline__ void reg_h(C2 (&a)[16]) {
+    using R = typename Amp<C2>::R;
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+        if ((j >> B) & 1) continue;
+        const int k = j | (1 << B);
+        const C2 x = a[j], y = a[k];
+        const C2 n0 = Amp<C2>::mk((x.x + y.x) * (R)KATE_SQRT2INV, (x.y + y.y) * (R)KATE_SQRT2INV);
+        a[j] = n0;
+        a[k] = Amp<C2>::mk(n0.x - y.x * (R)KATE_SQRT2, n0.y - y.y * (R)KATE_SQRT2);
+    }
+}
+
+template <int B, typename C2>
+__device__ __forceinline__ void reg_x(C2 (&a)[16], uint32_t creg) {
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+        if ((j >> B) & 1) continue;
+        if (((uint32_t)j & creg) != creg) continue;
+        const int k = j | (1 << B);
+        const C2 x = a[j];
+        a[j] = a[k];
+        a[k] = x;
+    }
+}
+
+// Real 2x2 [[a, b], [c, d]]: 4 FMA-class ops per amplitude.
+template <int B, typename C2, typename R>
+__device__ __forceinline__ void reg_ur(C2 (&a)[16], R u00, R u01, R u10, R u11) {
+    using A = Amp<C2>;
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+        if ((j >> B) & 1) continue;
+        const int k = j | (1 << B);
+        const C2 x = a[j], y = a[k];
+        a[j] = A::mk(A::fm(u01, y.x, u00 * x.x), A::fm(u01, y.y, u00 * x.y));
+        a[k] = A::mk(A::fm(u11, y.x, u10 * x.x), A::fm(u11, y.y, u10 * x.y));
+    }
+}
+
+// [[a, ib], [ic, d]] with a, b, c, d real (RX-like): 4 FMA-class ops per amplitude.
+template <int B, typename C2, typename R>
+__device__ __forceinline__ void reg_ux(C2 (&a)[16], R u00, R u01i, R u10i, R u11) {
+    using A = Amp<C2>;
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+        if ((j >> B) & 1) continue;
+        const int k = j | (1 << B);
+        const C2 x = a[j], y = a[k];
+        a[j] = A::mk(A::fm(-u01i, y.y, u00 * x.x), A::fm(u01i, y.x, u00 * x.y));
+        a[k] = A::mk(A::fm(-u10i, x.y, u11 * y.x), A::fm(u10i, x.x, u11 * y.y));
+    }
+}
+
+// Controlled NOT with a per-thread condition: selects, no branches.
+template <int B, typename C2>
+__device__ __forceinline__ void reg_xs(C2 (&a)[16], uint32_t creg, bool go) {
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+        if ((j >> B) & 1) continue;
+        if (((uint32_t)j & creg) != creg) continue;
+        const int k = j | (1 << B);
+        const C2 x = a[j], y = a[k];
+        a[j] = Amp<C2>::mk(go ? y.x : x.x, go ? y.y : x.y);
+        a[k] = Amp<C2>::mk(go ? x.x : y.x, go ? x.y : y.y);
+    }
+}
+
+// The swizzle is linear over GF(2): swz(a | b) = swz(a) ^ swz(b) for
+// disjoint a, b. A stage's shared-memory byte offset of register j is
+// therefore s0 ^ W(j), W(j) the XOR of w_i over the set bits i of j.
+__device__ __forceinline__ uint32_t reg_off(int j, uint32_t s0, uint32_t w0, uint32_t w1, uint32_t w2, uint32_t w3) {
+    return s0 ^ ((j & 1) ? w0 : 0u) ^ ((j & 2) ? w1 : 0u) ^ ((j & 4) ? w2 : 0u) ^ ((j & 8) ? w3 : 0u);
+}
+
+// A complex128 shared-memory offset as the same tile-index vector's offset
+// in a C2 tile.
+template <typename C2>
+__device__ __forceinline__ uint32_t conv_off(uint32_t v) {
+    if (sizeof(C2) == 16) return v;
+    return ops::swz2(ops::swz(v >> 4)) << 3;
+}
+
+// Per-CTA tables of one pass program.
+//   complex128: copy j of thread t moves element e = t + 256 j;
+//   complex64:  copy j of thread t moves elements e, e + 1 with e = 2t + 512 j.
+// Global offset of the copy: cb(c) + dT[t] + goff[j]; shared byte offset of
+// its (first) element: tls[t] ^ (tsw(j << 8) << 4), resp. ^ (tsw(j << 9) << 3).
+// On write-back the copy's (first) output element reads the tile at
+// pTs[t] ^ osw[j] (qubit remap), and for complex64 the second one at that ^ o1.
+template <typename C2>
+struct TileTables {
+    SOp ops[KATE_MAX_SOPS];
+    C2 mats[KATE_MAX_MATS];
+    uint64_t cb[3][256];   // coset base = cb[0][c & 255] | cb[1][(c >> 8) & 255] | cb[2][c >> 16]
+    uint64_t goff[16];
+    uint64_t dT[NT];
+    uint32_t tls[NT];
+    uint32_t pTs[NT];
+    uint32_t osw[16];
+    uint32_t o1;
+    uint16_t stab[KATE_MAX_STAGES][44];
+};
+
+// Fields of a pass program the tables are built from. PassProg and the
+// batch's packed programs both provide them.
+struct ProgView {
+    int m, ncb, nops, nmats, nstages, sop0;
+    const uint8_t* tphys;
+    const uint8_t* outsrc;
+    const uint8_t* cphys;
+    const SOp* ops;
+    const double (*mats)[2];
+    const uint16_t (*stab)[44];
+};
+
+__device__ __forceinline__ ProgView view(const PassProg& P) {
+    ProgView v;
+    v.m = P.m;
+    v.ncb = P.ncb;
+    v.nops = P.nops;
+    v.nmats = P.nmats;
+    v.nstages = P.nstages;
+    v.sop0 = P.sop0;
+    v.tphys = P.tphys;
+    v.outsrc = P.outsrc;
+    v.cphys = P.cphys;
+    v.ops = P.ops;
+    v.mats = P.mats;
+    v.stab = P.stab;
+    return v;
+}
+
+// Program part of the tables (ops, matrices, stage tables). No barrier.
+template <typename C2>
+__device__ __forceinline__ void setup_program(TileTables<C2>& T, const ProgView& P, uint32_t t) {
+    for (int i = t; i < P.nstages * 44; i += NT) (&T.stab[0][0])[i] = (uint16_t)conv_off<C2>((&P.stab[0][0])[i]);
+    for (int i = t; i < P.nops; i += NT) {
+        SOp o = P.ops[i];
+        if (o.kind == SOP_XF || o.kind == SOP_XL) o.idx = (uint16_t)conv_off<C2>(o.idx);
+        T.ops[i] = o;
+    }
+    for (int i = t; i < P.nmats; i += NT) T.mats[i] = Amp<C2>::mk(P.mats[i][0], P.mats[i][1]);
+}
+
+// Global-access part of the tables (coset bases, copy offsets). No barrier.
+template <typename C2>
+__device__ __forceinline__ void setup_io(TileTables<C2>& T, const ProgView& P, uint32_t t) {
+    constexpr int SH = Amp<C2>::SH;
+    constexpr int E = SH == 4 ? 0 : 1;  // log2 elements per copy
+    for (int part = 0; part < 3; part++) {
+        uint64_t b = 0;
+        for (int i = 0; i < 8; i++) {
+            const int bit = part * 8 + i;
+            if (bit < P.ncb && ((t >> i) & 1u)) b |= 1ull << P.cphys[bit];
+        }
+        T.cb[part][t] = b;
+    }
+    constexpr int HB = 8 + E;  // tile bits of the copy index j start here
+    if (t < (uint32_t)(1 << (TB - HB))) {
+        uint64_t g = 0;
+        uint32_t o = 0;
+        for (int i = 0; i < TB - HB; i++)
+            if ((t >> i) & 1u) {
+                g |= 1ull << P.tphys[HB + i];
+                o |= 1u << P.outsrc[HB + i];
+            }
+        T.goff[t] = g;
+        T.osw[t] = ops::tsw<C2>(o) << SH;
+    }
+    if (t == 0) T.o1 = ops::tsw<C2>(1u << P.outsrc[0]) << SH;
+    uint64_t dT = 0;
+    uint32_t pT = 0;
+    for (int i = 0; i < 8; i++) {
+        dT |= (uint64_t)((t >> i) & 1u) << P.tphys[i + E];
+        pT |= ((t >> i) & 1u) << P.outsrc[i + E];
+    }
+    T.dT[t] = dT;
+    T.pTs[t] = ops::tsw<C2>(pT) << SH;
+    T.tls[t] = ops::tsw<C2>(t << E) << SH;
+}
+
+template <typename C2>
+__device__ __forceinline__ uint64_t coset_base(const TileTables<C2>& T, uint32_t c) {
+    return T.cb[0][c & 255u] | T.cb[1][(c >> 8) & 255u] | T.cb[2][c >> 16];
+}
+
+// Issues the cp.async copies of coset c into the tile at shared address
+// buf, and commits them as one group.
+template <typename C2>
+__device__ __forceinline__ void load_async(const TileTables<C2>& T, const C2* __restrict__ st, uint32_t c, uint32_t buf,
+                                           uint32_t t) {
+    constexpr int SH = Amp<C2>::SH, HB = SH == 4 ? 8 : 9;
+    const C2* src = st + (coset_base(T, c) + T.dT[t]);
+    const uint32_t tls = T.tls[t];
+#pragma unroll
+    for (int j = 0; j < Amp<C2>::NCP; j++) {
+        const uint32_t d = buf + (tls ^ (ops::tsw<C2>((uint32_t)j << HB) << SH));
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src + T.goff[j]) : "memory");
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
+__device__ __forceinline__ void st_pair(float2* p, float2 a, float2 b) {
+    *reinterpret_cast<float4*>(p) = make_float4(a.x, a.y, b.x, b.y);
+}
+__device__ __forceinline__ void st_pair_cg(float2* p, float2 a, float2 b) {
+    __stcg(reinterpret_cast<float4*>(p), make_float4(a.x, a.y, b.x, b.y));
+}
+
+// Writes the tile at shared address tb back to coset c (qubit remap
+// applied). CG: stores bypass L1 (other SMs read them in the same launch).
+template <typename C2, bool CG>
+__device__ __forceinline__ void store_tile(const TileTables<C2>& T, C2* __restrict__ st, uint32_t c, uint32_t tb,
+                                           uint32_t t) {
+    using A = Amp<C2>;
+    C2* dst = st + (coset_base(T, c) + T.dT[t]);
+    const uint32_t pTs = T.pTs[t];
+    if constexpr (A::SH == 4) {
+        // Four at a time: bounds the registers in flight.
+#pragma unroll
+        for (int j0 = 0; j0 < 16; j0 += 4) {
+#pragma unroll
+            for (int j = j0; j < j0 + 4; j++) {
+                const C2 v = A::lds(tb + (pTs ^ T.osw[j]));
+                if (CG) __stcg(dst + T.goff[j], v);
+                else dst[T.goff[j]] = v;
+            }
+            asm volatile("" ::: "memory");
+        }
+    } else {
+        const uint32_t o1 = T.o1;
+#pragma unroll
+        for (int j0 = 0; j0 < 8; j0 += 4) {
+#pragma unroll
+            for (int j = j0; j < j0 + 4; j++) {
+                const uint32_t o = pTs ^ T.osw[j];
+                const C2 v0 = A::lds(tb + o), v1 = A::lds(tb + (o ^ o1));
+                if (CG) st_pair_cg(dst + T.goff[j], v0, v1);
+                else st_pair(dst + T.goff[j], v0, v1);
+            }
+            asm volatile("" ::: "memory");
+        }
+    }
+}
+
+// Runs the program in T on the tile at shared address tb (generic pointer
+// tile), for coset base cbase. Ends with the last stage's registers stored;
+// no trailing barrier. SM: whether the program may hold shared-memory ops.
+template <typename C2, bool SM, int MAXK = 5>
+__device__ __forceinline__ void run_program(const TileTables<C2>& T, int nops, uint32_t tb, C2* tile, uint64_t cbase,
+                                            const DevOp* __restrict__ sops, int sop0,
+                                            const double2* __restrict__ pool, uint32_t t) {
+    using A = Amp<C2>;
+    using R = typename A::R;
+    C2 a[16];
+    bool open = false;
+    uint32_t s0s = 0;    // store offset base of the open stage (flipped by SOP_XF)
+    uint32_t lflip = 0;  // load offset flips for the next stage (SOP_XL)
+    int si = 0;          // open stage's table
+    auto store_regs = [&]() {
+        const uint16_t* tab = T.stab[si];
+        const uint32_t v0 = tab[36], v1 = tab[37], v2 = tab[38], v3 = tab[39];
+#pragma unroll
+        for (int j = 0; j < 16; j++) A::sts(tb + reg_off(j, s0s, v0, v1, v2, v3), a[j]);
+    };
+    for (int k = 0; k < nops; k++) {
+        const SOp op = T.ops[k];
+        switch (op.kind) {
+        case SOP_STAGE: {
+            if (open) store_regs();
+            __syncthreads();
+            si = op.idx;
+            const uint16_t* tab = T.stab[si];
+            const uint32_t s0 = (uint32_t)tab[t & 15u] ^ (uint32_t)tab[16 + (t >> 4)];
+            const uint32_t w0 = tab[32], w1 = tab[33], w2 = tab[34], w3 = tab[35];
+            const uint32_t sl = s0 ^ lflip;
+#pragma unroll
+            for (int j = 0; j < 16; j++) a[j] = A::lds(tb + reg_off(j, sl, w0, w1, w2, w3));
+            s0s = s0;
+            lflip = 0;
+            open = true;
+            break;
+        }
+        case SOP_XF: {
+            if ((t & op.cthr) == op.cthr && (op.ccos == 0 || (cbase & op.ccos) == op.ccos)) s0s ^= op.idx;
+            break;
+        }
+        case SOP_XL: {
+            if ((t & op.cthr) == op.cthr && (op.ccos == 0 || (cbase & op.ccos) == op.ccos)) lflip ^= op.idx;
+            break;
+        }
+        case SOP_SMEM: {
+            if (!SM) break;
+            if (open) {
+                store_regs();
+                open = false;
+            }
+            // The registers are dead until the next stage loads them.
+#pragma unroll
+            for (int j = 0; j < 16; j++) a[j] = A::mk(0, 0);
+            __syncthreads();
+            const DevOp d = sops[sop0 + op.idx];
+            ops::apply_op<C2, MAXK>(tile, TB, cbase, d, pool, (int)t, NT);
+            __syncthreads();
+            break;
+        }
+        case SOP_U: {
+            const C2 u00 = T.mats[op.idx], u01 = T.mats[op.idx + 1], u10 = T.mats[op.idx + 2], u11 = T.mats[op.idx + 3];
+            switch (op.a) {
+            case 0: reg_u<0>(a, u00, u01, u10, u11); break;
+            case 1: reg_u<1>(a, u00, u01, u10, u11); break;
+            case 2: reg_u<2>(a, u00, u01, u10, u11); break;
+            default: reg_u<3>(a, u00, u01, u10, u11); break;
+            }
+            break;
+        }
+        case SOP_UR: {
+            const R u00 = T.mats[op.idx].x, u01 = T.mats[op.idx + 1].x, u10 = T.mats[op.idx + 2].x,
+                    u11 = T.mats[op.idx + 3].x;
+            switch (op.a) {
+            case 0: reg_ur<0>(a, u00, u01, u10, u11); break;
+            case 1: reg_ur<1>(a, u00, u01, u10, u11); break;
+            case 2: reg_ur<2>(a, u00, u01, u10, u11); break;
+            default: reg_ur<3>(a, u00, u01, u10, u11); break;
+            }
+            break;
+        }
+        case SOP_UX: {
+            const R u00 = T.mats[op.idx].x, u01 = T.mats[op.idx + 1].y, u10 = T.mats[op.idx + 2].y,
+                    u11 = T.mats[op.idx + 3].x;
+            switch (op.a) {
+            case 0: reg_ux<0>(a, u00, u01, u10, u11); break;
+            case 1: reg_ux<1>(a, u00, u01, u10, u11); break;
+            case 2: reg_ux<2>(a, u00, u01, u10, u11); break;
+            default: reg_ux<3>(a, u00, u01, u10, u11); break;
+            }
+            break;
+        }
+        case SOP_H: {
+            switch (op.a) {
+            case 0: reg_h<0>(a); break;
+            case 1: reg_h<1>(a); break;
+            case 2: reg_h<2>(a); break;
+            default: reg_h<3>(a); break;
+            }
+            break;
+        }
+        case SOP_X: {
+            const bool go = (t & op.cthr) == op.cthr && (op.ccos == 0 || (cbase & op.ccos) == op.ccos);
+            if (op.cthr == 0) {  // warp-uniform condition: branch
+                if (!go) break;
+                switch (op.a) {
+                case 0: reg_x<0>(a, op.creg); break;
+                case 1: reg_x<1>(a, op.creg); break;
+                case 2: reg_x<2>(a, op.creg); break;
+                default: reg_x<3>(a, op.creg); break;
+                }
+            } else {
+                switch (op.a) {
+                case 0: reg_xs<0>(a, op.creg, go); break;
+                case 1: reg_xs<1>(a, op.creg, go); break;
+                case 2: reg_xs<2>(a, op.creg, go); break;
+                default: reg_xs<3>(a, op.creg, go); break;
+                }
+            }
+            break;
+        }
+        case SOP_PH: {
+            if ((t & op.cthr) != op.cthr || (op.ccos != 0 && (cbase & op.ccos) != op.ccos)) break;
+            const C2 ph = T.mats[op.idx];
+#pragma unroll
+            for (int j = 0; j < 16; j++)
+                if (((uint32_t)j & op.creg) == op.creg) a[j] = cmul(a[j], ph);
+            break;
+        }
+        case SOP_D1: {
+            const C2 d0 = T.mats[op.idx], d1 = T.mats[op.idx + 1];
+            const bool b = op.src == SRC_THR ? ((t >> op.a) & 1u) : (uint32_t)((cbase >> op.a) & 1ull);
+            const C2 d = b ? d1 : d0;
+#pragma unroll
+            for (int j = 0; j < 16; j++) a[j] = cmul(a[j], d);
+            break;
+        }
+        case SOP_DR: {
+#pragma unroll
+            for (int j = 0; j < 16; j++) a[j] = cmul(a[j], T.mats[op.idx + j]);
+            break;
+        }
+        default:
+            break;
+        }
+    }
+    if (open) store_regs();
+}
+
+}  // namespace
+}  // namespace stage
+}  // namespace kate

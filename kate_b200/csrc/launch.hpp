@@ -30,17 +30,25 @@ cudaError_t launch_init_product_c128(void* st, int n, const ProductInit& P, cuda
 cudaError_t launch_pass_generic_c128(void* st, int n, const DevPass& p, const DevOp* ops, const void* pool,
                                      int grid, cudaStream_t s);
 int generic_pass_grid(int n, int m, int device);
-// Register-staged tile kernel (12-qubit tiles, 256 threads x 16 amplitudes).
-// nbuf = 2: one CTA per SM with a prefetched second tile; nbuf = 1: two
-// CTAs per SM with one tile each.
-cudaError_t launch_tile_c128(void* st, const PassProg& prog, const DevOp* sops, const void* pool, int grid, int nbuf,
-                             cudaStream_t s);
-int tile_pass_grid(int n, int device, int nbuf);
+// Register-staged tile kernel (12-qubit tiles, 256 threads x 16 amplitudes),
+// prec 0: complex128 / FP64, 1: complex64 / FP32. nbuf = 2: one CTA per SM
+// with a prefetched second tile; nbuf = 1: two CTAs per SM with one tile each.
+cudaError_t launch_tile(void* st, int prec, const PassProg& prog, const DevOp* sops, const void* pool, int grid,
+                        int nbuf, cudaStream_t s);
+int tile_pass_grid(int n, int device, int nbuf, int prec);
 
 // Complex64 pass of 5-qubit dense blocks on the tensor cores. err: device
 // int set to 1 if a bounded wait gave up.
 cudaError_t launch_block_c64(void* st, const BlockProg& prog, const void* bimg, int* err, int grid, cudaStream_t s);
 int block_c64_grid(int n, int device);
+
+// Persistent batch kernel (k_batch.cu). head, done[circuits], zout (large
+// circuits' outputs) must be zero at launch; err is set to 1 when a
+// dependency wait gave up (the kernel then stops).
+cudaError_t launch_batch(void* arena, int prec, const BatchTask* tasks, int ntasks, const BatchCirc* circs,
+                         const BatchProg* progs, const void* blob, const DevOp* sops, const void* pool, int* head,
+                         int* done, double* zout, int* err, int grid, cudaStream_t s);
+int batch_grid(int device, int prec);
 
 // Bit sums: per CTA, for every local bit, the sum over amplitudes with the
 // bit 0 and with the bit 1, plus the total. kind 0 sums amplitudes (double2

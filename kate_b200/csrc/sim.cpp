@@ -55,7 +55,7 @@ struct SimImpl {
     cudaError_t launch_pass(size_t i, cudaStream_t st) {
         const PlannedPass& p = plan.passes[i];
         if (p.bprog) return launch_block_c64(d_state, *p.bprog, d_bimg, d_err, block_grid, st);
-        if (p.prog) return launch_tile_c128(d_state, *p.prog, d_sops, d_pool, tile_grid, nbuf, st);
+        if (p.prog) return launch_tile(d_state, precision, *p.prog, d_sops, d_pool, tile_grid, nbuf, st);
         return launch_pass_generic(d_state, precision, hpasses[i], d_ops, d_pool, grid, st);
     }
     int block_grid = 0;
@@ -180,8 +180,8 @@ std::string Simulator::create(const Program& prog_in, int precision, int device,
     impl->grid = generic_pass_grid(impl->n, std::min(impl->opt.max_tile, impl->n), device);
     if (const char* e = std::getenv("KATE_TILE_NBUF")) impl->nbuf = std::atoi(e) == 2 ? 2 : 1;
     if (impl->n >= KATE_TILE_BITS) {
-        if (precision == 0) impl->tile_grid = tile_pass_grid(impl->n, device, impl->nbuf);
-        else impl->block_grid = block_c64_grid(impl->n, device);
+        impl->tile_grid = tile_pass_grid(impl->n, device, impl->nbuf, precision);
+        if (precision == 1) impl->block_grid = block_c64_grid(impl->n, device);
     }
     impl->phys.resize(impl->n);
     std::iota(impl->phys.begin(), impl->phys.end(), 0);

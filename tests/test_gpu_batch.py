@@ -1,0 +1,108 @@
+"""Batch engine (one persistent launch for many circuits): <Z_q> of every
+circuit of a mixed batch against the oracle's state, through the C ABI.
+Bars: complex128 1e-12; complex64 (FP32 arithmetic) 2e-5."""
+import numpy as np
+import pytest
+
+import kate_b200 as K
+from kate_b200 import _lib, circuits
+from common import random_circuit
+
+pytestmark = pytest.mark.gpu
+
+
+def zexp(n, st):
+    p = np.abs(st) ** 2
+    idx = np.arange(1 << n)
+    return np.array([p[((idx >> q) & 1) == 0].sum() - p[((idx >> q) & 1) == 1].sum() for q in range(n)])
+
+
+def mixed(seed):
+    rng = np.random.default_rng(seed)
+    specs = []
+    for n in [1, 2, 3, 5, 8, 11, 12, 13, 14, 16, 18]:
+        specs.append((n, random_circuit(n, 60, rng)))
+    for n in [10, 12, 13, 17]:
+        specs.append((n, circuits.hea(n, 2 * n, seed=n)))
+    specs.append((5, []))
+    specs.append((14, []))
+    return specs
+
+
+@pytest.mark.parametrize("prec,tol", [(K.C128, 1e-12), (K.C64, 2e-5)])
+def test_mixed_batch_matches_oracle(oracle, prec, tol):
+    specs = mixed(1)
+    b = K.Batch([K.Circuit(n, g) for n, g in specs], precision=prec)
+    b.run()
+    got = b.expect_z()
+    for (n, g), z in zip(specs, got):
+        ref = zexp(n, oracle.simulate(n, g))
+        assert np.abs(z - ref).max() <= tol, (n, len(g), np.abs(z - ref).max())
+
+
+def test_runs_repeat_and_options_do_not_change_results(oracle):
+    specs = mixed(2)
+    circs = [K.Circuit(n, g) for n, g in specs]
+    b = K.Batch(circs, precision=K.C128)
+    b.run()
+    z1 = b.expect_z_flat().copy()
+    b.run()
+    b.run()
+    assert np.abs(b.expect_z_flat() - z1).max() <= 1e-13
+    o = _lib.BatchOptions()
+    K._lib.lib().kate_batch_options_default(ctypes_ref(o))
+    o.chunk = 1
+    o.zchunks = 1
+    o.window_bytes = 1 << 20  # one large state per window
+    for n in range(K._lib.KATE_BATCH_MAX_QUBITS + 1):
+        o.tune[n].fusion = 3
+        o.tune[n].max_gates = 40
+    b2 = K.Batch(circs, precision=K.C128, options=o)
+    b2.run()
+    assert b2.info()["tasks"] > b.info()["tasks"]
+    assert np.abs(b2.expect_z_flat() - z1).max() <= 1e-12
+
+
+def ctypes_ref(x):
+    import ctypes
+    return ctypes.byref(x)
+
+
+def test_compiled_circuits_match_simulator():
+    rng = np.random.default_rng(9)
+    circs = []
+    for n in (9, 14):
+        c = K.Circuit(n, random_circuit(n, 80, rng))
+        c.gateScheduling()
+        c.gateFusion(3, 1e-6)
+        c.gateGrouping(6)
+        c.allocate(0)
+        circs.append(c)
+    b = K.Batch(circs, precision=K.C128)
+    b.run()
+    for c, z in zip(circs, b.expect_z()):
+        sim = K.Simulator(c, 1, K.C128, 0)
+        sim.execute()
+        assert np.abs(sim.expect_z() - z).max() <= 1e-12
+
+
+def test_autotune_then_run(oracle):
+    specs = [(n, circuits.hea(n, 2 * n, seed=100 + i)) for i, n in enumerate([10, 11, 13, 13, 15])]
+    b = K.Batch([K.Circuit(n, g) for n, g in specs], precision=K.C64, autotune=True)
+    for n in (10, 11, 13, 15):
+        assert b.options.tune[n].fusion >= 1 and b.options.tune[n].max_gates >= 1
+    b.run()
+    for (n, g), z in zip(specs, b.expect_z()):
+        assert np.abs(z - zexp(n, oracle.simulate(n, g))).max() <= 2e-5
+
+
+def test_hea_batch_of_many_circuits(oracle):
+    rng = np.random.default_rng(4)
+    ns = [int(x) for x in rng.integers(10, 17, 300)]
+    specs = [(n, circuits.hea(n, 2 * n, seed=1000 + i)) for i, n in enumerate(ns)]
+    b = K.Batch([K.Circuit(n, g) for n, g in specs], precision=K.C64)
+    b.run()
+    got = b.expect_z()
+    for i in range(0, len(specs), 37):
+        n, g = specs[i]
+        assert np.abs(got[i] - zexp(n, oracle.simulate(n, g))).max() <= 2e-5
