@@ -30,6 +30,28 @@ struct LOp {
     std::vector<int> qs; // logical qubits (dependencies)
 };
 
+bool is_one(Cx v) { return v.re == 1.0 && v.im == 0.0; }
+
+Cx cdiv(Cx a, Cx b) {
+    const double d = b.re * b.re + b.im * b.im;
+    return Cx((a.re * b.re + a.im * b.im) / d, (a.im * b.re - a.re * b.im) / d);
+}
+
+// Multiplicative Moebius transform of a 2^k diagonal table: h[S] with
+// table[b] = prod over S subset of b of h[S]. False (h untouched) when an
+// entry is zero or k is outside 2..5.
+bool diag_factors(const std::vector<Cx>& table, int k, std::vector<Cx>* h) {
+    if (k < 2 || k > 5 || table.size() != (1u << k)) return false;
+    for (const Cx& v : table)
+        if (v.re == 0.0 && v.im == 0.0) return false;
+    if (!h) return true;
+    *h = table;
+    for (int i = 0; i < k; i++)
+        for (uint32_t S = 0; S < (1u << k); S++)
+            if ((S >> i) & 1u) (*h)[S] = cdiv((*h)[S], (*h)[S & ~(1u << i)]);
+    return true;
+}
+
 }  // namespace
 
 int classify_2x2(const Cx* m) {
@@ -85,6 +107,49 @@ std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n,
             if (o.dtile < 0) o.dphys = phys[g.fq[0]];
             o.m[0] = g.table[0];
             o.m[1] = g.table[1];
+        } else if (g.kind == OPK_DIAG && diag_factors(g.table, (int)g.fq.size(), nullptr)) {
+            // A k-qubit diagonal as register ops: its multiplicative Moebius
+            // factors h[S] (table[b] = product of h[S] over the bit sets S
+            // contained in b) become one-qubit diagonals (|S| = 1, with h[{}]
+            // folded into the first) and controlled phases on the qubits of S.
+            const int k = (int)g.fq.size();
+            std::vector<Cx> h;
+            diag_factors(g.table, k, &h);
+            bool first = true;
+            for (uint32_t S = 1; S < (1u << k); S++) {
+                const int pc = __builtin_popcount(S);
+                Cx v = h[S];
+                if (pc == 1) {
+                    const int i = __builtin_ctz(S);
+                    const Cx d0 = first ? h[0] : Cx(1.0, 0.0);
+                    const Cx d1 = first ? h[0] * v : v;
+                    first = false;
+                    if (is_one(d0) && is_one(d1)) continue;
+                    LOp d;
+                    d.kind = SOP_D1;
+                    d.dtile = tile_bit(g.fq[i]);
+                    if (d.dtile < 0) d.dphys = phys[g.fq[i]];
+                    d.m[0] = d0;
+                    d.m[1] = d1;
+                    d.qs = {g.fq[i]};
+                    L.push_back(std::move(d));
+                } else {
+                    if (is_one(v)) continue;
+                    LOp c;
+                    c.kind = SOP_PH;
+                    c.m[0] = v;
+                    for (int i = 0; i < k; i++)
+                        if ((S >> i) & 1u) {
+                            const int q = g.fq[i];
+                            const int t = tile_bit(q);
+                            if (t >= 0) c.tctl |= 1u << t;
+                            else c.pctl |= 1ull << phys[q];
+                            c.qs.push_back(q);
+                        }
+                    L.push_back(std::move(c));
+                }
+            }
+            continue;
         } else {
             o.kind = SOP_SMEM;
             PlannedPass one;

@@ -128,3 +128,16 @@ def test_register_staged_layered_matches_oracle(oracle):
     gates = circuits.layered(n, 6, seed=3)
     pv = PlanView(K.Circuit(n, gates), 12, 4, 0)
     assert np.abs(pv.run_staged(zero_state(n)) - oracle.simulate(n, gates)).max() <= 1e-12
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_multi_qubit_diagonals_become_register_ops(oracle, seed):
+    """k-qubit diagonals (CZ, random diagonal tables) lower to one-qubit
+    diagonals and controlled phases, not shared-memory ops."""
+    rng = np.random.default_rng(500 + seed)
+    n = 13 + seed % 3
+    gates = circuits.hea(n, 4, seed=seed) + random_circuit(n, 60, rng, kinds=("diag2", "diag1", "d1", "cnot"))
+    pv = PlanView(K.Circuit(n, gates), 12, 4, 0)
+    assert all(p is not None for p in pv.programs)
+    assert pv.smem_ops == [] or len(pv.smem_ops) == 0
+    assert np.abs(pv.run_staged(zero_state(n)) - oracle.simulate(n, gates)).max() <= 1e-12
