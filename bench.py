@@ -25,6 +25,20 @@ pass = 20 layers). Metric: layers per second of the gate phase.
 ``--impl reference`` times the reference's CPU implementation alone on this
 workload (same metric), rank 0 only. ``--gpus N`` (torchrun) runs N
 independent replicas, one per GPU (the path does not shard on one GPU).
+
+Other workloads (``--workload``), one JSON line each:
+  precision  32-qubit complex64 brickwork of Haar SU(4) gates, 20 layers,
+             fused 5-qubit blocks on the tensor cores (3xTF32): layers/s,
+             speed-up over the complex128 path on the same circuit, and the
+             infidelity against complex128 at n=28.
+  batch      4096 hardware-efficient-ansatz circuits (n uniform in 10..22,
+             depth 2n, complex64) in one persistent CUDA-graph launch,
+             autotuned: circuits/s, against one Simulator launch per circuit.
+  serve      a Poisson stream of layered-circuit requests (n truncated
+             geometric on 12..28, depth n, complex64, 1024 samples + <Z>)
+             through the continuous-batching server under a 150 GB
+             admission budget, rates swept: circuits/s and p50/p99 latency,
+             against one-at-a-time plain launches.
 """
 from __future__ import annotations
 
@@ -50,11 +64,18 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="kate_b200", choices=["kate_b200", "reference"])
-    ap.add_argument("--nqubits", type=int, default=30)
+    ap.add_argument("--workload", default="layers", choices=["layers", "precision", "batch", "serve"])
+    ap.add_argument("--nqubits", type=int, default=None)
     ap.add_argument("--layers", type=int, default=20)
+    ap.add_argument("--circuits", type=int, default=4096, help="batch: circuits in the batch")
+    ap.add_argument("--requests", type=int, default=400, help="serve: requests per rate")
+    ap.add_argument("--rates", default="100,400,1600,6400", help="serve: arrival rates (requests/s)")
     ap.add_argument("--seed", type=int, default=1234)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    return ap.parse_args()
+    a = ap.parse_args()
+    if a.nqubits is None:
+        a.nqubits = 32 if a.workload == "precision" else 30
+    return a
 
 
 def workload_config(args):
@@ -209,6 +230,9 @@ def run_reference(args):
 
 def main():
     args = parse()
+    if args.workload != "layers":
+        {"precision": run_precision, "batch": run_batch, "serve": run_serve}[args.workload](args)
+        return
     if args.impl == "reference":
         run_reference(args)
         return
@@ -303,7 +327,7 @@ def main():
                         "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": committed_traffic(n),
-                             "peak_source": peak_kind, "kernel": "k_pass_generic",
+                             "peak_source": peak_kind, "kernel": "k_tile<double2> (register-staged group pass)",
                              "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_pass_ms,
                              "profiled_pass_ms": {"min": min(pass_ms), "max": max(pass_ms),
                                                   "mean": sum(pass_ms) / len(pass_ms)}},
@@ -314,6 +338,400 @@ def main():
     if dist:
         tdist.barrier()
         tdist.destroy_process_group()
+
+
+
+# ---------------------------------------------------------------------------
+# Other workloads
+# ---------------------------------------------------------------------------
+
+def _common(metric, unit, value, args, ms_per_step, dtype, config, **extra):
+    line = {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": dtype, "data": "synthetic (seeded)", "config": config}
+    line.update(extra)
+    return line
+
+
+def _ref_seconds(n, gates, fuse=True):
+    """Gate-phase seconds of one circuit on the reference's CPU simulator."""
+    from oracle.oracle import Ref
+    ref = Ref()
+    c = ref.circuit(n, gates)
+    if fuse:
+        c.schedule()
+        c.fuse(5, 1e-6)
+        c.group(min(12, n))
+    c.compile_default(0)
+    sess = c.session()
+    ms = sess.run()
+    sess.close()
+    return ms / 1000.0, ref.hw_threads()
+
+
+def _reference_unavailable():
+    from oracle.oracle import available_ref
+    return not available_ref()
+
+
+def run_precision(args):
+    """Brickwork SU(4) at n qubits, complex64 on the tensor-core path."""
+    import numpy as np
+    import torch
+    import kate_b200 as K
+    from kate_b200 import circuits
+
+    n, L = args.nqubits, args.layers
+    gates = circuits.brickwork_su4(n, L, args.seed)
+    cfg = {"workload": f"brickwork of Haar SU(4) gates, n={n}, {L} layers, complex64, 5-qubit blocks on "
+                       f"tensor cores (3xTF32)", "nqubits": n, "layers": L, "gates": len(gates), "seed": args.seed,
+           "state_bytes": 8 << n, "l2": "state larger than L2; no flush needed", "parallelism": "replicas"}
+    if args.impl == "reference":
+        if _reference_unavailable():
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built"}))
+            return
+        nn = min(n, 24)
+        sec, cores = _ref_seconds(nn, circuits.brickwork_su4(nn, 1, args.seed))
+        v = 1.0 / (sec * 2 ** (n - nn))
+        print(json.dumps(_common("layers/s", "layers/s", v, args, 1000 / v, "c128 (f64)", cfg, impl="reference",
+                                 cpu_baseline={"value": v, "unit": "layers/s", "cores": cores, "kind": "reference",
+                                               "sample": f"1 layer at n={nn} (complex128, the reference has no "
+                                                         f"complex64), scaled by 2^{n - nn}"},
+                                 e2e={"value": v, "unit": "layers/s", "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0})))
+        return
+    torch.cuda.set_device(0)
+    circ = K.Circuit(n, gates)
+    sim = K.Simulator(circ, 1, K.C64, 0)
+    passes = sim.passes()
+    stream = torch.cuda.Stream()
+    for _ in range(args.warmup):
+        sim.run_async(stream.cuda_stream)
+    stream.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(0) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            sim.run_async(stream.cuda_stream)
+        ev1.record(stream)
+        ev1.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    init_ms, pass_ms = sim.profile_passes()
+    avg_pass = sum(pass_ms) / len(pass_ms)
+    alg = 2.0 * 8.0 * 2 ** n
+    peak, peak_kind = measured_hbm_peak()
+    launches = sim.launches_per_run()
+    sim.close()
+    del sim
+    # The complex128 path on the same circuit.
+    s128 = K.Simulator(circ, 1, K.C128, 0)
+    s128.run_async(stream.cuda_stream)
+    stream.synchronize()
+    ev0.record(stream)
+    s128.run_async(stream.cuda_stream)
+    ev1.record(stream)
+    ev1.synchronize()
+    ms128 = ev0.elapsed_time(ev1)
+    s128.close()
+    del s128
+    # Infidelity at n = 28 against complex128.
+    nf = min(n, 28)
+    cf = K.Circuit(nf, circuits.brickwork_su4(nf, L, args.seed))
+    a = K.Simulator(cf, 1, K.C64, 0)
+    a.execute()
+    psi64 = a.state()
+    a.close()
+    b = K.Simulator(cf, 1, K.C128, 0)
+    b.execute()
+    psi128 = b.state()
+    b.close()
+    ov = np.vdot(psi128, psi64)
+    infid = float(1.0 - abs(ov) ** 2 / (np.vdot(psi64, psi64).real * np.vdot(psi128, psi128).real))
+    del psi64, psi128
+    # End to end: plan + upload + |0> init + passes + proba_state readback.
+    t0 = time.perf_counter()
+    e = K.Simulator(circ, 1, K.C64, 0)
+    e.execute()
+    e.close()
+    e2e_ms = (time.perf_counter() - t0) * 1000
+    cpu = None
+    if not args.no_cpu_baseline and not _reference_unavailable():
+        nn = 24
+        sec, cores = _ref_seconds(nn, circuits.brickwork_su4(nn, 1, args.seed))
+        cpu = {"value": 1.0 / (sec * 2 ** (n - nn)), "unit": "layers/s", "cores": cores, "kind": "reference",
+               "sample": f"1 layer at n={nn} on the reference CPUSimulator (complex128), scaled by 2^{n - nn}"}
+    cfg.update({"c128_ms_per_step": ms128, "speedup_vs_c128": ms128 / ms, "infidelity_vs_c128": infid,
+                "infidelity_nqubits": nf, "passes_per_step": len(passes)})
+    print(json.dumps(_common(
+        f"{n}q SU(4) brickwork layers/s (complex64)", "layers/s", L * 1000.0 / ms, args, ms, "c64 (tf32x3 / f32)",
+        cfg,
+        e2e={"value": L * 1000.0 / e2e_ms, "unit": "layers/s", "h2d_bytes_per_step": len(gates) * 16 * 16,
+             "d2h_bytes_per_step": 2 * n * 8, "ms_per_step": e2e_ms},
+        roofline={"bound": "hbm", "achieved": alg / (avg_pass / 1000) / 1e9, "peak": peak, "unit": "GB/s",
+                  "frac": alg / (avg_pass / 1000) / 1e9 / peak, "traffic": None, "peak_source": peak_kind,
+                  "kernel": "k_block_c64 (tcgen05 kind::tf32, 3xTF32)", "alg_bytes_per_launch": alg,
+                  "avg_launch_ms": avg_pass},
+        gpu_launches=launches * args.steps, clocks=clk.summary(), cpu_baseline=cpu)))
+
+
+def _hea_batch(K, C, count, seed=2024):
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    ns = [int(x) for x in rng.integers(10, 23, count)]
+    circs = []
+    for i, n in enumerate(ns):
+        c = K.Circuit(n)
+        c.appendFlat(*C.hea_flat(n, 2 * n, seed=i))
+        circs.append(c)
+    return ns, circs
+
+
+def run_batch(args):
+    """4096 HEA circuits in one persistent CUDA-graph launch."""
+    import torch
+    import kate_b200 as K
+    from kate_b200 import circuits as C
+
+    N = args.circuits
+    cfg = {"workload": f"{N} hardware-efficient-ansatz circuits, n uniform in 10..22 (seeded), depth 2n "
+                       f"(RY, RZ on every qubit, CZ brickwork), complex64, <Z_q> outputs, one persistent "
+                       f"CUDA-graph launch", "circuits": N, "seed": 2024, "parallelism": "replicas",
+           "l2": "states total ~21 GB, larger than L2; no flush needed"}
+    if args.impl == "reference":
+        if _reference_unavailable():
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built"}))
+            return
+        import numpy as np
+        rng = np.random.default_rng(2024)
+        ns = [int(x) for x in rng.integers(10, 23, N)]
+        tot, cnt, cores = 0.0, 0, 1
+        t_end = time.perf_counter() + 20.0
+        for i, n in enumerate(ns):
+            if time.perf_counter() > t_end and cnt >= 8:
+                break
+            sec, cores = _ref_seconds(n, C.hea(n, 2 * n, seed=i))
+            tot += sec
+            cnt += 1
+        # Scale the sample's mean time by the batch's mean state size ratio.
+        import statistics as st
+        w_all = st.mean(2.0 ** n for n in ns)
+        w_s = st.mean(2.0 ** n for n in ns[:cnt])
+        v = cnt / tot * (w_s / w_all)
+        print(json.dumps(_common("circuits/s", "circuits/s", v, args, 1000.0 * N / v, "c128 (f64)", cfg,
+                                 impl="reference",
+                                 cpu_baseline={"value": v, "unit": "circuits/s", "cores": cores, "kind": "reference",
+                                               "sample": f"first {cnt} circuits of the batch on the reference "
+                                                         f"CPUSimulator (complex128), rate scaled by mean 2^n"},
+                                 e2e={"value": v, "unit": "circuits/s", "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0})))
+        return
+    torch.cuda.set_device(0)
+    ns, circs = _hea_batch(K, C, N)
+    t0 = time.perf_counter()
+    b = K.Batch(circs, precision=K.C64, autotune=True)
+    create_s = time.perf_counter() - t0
+    tune = {n: [b.options.tune[n].fusion, b.options.tune[n].max_gates] for n in sorted(set(ns))}
+    info = b.info()
+    b.time(max(1, args.warmup))
+    with Clocks(0) as clk:
+        ms = b.time(args.steps)
+    value = N / (ms / 1000.0)
+    # Algorithmic bytes of the launch: every pass of a resident state reads
+    # and writes it once (the first pass only writes; the <Z> reduction reads
+    # it once more), 8 bytes per amplitude. Circuits run in shared memory
+    # move no state bytes.
+    nprog, nres = b.circuit_info()
+    alg = float(sum(int(p) * 16.0 * 2 ** int(r) for p, r in zip(nprog, nres) if r > 0))
+    peak, peak_kind = measured_hbm_peak()
+    z = b.expect_z_flat()
+    b.close()
+    # End to end: create (plan + upload) + run + readback, through the C ABI.
+    t0 = time.perf_counter()
+    b2 = K.Batch(circs, precision=K.C64, options=b.options)
+    b2.run()
+    b2.expect_z_flat()
+    b2.close()
+    e2e_s = time.perf_counter() - t0
+    # Baseline: one Simulator launch per circuit (plans and states prepared beforehand).
+    M = min(256, N)
+    sims = [K.Simulator(circs[i], 1, K.C64, 0) for i in range(M)]
+    for s_ in sims[:4]:
+        s_.run_async()
+        s_.synchronize()
+    t0 = time.perf_counter()
+    for s_ in sims:
+        s_.run_async()
+        s_.expect_z()
+    plain = M / (time.perf_counter() - t0)
+    for s_ in sims:
+        s_.close()
+    cpu = None
+    if not args.no_cpu_baseline and not _reference_unavailable():
+        tot, cnt, cores = 0.0, 0, 1
+        t_end = time.perf_counter() + 15.0
+        for i, n in enumerate(ns):
+            if time.perf_counter() > t_end and cnt >= 8:
+                break
+            sec, cores = _ref_seconds(n, C.hea(n, 2 * n, seed=i))
+            tot += sec
+            cnt += 1
+        w_all = statistics.mean(2.0 ** n for n in ns)
+        w_s = statistics.mean(2.0 ** n for n in ns[:cnt])
+        cpu = {"value": cnt / tot * (w_s / w_all), "unit": "circuits/s", "cores": cores, "kind": "reference",
+               "sample": f"first {cnt} circuits on the reference CPUSimulator (complex128), rate scaled by mean 2^n"}
+    h2d = info["programs"] * 6000
+    cfg.update({"autotuned": tune, "tasks": info["tasks"], "pass_programs": info["programs"],
+                "arena_bytes": info["arena_bytes"], "ctas": info["ctas"], "create_s": create_s,
+                "baseline_one_launch_per_circuit_cps": plain, "speedup_vs_one_launch_per_circuit": value / plain})
+    print(json.dumps(_common(
+        "circuits/s", "circuits/s", value, args, ms, "c64 (f32)", cfg,
+        e2e={"value": N / e2e_s, "unit": "circuits/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 8 * len(z),
+             "ms_per_step": e2e_s * 1000, "note": "plan + upload + run + <Z> readback per step"},
+        roofline={"bound": "fp32 issue (hbm shown)", "achieved": alg / (ms / 1000) / 1e9, "peak": peak, "unit": "GB/s",
+                  "frac": alg / (ms / 1000) / 1e9 / peak, "traffic": None, "peak_source": peak_kind,
+                  "kernel": "k_batch<float2> (persistent task queue)", "alg_bytes_per_launch": alg,
+                  "avg_launch_ms": ms},
+        gpu_launches=args.steps, clocks=clk.summary(), cpu_baseline=cpu)))
+
+
+def _geometric_n(rng, lo=12, hi=28, p=0.3):
+    while True:
+        k = int(rng.geometric(p)) - 1
+        if lo + k <= hi:
+            return lo + k
+
+
+def run_serve(args):
+    """Poisson request stream through the continuous-batching server."""
+    import threading
+    import numpy as np
+    import torch
+    import kate_b200 as K
+    from kate_b200 import circuits as C
+
+    R = args.requests
+    rates = [float(x) for x in args.rates.split(",")]
+    rng = np.random.default_rng(args.seed)
+    ns = [_geometric_n(rng) for _ in range(R)]
+    cfg = {"workload": f"Poisson stream of {R} requests per rate, n truncated geometric (p=0.3) on 12..28, "
+                       f"layered RX/RZ/CNOT-ladder circuit of depth n, complex64, 1024 samples + <Z_q> each, "
+                       f"150 GB admission budget", "requests": R, "rates": rates, "seed": args.seed,
+           "mean_n": float(np.mean(ns)), "max_n": int(max(ns)), "parallelism": "replicas"}
+    if args.impl == "reference":
+        if _reference_unavailable():
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built"}))
+            return
+        tot, cnt, cores = 0.0, 0, 1
+        t_end = time.perf_counter() + 20.0
+        for i, n in enumerate(ns):
+            if time.perf_counter() > t_end and cnt >= 8:
+                break
+            sec, cores = _ref_seconds(n, C.layered(n, n, seed=i))
+            tot += sec
+            cnt += 1
+        w_all = statistics.mean(2.0 ** n * n for n in ns)
+        w_s = statistics.mean(2.0 ** n * n for n in ns[:cnt])
+        v = cnt / tot * (w_s / w_all)
+        print(json.dumps(_common("served circuits/s", "circuits/s", v, args, 1000.0 / v, "c128 (f64)", cfg,
+                                 impl="reference",
+                                 cpu_baseline={"value": v, "unit": "circuits/s", "cores": cores, "kind": "reference",
+                                               "sample": f"first {cnt} requests on the reference CPUSimulator "
+                                                         f"(complex128, no sampling), rate scaled by mean n 2^n"},
+                                 e2e={"value": v, "unit": "circuits/s", "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0})))
+        return
+    torch.cuda.set_device(0)
+    circs = [K.Circuit(n, C.layered(n, n, seed=i)) for i, n in enumerate(ns)]
+    srv = K.Server(K.C64, 0, budget_bytes=150 * 10 ** 9)
+    # Warm-up: a few requests of every size class present.
+    for n in sorted(set(ns))[:6]:
+        srv.wait(srv.submit(K.Circuit(n, C.layered(n, n, seed=999)), 1024, 1), timeout=600)
+    sweep = []
+    with Clocks(0) as clk:
+        for rate in rates:
+            gaps = rng.exponential(1.0 / rate, R)
+            results = [None] * R
+            ids = [None] * R
+            ready = threading.Event()
+
+            def waiter():
+                ready.wait()
+                for i in range(R):
+                    while ids[i] is None:
+                        time.sleep(0.0002)
+                    results[i] = srv.wait(ids[i], timeout=3600)
+
+            th = threading.Thread(target=waiter)
+            th.start()
+            t_start = time.perf_counter()
+            due = t_start
+            ready.set()
+            for i in range(R):
+                due += gaps[i]
+                d = due - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+                ids[i] = srv.submit(circs[i], 1024, 1000 + i)
+            th.join()
+            t_sub = np.array([r[2][0] for r in results])
+            t_done = np.array([r[2][2] for r in results])
+            lat = (t_done - t_sub) * 1000.0
+            span = float(t_done.max() - t_sub.min())
+            sweep.append({"rate": rate, "circuits_per_s": R / span, "p50_ms": float(np.percentile(lat, 50)),
+                          "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()),
+                          "offered_s": float(gaps.sum())})
+    st = srv.stats()
+    srv.close()
+    # Baseline: one-at-a-time plain launches (a Simulator per request, run,
+    # <Z>, 1024 samples), served FIFO; latencies at each rate from the
+    # measured service times under the same arrival process.
+    svc = []
+    for i in range(R):
+        t0 = time.perf_counter()
+        s_ = K.Simulator(circs[i], 1, K.C64, 0)
+        s_.execute()
+        s_.expect_z()
+        s_.sample(1024, seed=1000 + i)
+        s_.close()
+        svc.append(time.perf_counter() - t0)
+    base = []
+    rng2 = np.random.default_rng(args.seed + 1)
+    for rate in rates:
+        arr = np.cumsum(rng2.exponential(1.0 / rate, R))
+        done, t = [], 0.0
+        for a, s_ in zip(arr, svc):
+            t = max(t, a) + s_
+            done.append(t)
+        lat = (np.array(done) - arr) * 1000
+        base.append({"rate": rate, "circuits_per_s": R / (done[-1] - arr[0]),
+                     "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))})
+    best = max(sweep, key=lambda x: x["circuits_per_s"])
+    plain_cps = R / sum(svc)
+    cfg.update({"sweep": sweep, "baseline_one_at_a_time": base, "baseline_service_cps": plain_cps,
+                "speedup_vs_one_at_a_time": best["circuits_per_s"] / plain_cps, "engine_steps": st["steps"],
+                "peak_resident_bytes": st["peak_resident_bytes"]})
+    cpu = None
+    if not args.no_cpu_baseline and not _reference_unavailable():
+        tot, cnt, cores = 0.0, 0, 1
+        t_end = time.perf_counter() + 15.0
+        for i, n in enumerate(ns):
+            if time.perf_counter() > t_end and cnt >= 8:
+                break
+            sec, cores = _ref_seconds(n, C.layered(n, n, seed=i))
+            tot += sec
+            cnt += 1
+        w_all = statistics.mean(2.0 ** n * n for n in ns)
+        w_s = statistics.mean(2.0 ** n * n for n in ns[:cnt])
+        cpu = {"value": cnt / tot * (w_s / w_all), "unit": "circuits/s", "cores": cores, "kind": "reference",
+               "sample": f"first {cnt} requests on the reference CPUSimulator (complex128, no sampling), rate "
+                         f"scaled by mean n 2^n"}
+    print(json.dumps(_common(
+        "served circuits/s", "circuits/s", best["circuits_per_s"], args, 1000.0 / best["circuits_per_s"],
+        "c64 (f32)", cfg, p50_ms=best["p50_ms"], p99_ms=best["p99_ms"],
+        e2e={"value": best["circuits_per_s"], "unit": "circuits/s",
+             "h2d_bytes_per_step": None, "d2h_bytes_per_step": 8 * (1024 + 28),
+             "note": "the serving rate is measured end to end: submit from host circuits to results on the host"},
+        gpu_launches=st["steps"], clocks=clk.summary(), cpu_baseline=cpu)))
 
 
 if __name__ == "__main__":

@@ -75,6 +75,7 @@ typedef struct kate_circuit kate_circuit;
 typedef struct kate_sim kate_sim;
 typedef struct kate_plan kate_plan;
 typedef struct kate_batch kate_batch;
+typedef struct kate_server kate_server;
 
 /* Message of the last failed call on this thread ("" if none). */
 KATE_API const char* kate_last_error(void);
@@ -287,7 +288,7 @@ KATE_API kate_status kate_proba_state_noalloc(const void* d_state, int nqbits, c
  * kate_sim_expect_z (by program label). Circuits have 1 to
  * KATE_BATCH_MAX_QUBITS qubits; those of at most 12 run entirely in one
  * CTA's shared memory. */
-#define KATE_BATCH_MAX_QUBITS 24
+#define KATE_BATCH_MAX_QUBITS 28
 typedef struct {
     int fusion;    /* gateFusion width applied to circuits without groups or instructions (1: none; 0: default) */
     int max_gates; /* gates per pass program (0: default) */
@@ -321,8 +322,52 @@ KATE_API kate_status kate_batch_expect_z(kate_batch* b, double* out);
 KATE_API kate_status kate_batch_num_outputs(const kate_batch* b, long long* out);
 /* info[0] tasks, info[1] pass programs, info[2] arena bytes, info[3] CTAs. */
 KATE_API kate_status kate_batch_info(const kate_batch* b, long long* info);
+/* Per circuit i: programs[i] pass programs, resident_qubits[i] qubits of
+ * its device state (0 when it runs in shared memory). Arrays of count. */
+KATE_API kate_status kate_batch_circuit_info(const kate_batch* b, int* programs, int* resident_qubits);
 /* Average device time of `runs` back-to-back runs (CUDA events). */
 KATE_API kate_status kate_batch_time(kate_batch* b, int runs, float* ms);
+
+/* ---- serving: a request stream with continuous batching ----
+ * Replaces a caller's loop that blocks on `Simulator(circuit).execute()`
+ * per request (HIPcode/simulator.hpp:301-353). A server owns an engine
+ * thread: kate_server_submit queues a request (12 to 28 qubits, `shots`
+ * samples from the seeded splitmix64 stream `seed`) and returns at once;
+ * host threads plan it; the engine admits requests in submission order
+ * while their states fit `budget_bytes` of device memory, and runs steps,
+ * each one launch in which every scheduled request advances by some of its
+ * group passes, so requests join and leave between steps. A finished
+ * request yields <Z_q> per program label (as kate_sim_expect_z) and its
+ * samples (basis-state indices in label order, as kate_sim_sample). */
+typedef struct {
+    unsigned long long budget_bytes; /* resident states (default 150 GiB) */
+    unsigned long long aux_bytes;    /* programs, outputs and sums (default 2 GiB) */
+    long long step_tiles;            /* 4096-amplitude tile passes per step (default 65536) */
+    int chunk;                       /* cosets per pass task (default 4) */
+    int zchunks;                     /* 65536-amplitude chunks per <Z> task (default 4) */
+    int schunks;                     /* chunks per sampling task (default 16) */
+    int planners;                    /* planning threads (0: hardware concurrency, at most 16) */
+    int fusion;                      /* gateFusion width for unfused circuits (1: none) */
+    int max_gates;                   /* gates per pass program */
+} kate_server_options;
+
+KATE_API kate_status kate_server_options_default(kate_server_options* opt);
+/* opt: nullable (defaults). Allocates the state and aux arenas up front. */
+KATE_API kate_status kate_server_create(int precision, int device, const kate_server_options* opt, kate_server** out);
+/* Stops the engine after its running step; requests not collected are dropped. */
+KATE_API kate_status kate_server_destroy(kate_server* s);
+/* Thread-safe; does not wait for the GPU. */
+KATE_API kate_status kate_server_submit(kate_server* s, const kate_circuit* c, int shots, uint64_t seed, long long* id);
+/* Waits up to timeout_s for request id; KATE_ETIMEDOUT if it is not done.
+ * On success writes nqbits, z (nqbits doubles), samples (shots entries) and
+ * times (3 doubles: submitted, admitted, done; seconds since the server
+ * started), each nullable, and forgets the request. */
+KATE_API kate_status kate_server_wait(kate_server* s, long long id, double timeout_s, int* nqbits, double* z,
+                                      uint64_t* samples, double* times);
+/* out[8]: submitted, completed, live, queued, steps, resident bytes, peak resident bytes, failed. */
+KATE_API kate_status kate_server_stats(const kate_server* s, long long* out);
+/* Seconds since the server started (the clock of kate_server_wait's times). */
+KATE_API kate_status kate_server_now(const kate_server* s, double* t);
 
 #ifdef __cplusplus
 }

@@ -45,6 +45,7 @@ def _check(st: int):
 
 _ip = ctypes.POINTER(ctypes.c_int)
 _dp = ctypes.POINTER(ctypes.c_double)
+_u64p = ctypes.POINTER(ctypes.c_uint64)
 
 
 def _iarr(v) -> np.ndarray:
@@ -455,8 +456,76 @@ class Batch:
         _check(self._lib.kate_batch_info(self._h, v))
         return {"tasks": v[0], "programs": v[1], "arena_bytes": v[2], "ctas": v[3]}
 
+    def circuit_info(self):
+        """(pass programs, resident qubits) per circuit; resident qubits is 0
+        for circuits run in shared memory."""
+        n = len(self.circuits)
+        p = np.zeros(n, dtype=np.int32)
+        r = np.zeros(n, dtype=np.int32)
+        _check(self._lib.kate_batch_circuit_info(self._h, p.ctypes.data_as(_ip), r.ctypes.data_as(_ip)))
+        return p, r
+
     def time(self, runs: int = 1) -> float:
         ms = ctypes.c_float()
         _check(self._lib.kate_batch_time(self._h, int(runs), ctypes.byref(ms)))
         return ms.value
+
+
+class Server:
+    """Continuous-batching request server on one GPU (see kate_server_* in
+    include/kate_b200.h). ``submit`` returns a request id at once; ``wait``
+    returns ``(z, samples, times)`` with times = (submitted, admitted, done)
+    in seconds on the server's clock."""
+
+    def __init__(self, precision: int = C64, device: int = 0, options=None, **kw):
+        self._lib = _lib.lib()
+        self._h = None
+        if options is None:
+            options = _lib.ServerOptions()
+            _check(self._lib.kate_server_options_default(ctypes.byref(options)))
+        for k, v in kw.items():
+            setattr(options, k, v)
+        self.options = options
+        h = ctypes.c_void_p()
+        _check(self._lib.kate_server_create(int(precision), int(device), ctypes.byref(options), ctypes.byref(h)))
+        self._h = h
+        self._meta = {}
+
+    def __del__(self):
+        self.close()
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            self._lib.kate_server_destroy(h)
+            self._h = None
+
+    def submit(self, circuit: Circuit, shots: int = 1024, seed: int = 0) -> int:
+        v = ctypes.c_longlong()
+        _check(self._lib.kate_server_submit(self._h, circuit.handle, int(shots), ctypes.c_uint64(seed & (2**64 - 1)),
+                                            ctypes.byref(v)))
+        self._meta[v.value] = (circuit.nqbits, int(shots))
+        return v.value
+
+    def wait(self, rid: int, timeout: float = 60.0):
+        n, shots = self._meta[rid]
+        z = np.zeros(n, dtype=np.float64)
+        s = np.zeros(max(1, shots), dtype=np.uint64)
+        t = np.zeros(3, dtype=np.float64)
+        nq = ctypes.c_int()
+        _check(self._lib.kate_server_wait(self._h, int(rid), float(timeout), ctypes.byref(nq), z.ctypes.data_as(_dp),
+                                          s.ctypes.data_as(_u64p), t.ctypes.data_as(_dp)))
+        del self._meta[rid]
+        return z, s[:shots], tuple(t)
+
+    def stats(self) -> dict:
+        v = (ctypes.c_longlong * 8)()
+        _check(self._lib.kate_server_stats(self._h, v))
+        keys = ("submitted", "completed", "live", "queued", "steps", "resident_bytes", "peak_resident_bytes", "failed")
+        return dict(zip(keys, list(v)))
+
+    def now(self) -> float:
+        t = ctypes.c_double()
+        _check(self._lib.kate_server_now(self._h, ctypes.byref(t)))
+        return t.value
 

@@ -85,9 +85,17 @@ SIGNATURES = {
     "kate_batch_num_outputs": [_vp, _c.POINTER(_c.c_longlong)],
     "kate_batch_info": [_vp, _c.POINTER(_c.c_longlong)],
     "kate_batch_time": [_vp, _i, _c.POINTER(_c.c_float)],
+    "kate_batch_circuit_info": [_vp, _ip, _ip],
+    "kate_server_options_default": [_vp],
+    "kate_server_create": [_i, _i, _vp, _vpp],
+    "kate_server_destroy": [_vp],
+    "kate_server_submit": [_vp, _vp, _i, _u64, _c.POINTER(_c.c_longlong)],
+    "kate_server_wait": [_vp, _c.c_longlong, _d, _ip, _dp, _u64p, _dp],
+    "kate_server_stats": [_vp, _c.POINTER(_c.c_longlong)],
+    "kate_server_now": [_vp, _dp],
 }
 
-KATE_BATCH_MAX_QUBITS = 24
+KATE_BATCH_MAX_QUBITS = 28
 
 
 class BatchTuning(_c.Structure):
@@ -117,3 +125,10 @@ def lib():
 
 def last_error() -> str:
     return lib().kate_last_error().decode(errors="replace")
+
+
+class ServerOptions(_c.Structure):
+    """kate_server_options (include/kate_b200.h)."""
+    _fields_ = [("budget_bytes", _c.c_ulonglong), ("aux_bytes", _c.c_ulonglong), ("step_tiles", _c.c_longlong),
+                ("chunk", _c.c_int), ("zchunks", _c.c_int), ("schunks", _c.c_int), ("planners", _c.c_int),
+                ("fusion", _c.c_int), ("max_gates", _c.c_int)]

@@ -27,21 +27,6 @@ std::string cuda_err(const char* what, cudaError_t e) {
 
 const BatchTune kDefaultTune{};
 
-// One circuit, planned and packed. Offsets are local to the circuit until
-// the packs are concatenated.
-struct CircPack {
-    std::string err;
-    int n_out = 0;   // the circuit's qubits: one <Z> output each
-    int n_sim = 0;   // qubits simulated (narrow circuits are padded to a full tile)
-    bool small = false;
-    std::vector<uint8_t> zbit;
-    std::vector<BatchProg> progs;
-    std::vector<uint8_t> blob;
-    std::vector<DevOp> sops;
-    std::vector<Cx> pool;
-    std::vector<std::pair<uint64_t, int>> generic;  // (blob offset, count) of DevOp arrays
-};
-
 uint64_t put_bytes(std::vector<uint8_t>& blob, const void* p, size_t bytes) {
     const size_t off = (blob.size() + 15) & ~size_t(15);
     blob.resize(off + bytes);
@@ -49,12 +34,15 @@ uint64_t put_bytes(std::vector<uint8_t>& blob, const void* p, size_t bytes) {
     return off;
 }
 
-std::string pack_circuit(const Program& in, const BatchTune& tune, CircPack& out) {
+}  // namespace
+
+std::string pack_circuit(const Program& in, const BatchTune& tune, bool resident, CircPack& out) {
     Program p = in;
     const int n = p.nqbits;
-    if (n < 1 || n > KATE_BATCH_MAX_QUBITS) return "batch circuits have 1 to 24 qubits";
+    if (n < 1 || n > KATE_BATCH_MAX_QUBITS) return "batch circuits have 1 to 28 qubits";
+    if (resident && n < KATE_TILE_BITS) return "resident circuits have at least 12 qubits";
     out.n_out = n;
-    out.small = n <= KATE_BATCH_SMALL_MAX;
+    out.small = !resident && n <= KATE_BATCH_SMALL_MAX;
     std::string e;
     if (p.instructions.empty() && p.groups.empty() && tune.fusion >= 2) {
         e = pass_schedule(p);
@@ -136,6 +124,8 @@ std::string pack_circuit(const Program& in, const BatchTune& tune, CircPack& out
     return "";
 }
 
+namespace {
+
 // Plans every circuit on host threads.
 std::vector<CircPack> pack_all(const std::vector<const Program*>& circuits, const BatchOptions& opt) {
     std::vector<CircPack> packs(circuits.size());
@@ -144,7 +134,7 @@ std::vector<CircPack> pack_all(const std::vector<const Program*>& circuits, cons
         for (size_t i; (i = next.fetch_add(1)) < circuits.size();) {
             const BatchTune& tu = opt.for_n(circuits[i]->nqbits);
             try {
-                packs[i].err = pack_circuit(*circuits[i], tu, packs[i]);
+                packs[i].err = pack_circuit(*circuits[i], tu, false, packs[i]);
             } catch (const std::exception& ex) {
                 packs[i].err = ex.what();
             }
@@ -176,6 +166,7 @@ struct BatchImpl {
     int grid = 0;
     std::vector<BatchTask> tasks;
     std::vector<BatchCirc> circs;
+    std::vector<int> cprogs, cres;  // per circuit: programs, resident qubits
     std::vector<BatchProg> progs;
     std::vector<uint8_t> blob;
     std::vector<DevOp> sops;
@@ -281,7 +272,8 @@ std::string Batch::create(const std::vector<const Program*>& circuits, int preci
         }
         BatchCirc bc{};
         bc.n = P.n_out;
-        bc.zoff = (int32_t)S->nout;
+        bc.zoff = S->nout;
+        bc.poff = -1;
         S->nout += P.n_out;
         for (int x = 0; x < P.n_out; x++) bc.zbit[x] = P.zbit[x];
         if (!P.small) {
@@ -289,11 +281,12 @@ std::string Batch::create(const std::vector<const Program*>& circuits, int preci
             S->arena_amps += 1ull << P.n_sim;
         }
         S->circs.push_back(bc);
+        S->cprogs.push_back((int)P.progs.size());
+        S->cres.push_back(P.small ? 0 : P.n_sim);
         std::vector<uint8_t>().swap(P.blob);
         std::vector<Cx>().swap(P.pool);
         std::vector<DevOp>().swap(P.sops);
     }
-    if (S->nout > INT32_MAX) return fail("too many outputs");
     if (S->sops.size() > (size_t)INT32_MAX) return fail("too many shared-memory ops");
 
     // Task queue. Large circuits, window by window, level by level; small
@@ -490,6 +483,10 @@ int64_t Batch::num_tasks() const { return (int64_t)d_->tasks.size(); }
 uint64_t Batch::arena_bytes() const { return d_->arena_amps * d_->amp_bytes(); }
 int Batch::grid() const { return d_->grid; }
 int64_t Batch::num_programs() const { return (int64_t)d_->progs.size(); }
+void Batch::circuit_info(int i, int* programs, int* resident_qubits) const {
+    *programs = d_->cprogs[i];
+    *resident_qubits = d_->cres[i];
+}
 
 std::string batch_autotune(const std::vector<const Program*>& circuits, int precision, int device,
                            BatchOptions* opt) {

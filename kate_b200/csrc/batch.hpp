@@ -33,6 +33,25 @@ struct BatchOptions {
     const BatchTune& for_n(int n) const;
 };
 
+// One circuit, planned and packed for the batch kernel. Offsets (blob
+// bytes, smem-op and pool indices) are local to the circuit.
+struct CircPack {
+    std::string err;
+    int n_out = 0;   // the circuit's qubits: one <Z> output each
+    int n_sim = 0;   // qubits simulated (narrow circuits are padded to a full tile)
+    bool small = false;  // runs whole in one CTA's shared memory (BT_SMALL)
+    std::vector<uint8_t> zbit;     // output x reads this bit of the final layout
+    std::vector<BatchProg> progs;  // one per pass
+    std::vector<uint8_t> blob;
+    std::vector<DevOp> sops;
+    std::vector<Cx> pool;
+    std::vector<std::pair<uint64_t, int>> generic;  // (blob offset, count) of DevOp arrays
+};
+
+// Plans one circuit. resident: keep the state in device memory even when it
+// would fit a tile (at least 12 qubits), so it can be sampled afterwards.
+std::string pack_circuit(const Program& in, const BatchTune& tune, bool resident, CircPack& out);
+
 struct BatchImpl;
 
 class Batch {
@@ -51,6 +70,8 @@ public:
     uint64_t arena_bytes() const;
     int grid() const;
     int64_t num_programs() const;
+    // Per circuit: pass programs and qubits simulated (0 for circuits run in shared memory).
+    void circuit_info(int i, int* programs, int* resident_qubits) const;
 
 private:
     BatchImpl* d_ = nullptr;

@@ -8,6 +8,7 @@
 #include "batch.hpp"
 #include "circuit.hpp"
 #include "plan.hpp"
+#include "serve.hpp"
 #include "sim.hpp"
 
 struct kate_circuit {
@@ -18,6 +19,10 @@ struct kate_sim {
 };
 struct kate_batch {
     kate::Batch* b = nullptr;
+    int ncirc = 0;
+};
+struct kate_server {
+    kate::Server* s = nullptr;
 };
 struct kate_plan {
     kate::Plan plan;
@@ -671,6 +676,7 @@ kate_status kate_batch_create(const kate_circuit* const* circuits, int count, in
         if (!e.empty()) return sim_status(e);
         auto* h = new kate_batch();
         h->b = b;
+        h->ncirc = count;
         *out = h;
         return KATE_OK;
     });
@@ -735,6 +741,12 @@ kate_status kate_batch_info(const kate_batch* b, long long* info) {
     return KATE_OK;
 }
 
+kate_status kate_batch_circuit_info(const kate_batch* b, int* programs, int* resident_qubits) {
+    REQUIRE(b && programs && resident_qubits, "null pointer");
+    for (int i = 0; i < b->ncirc; i++) b->b->circuit_info(i, programs + i, resident_qubits + i);
+    return KATE_OK;
+}
+
 kate_status kate_batch_time(kate_batch* b, int runs, float* ms) {
     return guarded([&] {
         REQUIRE(b && ms && runs > 0, "null pointer or no runs");
@@ -742,6 +754,103 @@ kate_status kate_batch_time(kate_batch* b, int runs, float* ms) {
         if (!e.empty()) return fail(KATE_ECUDA, e);
         return KATE_OK;
     });
+}
+
+// ---- serving ----
+
+kate_status kate_server_options_default(kate_server_options* opt) {
+    REQUIRE(opt, "null pointer");
+    std::memset(opt, 0, sizeof(*opt));
+    kate::ServeOptions d;
+    opt->budget_bytes = d.budget_bytes;
+    opt->aux_bytes = d.aux_bytes;
+    opt->step_tiles = d.step_tiles;
+    opt->chunk = d.chunk;
+    opt->zchunks = d.zchunks;
+    opt->schunks = d.schunks;
+    opt->planners = d.planners;
+    opt->fusion = d.tune.fusion;
+    opt->max_gates = d.tune.max_gates;
+    return KATE_OK;
+}
+
+kate_status kate_server_create(int precision, int device, const kate_server_options* opt, kate_server** out) {
+    return guarded([&] {
+        REQUIRE(out, "null pointer");
+        REQUIRE(precision == KATE_C128 || precision == KATE_C64, "unknown precision");
+        kate::ServeOptions o;
+        if (opt) {
+            if (opt->budget_bytes) o.budget_bytes = opt->budget_bytes;
+            if (opt->aux_bytes) o.aux_bytes = opt->aux_bytes;
+            if (opt->step_tiles > 0) o.step_tiles = opt->step_tiles;
+            if (opt->chunk > 0) o.chunk = opt->chunk;
+            if (opt->zchunks > 0) o.zchunks = opt->zchunks;
+            if (opt->schunks > 0) o.schunks = opt->schunks;
+            o.planners = opt->planners;
+            if (opt->fusion > 0) o.tune.fusion = opt->fusion;
+            if (opt->max_gates > 0) o.tune.max_gates = opt->max_gates;
+        }
+        kate::Server* s = nullptr;
+        std::string e = kate::Server::create(precision, device, o, &s);
+        if (!e.empty()) return sim_status(e);
+        auto* h = new kate_server();
+        h->s = s;
+        *out = h;
+        return KATE_OK;
+    });
+}
+
+kate_status kate_server_destroy(kate_server* s) {
+    if (s) {
+        delete s->s;
+        delete s;
+    }
+    return KATE_OK;
+}
+
+kate_status kate_server_submit(kate_server* s, const kate_circuit* c, int shots, uint64_t seed, long long* id) {
+    return guarded([&] {
+        REQUIRE(s && c && id, "null pointer");
+        int64_t v = 0;
+        std::string e = s->s->submit(c->prog, shots, seed, &v);
+        if (!e.empty()) return fail(KATE_EINVAL, e);
+        *id = (long long)v;
+        return KATE_OK;
+    });
+}
+
+kate_status kate_server_wait(kate_server* s, long long id, double timeout_s, int* nqbits, double* z,
+                             uint64_t* samples, double* times) {
+    return guarded([&] {
+        REQUIRE(s, "null server");
+        kate::ServeResult r;
+        std::string e = s->s->wait(id, timeout_s, &r);
+        if (e == "timeout") return fail(KATE_ETIMEDOUT, "request not finished within the timeout");
+        if (!e.empty()) return sim_status(e);
+        if (nqbits) *nqbits = r.n;
+        if (z) std::memcpy(z, r.z.data(), r.z.size() * sizeof(double));
+        if (samples && !r.samples.empty()) std::memcpy(samples, r.samples.data(), r.samples.size() * sizeof(uint64_t));
+        if (times) {
+            times[0] = r.t_submit;
+            times[1] = r.t_admit;
+            times[2] = r.t_done;
+        }
+        return KATE_OK;
+    });
+}
+
+kate_status kate_server_stats(const kate_server* s, long long* out) {
+    REQUIRE(s && out, "null pointer");
+    int64_t v[8];
+    s->s->stats(v);
+    for (int i = 0; i < 8; i++) out[i] = (long long)v[i];
+    return KATE_OK;
+}
+
+kate_status kate_server_now(const kate_server* s, double* t) {
+    REQUIRE(s && t, "null pointer");
+    *t = s->s->now();
+    return KATE_OK;
 }
 
 }  // extern "C"

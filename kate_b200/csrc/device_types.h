@@ -133,25 +133,32 @@ typedef struct {
 // `need` tasks of its circuit have finished, so it only ever waits on tasks
 // taken from the queue before it.
 #define KATE_BATCH_SMALL_MAX 12
-#define KATE_BATCH_MAX_QUBITS 24
+#define KATE_BATCH_MAX_QUBITS 28
 #define BT_SMALL 0
 #define BT_PASS 1
-#define BT_ZRED 2
+#define BT_ZRED 2    // also writes per-chunk probability sums when the circuit has psum storage
+#define BT_PREFIX 3  // exclusive prefix of the chunk sums (one task per circuit)
+#define BT_SAMPLE 4  // inverse-CDF sampling of the shots that fall in a range of chunks
 
 typedef struct {
     int32_t kind;
     int32_t circ;
     int32_t prog;     // BT_PASS: program index; BT_SMALL: first program index
     int32_t nprog;    // BT_SMALL: programs run back to back
-    uint32_t c0, c1;  // BT_PASS: coset range; BT_ZRED: range of 2^16-amplitude chunks
+    uint32_t c0, c1;  // BT_PASS: coset range; BT_ZRED / BT_SAMPLE: range of 2^16-amplitude chunks
     int32_t need;     // finished tasks of this circuit required before starting
     int32_t first;    // BT_PASS: the input is |0...0> (nothing is loaded)
 } BatchTask;
 
 typedef struct {
     uint64_t off;     // state offset in the arena (amplitudes)
-    int32_t n;        // <Z> outputs (the circuit's qubits)
-    int32_t zoff;     // first <Z> output of this circuit
+    int32_t n;        // qubits: <Z> outputs, and 2^n amplitudes for the reductions
+    int32_t shots;    // samples to draw (BT_SAMPLE)
+    int64_t zoff;     // first <Z> output of this circuit
+    int64_t poff;     // chunk sums at psum[poff + ch], their exclusive prefix at psum[poff + nch + ch],
+                      // the total at psum[poff + 2 nch]; -1: no sums
+    int64_t uoff;     // the shots' uniforms in [0, 1), ascending: unif[uoff + s]
+    int64_t soff;     // sampled (physical) amplitude indices: sout[soff + s]
     uint8_t zbit[40]; // output q reads bit zbit[q] of the tile (SMALL) or state (otherwise)
 } BatchCirc;
 

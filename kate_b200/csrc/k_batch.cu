@@ -12,7 +12,10 @@
 //             L1. The first pass of a circuit starts from |0...0> in shared
 //             memory instead of loading;
 //   BT_ZRED   <Z_q> partial sums over a range of amplitudes, added to the
-//             circuit's outputs with FP64 atomics.
+//             circuit's outputs with FP64 atomics (and, for sampling, each
+//             chunk's probability sum);
+//   BT_PREFIX exclusive prefix of a circuit's chunk sums;
+//   BT_SAMPLE inverse-CDF sampling of the shots falling in a chunk range.
 // Finished tasks bump their circuit's counter after a memory fence. Tasks
 // are queued level by level per circuit, so a task waits only on tasks
 // dequeued before it: every CTA that holds a task can finish it, whatever
@@ -136,11 +139,12 @@ __device__ __noinline__ void small_z(const C2* tile, int nz, const uint8_t* zbit
 // <Z_q> partial sums of an n-qubit state over 2^16-amplitude chunks
 // [ch0, ch1), added to out[q] (q reads physical bit zbit[q]). Thread t takes
 // amplitudes chunk * 2^16 + t + 256 k: physical bits 0..7 come from t, 8..15
-// from k, the rest from the chunk.
+// from k, the rest from the chunk. With psum, also stores each chunk's
+// probability sum at psum[ch] (block-reduced in a fixed order).
 template <typename C2>
 __device__ __noinline__ void zred(const C2* st, int n, uint32_t ch0, uint32_t ch1, const uint8_t* zbit, double* red,
-                                  double* out) {
-    const uint32_t t = threadIdx.x;
+                                  double* out, double* psum) {
+    const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
     double z[KATE_BATCH_MAX_QUBITS];
 #pragma unroll
     for (int q = 0; q < KATE_BATCH_MAX_QUBITS; q++) z[q] = 0.0;
@@ -164,9 +168,136 @@ __device__ __noinline__ void zred(const C2* st, int n, uint32_t ch0, uint32_t ch
             else if (b < 16) z[b] += kb[b - 8];
             else z[b] += ((ch >> (b - 16)) & 1u) ? -tot : tot;
         }
+        if (psum) {
+            double w = tot;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) w += __shfl_down_sync(0xffffffffu, w, o);
+            if (lane == 0) red[warp] = w;
+            __syncthreads();
+            if (t == 0) {
+                double sc = 0.0;
+                for (int i = 0; i < NT / 32; i++) sc += red[i];
+                psum[ch] = sc;
+            }
+            __syncthreads();
+        }
     }
     block_sums<KATE_BATCH_MAX_QUBITS>(z, n, red);
     if ((int)t < n) atomicAdd(out + t, red[KATE_BATCH_MAX_QUBITS * (NT / 32) + zbit[t]]);
+}
+
+// Block-wide exclusive scan of one double per thread (fixed order); also
+// returns the block total.
+__device__ double block_exscan(double v, double* red, double* total) {
+    const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+    double x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= (uint32_t)o) x += y;
+    }
+    if (lane == 31) red[warp] = x;
+    __syncthreads();
+    if (t == 0) {
+        double s = 0.0;
+        for (int i = 0; i < NT / 32; i++) {
+            const double w = red[i];
+            red[i] = s;
+            s += w;
+        }
+        red[NT / 32] = s;
+    }
+    __syncthreads();
+    const double r = red[warp] + x - v;
+    *total = red[NT / 32];
+    __syncthreads();
+    return r;
+}
+
+// Exclusive prefix of nch chunk sums psum[0..nch) into psum[nch..2 nch),
+// the total into psum[2 nch].
+__device__ __noinline__ void chunk_prefix(double* psum, uint32_t nch, double* red) {
+    const uint32_t t = threadIdx.x;
+    const uint32_t per = (nch + NT - 1) / NT, b0 = t * per, b1 = min(nch, b0 + per);
+    double loc = 0.0;
+    for (uint32_t c = b0; c < b1; c++) loc += psum[c];
+    double total;
+    double run = block_exscan(loc, red, &total);
+    for (uint32_t c = b0; c < b1; c++) {
+        psum[nch + c] = run;
+        run += psum[c];
+    }
+    if (t == 0) psum[2 * nch] = total;
+}
+
+// Inverse-CDF sampling over chunks [ch0, ch1): shot s (uniforms u ascending)
+// targets x = u * total; it falls in chunk ch when pre[ch] <= x < pre[ch] +
+// sum[ch] (targets at or past the total go to the last chunk). Inside a
+// chunk, thread t owns a contiguous run of amplitudes; a block scan of the
+// runs' sums locates each target's run, whose owner walks it.
+template <typename C2>
+__device__ __noinline__ void sample_chunks(const C2* st, int n, uint32_t ch0, uint32_t ch1, const double* psum,
+                                           const double* unif, int shots, uint64_t* out, double* red, int* srange) {
+    const uint32_t t = threadIdx.x;
+    const uint64_t dim = 1ull << n;
+    const uint32_t nch = (uint32_t)(dim >> 16 ? dim >> 16 : 1);
+    const double total = psum[2 * nch];
+    for (uint32_t ch = ch0; ch < ch1; ch++) {
+        const double lo_v = psum[nch + ch];
+        const double hi_v = lo_v + psum[ch];
+        const bool last = ch + 1 == nch;
+        if (t == 0) {
+            int lo = 0, hi = shots;  // first s with u_s * total >= lo_v
+            while (lo < hi) {
+                const int m = (lo + hi) >> 1;
+                if (unif[m] * total >= lo_v) hi = m;
+                else lo = m + 1;
+            }
+            int e = lo, e1 = shots;  // first s with u_s * total >= hi_v
+            if (!last)
+                while (e < e1) {
+                    const int m = (e + e1) >> 1;
+                    if (unif[m] * total >= hi_v) e1 = m;
+                    else e = m + 1;
+                }
+            srange[0] = lo;
+            srange[1] = last ? shots : e;
+        }
+        __syncthreads();
+        const int s0 = srange[0], s1 = srange[1];
+        __syncthreads();
+        if (s0 >= s1) continue;
+        const uint64_t x0 = (uint64_t)ch << 16;
+        const uint64_t len = dim - x0 < (1ull << 16) ? dim - x0 : (1ull << 16);
+        const uint64_t per = (len + NT - 1) / NT;
+        const uint64_t a0 = x0 + (t * per < len ? t * per : len), a1 = x0 + ((t + 1) * per < len ? (t + 1) * per : len);
+        double w = 0.0;
+        for (uint64_t x = a0; x < a1; x++) {
+            const double2 a = ldst(st + x);
+            w += a.x * a.x + a.y * a.y;
+        }
+        double btot;
+        const double base = block_exscan(w, red, &btot);
+        const bool tail = (t == NT - 1) || (a1 == x0 + len);
+        for (int s = s0; s < s1; s++) {
+            const double y = unif[s] * total - lo_v;
+            const bool mine = (y >= base && y < base + w) || (tail && y >= base + w && a1 > a0 && a1 == x0 + len);
+            if (!mine || a1 <= a0) continue;
+            double acc = base;
+            uint64_t pick = a1 - 1;
+            for (uint64_t x = a0; x < a1; x++) {
+                const double2 a = ldst(st + x);
+                const double p = a.x * a.x + a.y * a.y;
+                acc += p;
+                if (acc > y && p > 0.0) {
+                    pick = x;
+                    break;
+                }
+            }
+            out[s] = pick;
+        }
+        __syncthreads();
+    }
 }
 
 template <typename C2>
@@ -182,12 +313,14 @@ __global__ void __launch_bounds__(NT, sizeof(C2) == 8 ? 2 : 1)
     k_batch(C2* __restrict__ arena, const BatchTask* __restrict__ tasks, int ntasks, const BatchCirc* __restrict__ circs,
             const BatchProg* __restrict__ progs, const unsigned char* __restrict__ blob, const DevOp* __restrict__ sops,
             const double2* __restrict__ pool, int* __restrict__ head, int* __restrict__ done,
-            double* __restrict__ zout, int* __restrict__ err) {
+            double* __restrict__ zout, int* __restrict__ err, double* __restrict__ psum,
+            const double* __restrict__ unif, uint64_t* __restrict__ sout) {
     C2* tile = reinterpret_cast<C2*>(batch_smem_raw);
     TileTables<C2>& T = *reinterpret_cast<TileTables<C2>*>(batch_smem_raw + TS * sizeof(C2));
     __shared__ int s_task;
     __shared__ int s_abort;
     __shared__ uint8_t s_zbit[40];
+    __shared__ int s_range[2];
     __shared__ double red[KATE_BATCH_MAX_QUBITS * (NT / 32) + KATE_BATCH_MAX_QUBITS];
     const uint32_t t = threadIdx.x;
     const uint32_t tb = (uint32_t)__cvta_generic_to_shared(tile);
@@ -217,7 +350,7 @@ __global__ void __launch_bounds__(NT, sizeof(C2) == 8 ? 2 : 1)
         __syncthreads();
         if (s_abort) break;
         const int nz = circs[K.circ].n;
-        const int zoff = circs[K.circ].zoff;
+        const int64_t zoff = circs[K.circ].zoff;
 
         if (K.kind != BT_ZRED) {
             // SMALL: step s runs program prog + s on the resident tile.
@@ -258,7 +391,15 @@ __global__ void __launch_bounds__(NT, sizeof(C2) == 8 ? 2 : 1)
             __syncthreads();
             if (small) small_z(tile, nz, s_zbit, red, zout + zoff);
         } else {
-            zred(arena + circs[K.circ].off, nz, K.c0, K.c1, s_zbit, red, zout + zoff);
+            const BatchCirc& C = circs[K.circ];
+            const uint32_t nch = (uint32_t)(((1ull << nz) >> 16) ? ((1ull << nz) >> 16) : 1);
+            if (K.kind == BT_ZRED)
+                zred(arena + C.off, nz, K.c0, K.c1, s_zbit, red, zout + zoff, C.poff >= 0 ? psum + C.poff : nullptr);
+            else if (K.kind == BT_PREFIX)
+                chunk_prefix(psum + C.poff, nch, red);
+            else
+                sample_chunks(arena + C.off, nz, K.c0, K.c1, psum + C.poff, unif + C.uoff, C.shots, sout + C.soff,
+                              red, s_range);
         }
         __syncthreads();
         if (t == 0) {
@@ -298,15 +439,16 @@ int batch_grid(int device, int prec) {
 
 cudaError_t launch_batch(void* arena, int prec, const BatchTask* tasks, int ntasks, const BatchCirc* circs,
                          const BatchProg* progs, const void* blob, const DevOp* sops, const void* pool, int* head,
-                         int* done, double* zout, int* err, int grid, cudaStream_t s) {
+                         int* done, double* zout, int* err, int grid, cudaStream_t s, double* psum,
+                         const double* unif, uint64_t* sout) {
     const unsigned char* b = (const unsigned char*)blob;
     const double2* pl = (const double2*)pool;
     if (prec == 1)
         k_batch<float2><<<grid, NT, batch_smem<float2>(), s>>>((float2*)arena, tasks, ntasks, circs, progs, b, sops, pl,
-                                                               head, done, zout, err);
+                                                               head, done, zout, err, psum, unif, sout);
     else
         k_batch<double2><<<grid, NT, batch_smem<double2>(), s>>>((double2*)arena, tasks, ntasks, circs, progs, b, sops,
-                                                                 pl, head, done, zout, err);
+                                                                 pl, head, done, zout, err, psum, unif, sout);
     return cudaGetLastError();
 }
 
