@@ -352,7 +352,7 @@ __global__ void __launch_bounds__(NT, sizeof(C2) == 8 ? 2 : 1)
         const int nz = circs[K.circ].n;
         const int64_t zoff = circs[K.circ].zoff;
 
-        if (K.kind != BT_ZRED) {
+        if (K.kind == BT_SMALL || K.kind == BT_PASS) {
             // SMALL: step s runs program prog + s on the resident tile.
             // PASS: step s runs program prog on coset c0 + s.
             const bool small = K.kind == BT_SMALL;
@@ -397,7 +397,7 @@ __global__ void __launch_bounds__(NT, sizeof(C2) == 8 ? 2 : 1)
                 zred(arena + C.off, nz, K.c0, K.c1, s_zbit, red, zout + zoff, C.poff >= 0 ? psum + C.poff : nullptr);
             else if (K.kind == BT_PREFIX)
                 chunk_prefix(psum + C.poff, nch, red);
-            else
+            else if (K.kind == BT_SAMPLE)
                 sample_chunks(arena + C.off, nz, K.c0, K.c1, psum + C.poff, unif + C.uoff, C.shots, sout + C.soff,
                               red, s_range);
         }
