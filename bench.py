@@ -72,6 +72,8 @@ def parse():
     ap.add_argument("--rates", default="100,400,1600,6400", help="serve: arrival rates (requests/s)")
     ap.add_argument("--seed", type=int, default=1234)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="batch: default plan choices")
+    ap.add_argument("--no-baseline", action="store_true", help="batch/serve: skip the one-at-a-time baseline")
     a = ap.parse_args()
     if a.nqubits is None:
         a.nqubits = 32 if a.workload == "precision" else 30
@@ -528,7 +530,7 @@ def run_batch(args):
     torch.cuda.set_device(0)
     ns, circs = _hea_batch(K, C, N)
     t0 = time.perf_counter()
-    b = K.Batch(circs, precision=K.C64, autotune=True)
+    b = K.Batch(circs, precision=K.C64, autotune=not args.no_autotune)
     create_s = time.perf_counter() - t0
     tune = {n: [b.options.tune[n].fusion, b.options.tune[n].max_gates] for n in sorted(set(ns))}
     info = b.info()
@@ -553,7 +555,7 @@ def run_batch(args):
     b2.close()
     e2e_s = time.perf_counter() - t0
     # Baseline: one Simulator launch per circuit (plans and states prepared beforehand).
-    M = min(256, N)
+    M = 0 if args.no_baseline else min(256, N)
     sims = [K.Simulator(circs[i], 1, K.C64, 0) for i in range(M)]
     for s_ in sims[:4]:
         s_.run_async()
@@ -562,7 +564,7 @@ def run_batch(args):
     for s_ in sims:
         s_.run_async()
         s_.expect_z()
-    plain = M / (time.perf_counter() - t0)
+    plain = M / (time.perf_counter() - t0) if M else None
     for s_ in sims:
         s_.close()
     cpu = None
@@ -582,7 +584,8 @@ def run_batch(args):
     h2d = info["programs"] * 6000
     cfg.update({"autotuned": tune, "tasks": info["tasks"], "pass_programs": info["programs"],
                 "arena_bytes": info["arena_bytes"], "ctas": info["ctas"], "create_s": create_s,
-                "baseline_one_launch_per_circuit_cps": plain, "speedup_vs_one_launch_per_circuit": value / plain})
+                "baseline_one_launch_per_circuit_cps": plain,
+                "speedup_vs_one_launch_per_circuit": value / plain if plain else None})
     print(json.dumps(_common(
         "circuits/s", "circuits/s", value, args, ms, "c64 (f32)", cfg,
         e2e={"value": N / e2e_s, "unit": "circuits/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 8 * len(z),
