@@ -385,8 +385,10 @@ def run_precision(args):
 
     n, L = args.nqubits, args.layers
     gates = circuits.brickwork_su4(n, L, args.seed)
-    cfg = {"workload": f"brickwork of Haar SU(4) gates, n={n}, {L} layers, complex64, 5-qubit blocks on "
-                       f"tensor cores (3xTF32)", "nqubits": n, "layers": L, "gates": len(gates), "seed": args.seed,
+    cfg = {"workload": f"brickwork of Haar SU(4) gates, n={n}, {L} layers, complex64, gateScheduling + "
+                       f"gateFusion(5) into 5-qubit blocks on tensor cores (3xTF32); complex128 comparison on the "
+                       f"unfused circuit (its faster plan)", "nqubits": n, "layers": L, "gates": len(gates),
+           "seed": args.seed,
            "state_bytes": 8 << n, "l2": "state larger than L2; no flush needed", "parallelism": "replicas"}
     if args.impl == "reference":
         if _reference_unavailable():
@@ -403,8 +405,11 @@ def run_precision(args):
                                       "d2h_bytes_per_step": 0})))
         return
     torch.cuda.set_device(0)
-    circ = K.Circuit(n, gates)
-    sim = K.Simulator(circ, 1, K.C64, 0)
+    circ = K.Circuit(n, gates)  # complex128 plan: register stages, dense SU(4) as shared-memory ops
+    fused = K.Circuit(n, gates)  # complex64 plan: gateFusion(5) blocks on the tensor cores
+    fused.gateScheduling()
+    fused.gateFusion(5, 1e-6)
+    sim = K.Simulator(fused, 1, K.C64, 0)
     passes = sim.passes()
     stream = torch.cuda.Stream()
     for _ in range(args.warmup):
@@ -439,7 +444,10 @@ def run_precision(args):
     # Infidelity at n = 28 against complex128.
     nf = min(n, 28)
     cf = K.Circuit(nf, circuits.brickwork_su4(nf, L, args.seed))
-    a = K.Simulator(cf, 1, K.C64, 0)
+    cf64 = K.Circuit(nf, circuits.brickwork_su4(nf, L, args.seed))
+    cf64.gateScheduling()
+    cf64.gateFusion(5, 1e-6)
+    a = K.Simulator(cf64, 1, K.C64, 0)
     a.execute()
     psi64 = a.state()
     a.close()
@@ -452,7 +460,7 @@ def run_precision(args):
     del psi64, psi128
     # End to end: plan + upload + |0> init + passes + proba_state readback.
     t0 = time.perf_counter()
-    e = K.Simulator(circ, 1, K.C64, 0)
+    e = K.Simulator(fused, 1, K.C64, 0)
     e.execute()
     e.close()
     e2e_ms = (time.perf_counter() - t0) * 1000
@@ -463,7 +471,7 @@ def run_precision(args):
         cpu = {"value": 1.0 / (sec * 2 ** (n - nn)), "unit": "layers/s", "cores": cores, "kind": "reference",
                "sample": f"1 layer at n={nn} on the reference CPUSimulator (complex128), scaled by 2^{n - nn}"}
     cfg.update({"c128_ms_per_step": ms128, "speedup_vs_c128": ms128 / ms, "infidelity_vs_c128": infid,
-                "infidelity_nqubits": nf, "passes_per_step": len(passes)})
+                "infidelity_nqubits": nf, "passes_per_step": len(passes), "fused_gates": fused.num_gates()})
     print(json.dumps(_common(
         f"{n}q SU(4) brickwork layers/s (complex64)", "layers/s", L * 1000.0 / ms, args, ms, "c64 (tf32x3 / f32)",
         cfg,

@@ -6,8 +6,9 @@
 // grid-stride loop over cosets:
 //   1. the tile is copied global -> shared with 16-byte cp.async (each warp
 //      instruction reads runs of 2^c contiguous amplitudes, c >= 4); the
-//      copy of the next coset is issued before the current one is processed
-//      (two buffers, one CTA per SM), so HBM reads overlap compute;
+//      copies of the next cosets are issued before the current one is
+//      processed (a ring of up to three buffers, one CTA per SM), so HBM
+//      reads overlap compute;
 //   2. the pass program runs: a register stage loads 16 amplitudes per
 //      thread from shared memory, applies its ops in registers (2x2, H,
 //      controlled X, controlled phase, one-qubit diagonal), and stores them
@@ -34,11 +35,14 @@ constexpr size_t tile_smem_bytes() {
 }
 
 // SM: whether the program has shared-memory ops (the variant without them
-// has no call in its loop, so nothing is spilled around it). NBUF = 2: one
-// CTA per SM, the next coset prefetched while the current one is processed;
-// NBUF = 1: two CTAs per SM overlap each other's load and compute phases.
+// has no call in its loop, so nothing is spilled around it). NBUF tile
+// buffers: NBUF = 1, two CTAs per SM overlap each other's load and compute
+// phases; NBUF = 2 or 3, one CTA per SM keeps the next NBUF - 1 cosets'
+// copies in flight while it processes the current one (one cp.async group
+// per iteration, empty when there is nothing left to prefetch, so the group
+// count stays uniform).
 template <typename C2, bool SM, int NBUF>
-__global__ void __launch_bounds__(NT, 3 - NBUF)
+__global__ void __launch_bounds__(NT, NBUF == 1 ? 2 : 1)
     k_tile(C2* __restrict__ st, const __grid_constant__ PassProg P, const DevOp* __restrict__ sops,
            const double2* __restrict__ pool) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -54,19 +58,33 @@ __global__ void __launch_bounds__(NT, 3 - NBUF)
     __syncthreads();
     const uint32_t ncos = 1u << P.ncb;
     const int nops = P.nops, sop0 = P.sop0;
-    if (NBUF == 2 && blockIdx.x < ncos) load_async(T, st, blockIdx.x, sbase, t);
+    constexpr uint32_t BUF_BYTES = TS * sizeof(C2);
+    // NBUF = 1: grid-stride over cosets. NBUF > 1: each CTA takes a
+    // contiguous range of cosets, so the tiles it has in flight together are
+    // neighbours in memory (coset bit 0 is usually physical bit c), which
+    // lengthens the DRAM runs beyond 2^c amplitudes.
+    const uint32_t c_begin = NBUF == 1 ? blockIdx.x : (uint32_t)((uint64_t)blockIdx.x * ncos / gridDim.x);
+    const uint32_t c_end = NBUF == 1 ? ncos : (uint32_t)((uint64_t)(blockIdx.x + 1) * ncos / gridDim.x);
+    const uint32_t c_step = NBUF == 1 ? gridDim.x : 1u;
+    if (NBUF > 1) {
+        for (int k = 0; k < NBUF - 1; k++) {
+            const uint32_t c = c_begin + k;
+            if (c < c_end) load_async(T, st, c, sbase + k * BUF_BYTES, t);
+            else asm volatile("cp.async.commit_group;\n" ::: "memory");
+        }
+    }
     int it = 0;
-    for (uint32_t c = blockIdx.x; c < ncos; c += gridDim.x, it++) {
-        const uint32_t tb = sbase + (uint32_t)((NBUF == 2 ? (it & 1) : 0) * TS * sizeof(C2));
-        C2* tile = bufs + (NBUF == 2 ? (it & 1) : 0) * TS;
-        if (NBUF == 2) {
-            // Prefetch the next coset into the other buffer, then wait for this one.
-            if (c + gridDim.x < ncos) {
-                load_async(T, st, c + gridDim.x, sbase + (uint32_t)(((it + 1) & 1) * TS * sizeof(C2)), t);
-                asm volatile("cp.async.wait_group 1;\n" ::: "memory");
-            } else {
-                asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-            }
+    for (uint32_t c = c_begin; c < c_end; c += c_step, it++) {
+        const int slot = NBUF == 1 ? 0 : it % NBUF;
+        const uint32_t tb = sbase + (uint32_t)slot * BUF_BYTES;
+        C2* tile = bufs + slot * TS;
+        if (NBUF > 1) {
+            // Prefetch the coset NBUF - 1 iterations ahead into the buffer the
+            // previous iteration released, then wait for this one.
+            const uint32_t cn = c + (NBUF - 1);
+            if (cn < c_end) load_async(T, st, cn, sbase + (uint32_t)((it + NBUF - 1) % NBUF) * BUF_BYTES, t);
+            else asm volatile("cp.async.commit_group;\n" ::: "memory");
+            asm volatile("cp.async.wait_group %0;\n" ::"n"(NBUF - 1) : "memory");
         } else {
             load_async(T, st, c, sbase, t);
             asm volatile("cp.async.wait_group 0;\n" ::: "memory");
@@ -75,9 +93,10 @@ __global__ void __launch_bounds__(NT, 3 - NBUF)
         run_program<C2, SM>(T, nops, tb, tile, coset_base(T, c), sops, sop0, pool, t);
         __syncthreads();
         store_tile<C2, false>(T, st, c, tb, t);
-        // The buffer is refilled by the next load.
+        // The buffer is refilled by a later load.
         __syncthreads();
     }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
 }  // namespace
@@ -107,7 +126,11 @@ cudaError_t launch_tile_t(void* st, const PassProg& prog, const DevOp* sops, con
     for (int k = 0; k < prog.nops; k++) sm |= prog.ops[k].kind == SOP_SMEM;
     C2* x = (C2*)st;
     const double2* pl = (const double2*)pool;
-    if (nbuf == 2) {
+    if (nbuf == 3) {
+        const size_t smem = tile_smem_bytes<C2, 3>();
+        if (sm) k_tile<C2, true, 3><<<grid, NT, smem, s>>>(x, prog, sops, pl);
+        else k_tile<C2, false, 3><<<grid, NT, smem, s>>>(x, prog, sops, pl);
+    } else if (nbuf == 2) {
         const size_t smem = tile_smem_bytes<C2, 2>();
         if (sm) k_tile<C2, true, 2><<<grid, NT, smem, s>>>(x, prog, sops, pl);
         else k_tile<C2, false, 2><<<grid, NT, smem, s>>>(x, prog, sops, pl);
@@ -121,8 +144,12 @@ cudaError_t launch_tile_t(void* st, const PassProg& prog, const DevOp* sops, con
 
 int tile_pass_grid(int n, int device, int nbuf, int prec) {
     int g;
-    if (prec == 1) g = nbuf == 2 ? tile_grid_for<float2, 2>(device) : tile_grid_for<float2, 1>(device);
-    else g = nbuf == 2 ? tile_grid_for<double2, 2>(device) : tile_grid_for<double2, 1>(device);
+    if (prec == 1)
+        g = nbuf == 3 ? tile_grid_for<float2, 3>(device)
+                      : nbuf == 2 ? tile_grid_for<float2, 2>(device) : tile_grid_for<float2, 1>(device);
+    else
+        g = nbuf == 3 ? tile_grid_for<double2, 3>(device)
+                      : nbuf == 2 ? tile_grid_for<double2, 2>(device) : tile_grid_for<double2, 1>(device);
     const uint64_t ncos = 1ull << (n - TB);
     return (int)(ncos < (uint64_t)g ? ncos : (uint64_t)g);
 }

@@ -137,6 +137,11 @@ std::string Simulator::create(const Program& prog_in, int precision, int device,
         if (!e.empty()) return fail(e);
     }
     impl->opt.c64 = precision == 1;
+    // Contiguous low physical bits every tile holds (runs of 2^c amplitudes per access).
+    if (const char* e = std::getenv("KATE_COALESCE")) {
+        const int v = std::atoi(e);
+        if (v >= 1 && v <= 8) impl->opt.coalesce = v;
+    }
     std::string e = build_plan(impl->prog, impl->opt, &impl->plan);
     if (!e.empty()) return fail(e);
 
@@ -178,7 +183,10 @@ std::string Simulator::create(const Program& prog_in, int precision, int device,
     ce = cudaMalloc(&impl->d_state, impl->dim() * impl->amp_bytes());
     if (ce != cudaSuccess) return fail(cuda_err("cudaMalloc(state)", ce));
     impl->grid = generic_pass_grid(impl->n, std::min(impl->opt.max_tile, impl->n), device);
-    if (const char* e = std::getenv("KATE_TILE_NBUF")) impl->nbuf = std::atoi(e) == 2 ? 2 : 1;
+    if (const char* e = std::getenv("KATE_TILE_NBUF")) {
+        const int v = std::atoi(e);
+        impl->nbuf = v == 2 ? 2 : v == 3 ? 3 : 1;
+    }
     if (impl->n >= KATE_TILE_BITS) {
         impl->tile_grid = tile_pass_grid(impl->n, device, impl->nbuf, precision);
         if (precision == 1) impl->block_grid = block_c64_grid(impl->n, device);
