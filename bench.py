@@ -68,8 +68,9 @@ def parse():
     ap.add_argument("--nqubits", type=int, default=None)
     ap.add_argument("--layers", type=int, default=20)
     ap.add_argument("--circuits", type=int, default=4096, help="batch: circuits in the batch")
-    ap.add_argument("--requests", type=int, default=400, help="serve: requests per rate")
-    ap.add_argument("--rates", default="100,400,1600,6400", help="serve: arrival rates (requests/s)")
+    ap.add_argument("--requests", type=int, default=1000, help="serve: requests per rate")
+    ap.add_argument("--rates", default="1000,4000,16000", help="serve: arrival rates (requests/s)")
+    ap.add_argument("--step-us", type=int, default=0, help="serve: step latency target in us (0: default)")
     ap.add_argument("--seed", type=int, default=1234)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="batch: default plan choices")
@@ -653,7 +654,8 @@ def run_serve(args):
         return
     torch.cuda.set_device(0)
     circs = [K.Circuit(n, C.layered(n, n, seed=i)) for i, n in enumerate(ns)]
-    srv = K.Server(K.C64, 0, budget_bytes=150 * 10 ** 9)
+    kw = {"step_latency_us": args.step_us} if args.step_us else {}
+    srv = K.Server(K.C64, 0, budget_bytes=150 * 10 ** 9, **kw)
     # Warm-up: a few requests of every size class present.
     for n in sorted(set(ns))[:6]:
         srv.wait(srv.submit(K.Circuit(n, C.layered(n, n, seed=999)), 1024, 1), timeout=600)
@@ -720,7 +722,8 @@ def run_serve(args):
     plain_cps = R / sum(svc)
     cfg.update({"sweep": sweep, "baseline_one_at_a_time": base, "baseline_service_cps": plain_cps,
                 "speedup_vs_one_at_a_time": best["circuits_per_s"] / plain_cps, "engine_steps": st["steps"],
-                "peak_resident_bytes": st["peak_resident_bytes"]})
+                "peak_resident_bytes": st["peak_resident_bytes"],
+                "engine_thread_s": {k[3:]: st[k] / 1e6 for k in ("us_admit", "us_build", "us_kernel", "us_collect")}})
     cpu = None
     if not args.no_cpu_baseline and not _reference_unavailable():
         tot, cnt, cores = 0.0, 0, 1

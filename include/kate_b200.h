@@ -349,6 +349,7 @@ typedef struct {
     int planners;                    /* planning threads (0: hardware concurrency, at most 16) */
     int fusion;                      /* gateFusion width for unfused circuits (1: none) */
     int max_gates;                   /* gates per pass program */
+    int step_latency_us;             /* estimated critical path per step (default 1500; <0: no limit) */
 } kate_server_options;
 
 KATE_API kate_status kate_server_options_default(kate_server_options* opt);
@@ -364,7 +365,9 @@ KATE_API kate_status kate_server_submit(kate_server* s, const kate_circuit* c, i
  * started), each nullable, and forgets the request. */
 KATE_API kate_status kate_server_wait(kate_server* s, long long id, double timeout_s, int* nqbits, double* z,
                                       uint64_t* samples, double* times);
-/* out[8]: submitted, completed, live, queued, steps, resident bytes, peak resident bytes, failed. */
+/* out[12]: submitted, completed, live, queued, steps, resident bytes, peak resident bytes, failed, then the
+ * engine thread's microseconds in admission, step building, step kernels (launch to completion) and result
+ * collection. */
 KATE_API kate_status kate_server_stats(const kate_server* s, long long* out);
 /* Seconds since the server started (the clock of kate_server_wait's times). */
 KATE_API kate_status kate_server_now(const kate_server* s, double* t);

@@ -519,9 +519,10 @@ class Server:
         return z, s[:shots], tuple(t)
 
     def stats(self) -> dict:
-        v = (ctypes.c_longlong * 8)()
+        v = (ctypes.c_longlong * 12)()
         _check(self._lib.kate_server_stats(self._h, v))
-        keys = ("submitted", "completed", "live", "queued", "steps", "resident_bytes", "peak_resident_bytes", "failed")
+        keys = ("submitted", "completed", "live", "queued", "steps", "resident_bytes", "peak_resident_bytes", "failed",
+                "us_admit", "us_build", "us_kernel", "us_collect")
         return dict(zip(keys, list(v)))
 
     def now(self) -> float:

@@ -317,13 +317,15 @@ std::string Batch::create(const std::vector<const Program*>& circuits, int preci
                     const int before = need[k];
                     if (lev < np) {
                         const uint32_t ncos = 1u << (P.n_sim - KATE_TILE_BITS);
-                        for (uint32_t c0 = 0; c0 < ncos; c0 += chunk) {
+                        // Small states: fewer cosets per task, so a level spreads over several CTAs.
+                        const uint32_t cch = std::max<uint32_t>(1, std::min<uint32_t>(chunk, ncos / 16));
+                        for (uint32_t c0 = 0; c0 < ncos; c0 += cch) {
                             BatchTask t{};
                             t.kind = BT_PASS;
                             t.circ = ci;
                             t.prog = prog0[ci] + (int)lev;
                             t.c0 = c0;
-                            t.c1 = std::min<uint32_t>(ncos, c0 + chunk);
+                            t.c1 = std::min<uint32_t>(ncos, c0 + cch);
                             t.need = before;
                             t.first = lev == 0;
                             ltasks.push_back(t);

@@ -771,6 +771,7 @@ kate_status kate_server_options_default(kate_server_options* opt) {
     opt->planners = d.planners;
     opt->fusion = d.tune.fusion;
     opt->max_gates = d.tune.max_gates;
+    opt->step_latency_us = d.step_latency_us;
     return KATE_OK;
 }
 
@@ -789,6 +790,8 @@ kate_status kate_server_create(int precision, int device, const kate_server_opti
             o.planners = opt->planners;
             if (opt->fusion > 0) o.tune.fusion = opt->fusion;
             if (opt->max_gates > 0) o.tune.max_gates = opt->max_gates;
+            if (opt->step_latency_us > 0) o.step_latency_us = opt->step_latency_us;
+            if (opt->step_latency_us < 0) o.step_latency_us = 0;
         }
         kate::Server* s = nullptr;
         std::string e = kate::Server::create(precision, device, o, &s);
@@ -841,9 +844,9 @@ kate_status kate_server_wait(kate_server* s, long long id, double timeout_s, int
 
 kate_status kate_server_stats(const kate_server* s, long long* out) {
     REQUIRE(s && out, "null pointer");
-    int64_t v[8];
+    int64_t v[12];
     s->s->stats(v);
-    for (int i = 0; i < 8; i++) out[i] = (long long)v[i];
+    for (int i = 0; i < 12; i++) out[i] = (long long)v[i];
     return KATE_OK;
 }
 

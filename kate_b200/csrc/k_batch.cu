@@ -93,9 +93,9 @@ extern __shared__ __align__(16) unsigned char batch_smem_raw[];
 // from the shared-memory symbol (shared-window addressing).
 template <typename C2, bool SM>
 __device__ __noinline__ void run_staged(int nops, uint64_t cbase, const DevOp* __restrict__ sops, int sop0,
-                                        const double2* __restrict__ pool) {
-    C2* tile = reinterpret_cast<C2*>(batch_smem_raw);
-    const TileTables<C2>& T = *reinterpret_cast<const TileTables<C2>*>(batch_smem_raw + TS * sizeof(C2));
+                                        const double2* __restrict__ pool, uint32_t boff) {
+    C2* tile = reinterpret_cast<C2*>(batch_smem_raw + boff);
+    const TileTables<C2>& T = *reinterpret_cast<const TileTables<C2>*>(batch_smem_raw + 2 * TS * sizeof(C2));
     const uint32_t tb = (uint32_t)__cvta_generic_to_shared(tile);
     run_program<C2, SM>(T, nops, tb, tile, cbase, sops, sop0, pool, threadIdx.x);
 }
@@ -106,8 +106,9 @@ __device__ __forceinline__ void run_any(const TileTables<C2>& T, const BatchProg
                                         uint32_t tb, C2* tile, uint64_t cbase, const DevOp* __restrict__ sops,
                                         const double2* __restrict__ pool, uint32_t t) {
     if (P.nstages >= 0) {
-        if (P.flags & BPROG_SMEM) run_staged<C2, true>(P.nops, cbase, sops, P.sop0, pool);
-        else run_staged<C2, false>(P.nops, cbase, sops, P.sop0, pool);
+        const uint32_t boff = tb - (uint32_t)__cvta_generic_to_shared(batch_smem_raw);
+        if (P.flags & BPROG_SMEM) run_staged<C2, true>(P.nops, cbase, sops, P.sop0, pool, boff);
+        else run_staged<C2, false>(P.nops, cbase, sops, P.sop0, pool, boff);
     } else {
         const DevOp* gops = reinterpret_cast<const DevOp*>(blob + P.ops_off);
         for (int k = 0; k < P.nops; k++) {
@@ -315,8 +316,10 @@ __global__ void __launch_bounds__(NT, sizeof(C2) == 8 ? 2 : 1)
             const double2* __restrict__ pool, int* __restrict__ head, int* __restrict__ done,
             double* __restrict__ zout, int* __restrict__ err, double* __restrict__ psum,
             const double* __restrict__ unif, uint64_t* __restrict__ sout) {
+    // Two tile buffers (a pass task prefetches its next coset into the
+    // other one), then the program tables.
     C2* tile = reinterpret_cast<C2*>(batch_smem_raw);
-    TileTables<C2>& T = *reinterpret_cast<TileTables<C2>*>(batch_smem_raw + TS * sizeof(C2));
+    TileTables<C2>& T = *reinterpret_cast<TileTables<C2>*>(batch_smem_raw + 2 * TS * sizeof(C2));
     __shared__ int s_task;
     __shared__ int s_abort;
     __shared__ uint8_t s_zbit[40];
@@ -365,9 +368,17 @@ __global__ void __launch_bounds__(NT, sizeof(C2) == 8 ? 2 : 1)
                 setup_program(T, v, t);
                 setup_io(T, v, t);
             }
+            const bool pre = !small && !K.first;  // pass task that loads: double-buffered
+            if (pre) {
+                __syncthreads();
+                load_async(T, st, K.c0, tb, t);
+            }
             for (int s = 0; s < nsteps; s++) {
                 const BatchProg& P = progs[small ? K.prog + s : K.prog];
                 const uint32_t c = K.c0 + (uint32_t)s;
+                const uint32_t cur = pre ? (uint32_t)(s & 1) : 0u;
+                const uint32_t tbc = tb + cur * (uint32_t)(TS * sizeof(C2));
+                C2* tilec = tile + cur * TS;
                 uint64_t cbase = 0;
                 __syncthreads();
                 if (small) {
@@ -375,17 +386,19 @@ __global__ void __launch_bounds__(NT, sizeof(C2) == 8 ? 2 : 1)
                 } else {
                     cbase = coset_base(T, c);
                     if (K.first) {
-                        init_basis0(tile, cbase == 0, t);
+                        init_basis0(tilec, cbase == 0, t);
+                    } else if (s + 1 < nsteps) {
+                        load_async(T, st, c + 1, tb + (cur ^ 1u) * (uint32_t)(TS * sizeof(C2)), t);
+                        asm volatile("cp.async.wait_group 1;\n" ::: "memory");
                     } else {
-                        load_async(T, st, c, tb, t);
                         asm volatile("cp.async.wait_group 0;\n" ::: "memory");
                     }
                 }
                 __syncthreads();
-                run_any(T, P, blob, tb, tile, cbase, sops, pool, t);
+                run_any(T, P, blob, tbc, tilec, cbase, sops, pool, t);
                 if (!small) {
                     __syncthreads();
-                    store_tile<C2, true>(T, st, c, tb, t);
+                    store_tile<C2, true>(T, st, c, tbc, t);
                 }
             }
             __syncthreads();
@@ -411,7 +424,7 @@ __global__ void __launch_bounds__(NT, sizeof(C2) == 8 ? 2 : 1)
 
 template <typename C2>
 constexpr size_t batch_smem() {
-    return (size_t)TS * sizeof(C2) + sizeof(TileTables<C2>);
+    return (size_t)2 * TS * sizeof(C2) + sizeof(TileTables<C2>);
 }
 
 }  // namespace

@@ -158,16 +158,27 @@ struct ServerImpl {
     std::chrono::steady_clock::time_point t0;
     void* d_state = nullptr;
     unsigned char* d_aux = nullptr;
-    BatchTask* d_tasks = nullptr;
-    size_t tasks_cap = 0;
-    BatchCirc* d_circs = nullptr;
-    size_t circs_cap = 0;
-    int* d_head = nullptr;
-    int* d_done = nullptr;
-    int* d_err = nullptr;
-    BatchTask* h_tasks = nullptr;  // pinned
-    size_t h_tasks_cap = 0;
-    cudaStream_t stream = nullptr;
+    // Two step slots: while one step runs, the next one is already queued
+    // behind it on the stream; results of a finished step are copied on a
+    // second stream so they do not wait for the queued step.
+    struct Slot {
+        BatchTask* d_tasks = nullptr;
+        size_t tasks_cap = 0;
+        BatchCirc* d_circs = nullptr;
+        size_t circs_cap = 0;
+        int* d_ctr = nullptr;           // [0] queue head, [1] error flag, [2..] per-circuit done counters
+        BatchTask* h_tasks = nullptr;   // pinned
+        size_t h_tasks_cap = 0;
+        int* h_err = nullptr;           // pinned
+        cudaEvent_t ev = nullptr;
+        std::vector<Req*> finishing;    // requests whose last level runs in this step
+        double t_launch = 0;
+    } slots[2];
+    int slot_next = 0;
+    std::deque<int> inflight;  // launched steps, oldest first
+    static constexpr int kMaxStepCircuits = 65536;
+    cudaStream_t stream = nullptr;   // uploads and steps
+    cudaStream_t cstream = nullptr;  // result copies
     int grid = 0;
     Buddy states;
     FirstFit aux;
@@ -182,6 +193,9 @@ struct ServerImpl {
     std::unordered_map<int64_t, ServeResult> results;
     std::unordered_map<int64_t, std::string> failures;
     int64_t n_submitted = 0, n_completed = 0, n_failed = 0, n_steps = 0;
+    // Engine thread time, microseconds: admission (plan upload), step task
+    // building, step launch to completion, result collection.
+    std::atomic<int64_t> us_admit{0}, us_build{0}, us_kernel{0}, us_collect{0};
     std::atomic<uint64_t> resident{0}, peak_resident{0};
     std::vector<std::thread> planners;
     std::thread engine;
@@ -254,10 +268,11 @@ struct ServerImpl {
         const uint64_t o_blob = place(P.blob.size(), 16);
         const uint64_t o_sops = place(P.sops.size() * sizeof(DevOp), sizeof(DevOp));
         const uint64_t o_pool = place(P.pool.size() * 16, 16);
-        const uint64_t o_z = place(8 * P.n_out, 8);
+        // <Z> and the samples back to back: one copy returns both.
+        const uint64_t o_z = place(8 * P.n_out + 8 * (uint64_t)r->shots, 8);
+        const uint64_t o_s = o_z + 8 * P.n_out;
         const uint64_t o_ps = place(8 * (2ull * r->nch + 1), 8);
         const uint64_t o_u = place(8 * (uint64_t)r->shots, 8);
-        const uint64_t o_s = place(8 * (uint64_t)r->shots, 8);
         r->prog0 = (int64_t)(o_progs / sizeof(BatchProg));
         r->zoff = (int64_t)(o_z / 8);
         r->poff = (int64_t)(o_ps / 8);
@@ -316,6 +331,21 @@ struct ServerImpl {
         resident -= (1ull << r->pack.n_sim) * amp_bytes();
     }
 
+    // Estimated latency of level a of r in microseconds (the levels of a
+    // request run one after another inside a step): waves of tasks over the
+    // CTAs, about 20 us per 4096-amplitude tile pass plus 5 us per task.
+    double level_latency_us(const Req* r, int a) const {
+        if (a < r->npass) {
+            const uint32_t ch = std::max<uint32_t>(1, std::min<uint32_t>((uint32_t)std::max(1, opt.chunk), r->ncos / 64));
+            const uint64_t tasks = (r->ncos + ch - 1) / ch;
+            const uint64_t waves = (tasks + grid - 1) / std::max(1, grid);
+            return (double)waves * (20.0 * ch + 5.0);
+        }
+        if (a == r->npass) return 5.0 + 2.0 * std::min<uint32_t>(r->nch, (uint32_t)std::max(1, opt.zchunks)) * 8.0;
+        if (a == r->npass + 1) return 5.0;
+        return 20.0;
+    }
+
     // Cost of level a of r in tile passes (for the step budget).
     int64_t level_cost(const Req* r, int a) const {
         if (a < r->npass) return r->ncos;
@@ -338,13 +368,38 @@ struct ServerImpl {
         return "";
     }
 
-    // One engine step over the live requests. Returns requests finished.
-    std::string step(std::vector<Req*>& finished) {
+    void free_slots() {
+        for (auto& sl : slots) {
+            cudaFree(sl.d_tasks);
+            cudaFree(sl.d_circs);
+            cudaFree(sl.d_ctr);
+            if (sl.h_tasks) cudaFreeHost(sl.h_tasks);
+            if (sl.h_err) cudaFreeHost(sl.h_err);
+            if (sl.ev) cudaEventDestroy(sl.ev);
+            sl = Slot();
+        }
+        if (cstream) cudaStreamDestroy(cstream);
+        cstream = nullptr;
+    }
+
+    bool has_work() const {
+        for (const Req* r : live)
+            if (r->next_level < r->levels) return true;
+        return false;
+    }
+
+    // Builds the next step from the live requests' unscheduled levels and
+    // queues it on the stream in slot `si`. Sets *launched when a step was
+    // queued.
+    std::string launch_step(int si, bool* launched) {
+        *launched = false;
+        Slot& S = slots[si];
         // Order: requests admitted more than a second ago first (no
         // starvation), then by remaining work (short jobs first).
         const double tnow = now();
         std::vector<std::pair<std::pair<int, int64_t>, Req*>> order;
         for (Req* r : live) {
+            if (r->next_level >= r->levels) continue;
             int64_t rem = 0;
             for (int a = r->next_level; a < r->levels; a++) rem += level_cost(r, a);
             order.push_back({{tnow - r->t_admit > 1.0 ? 0 : 1, rem}, r});
@@ -354,12 +409,17 @@ struct ServerImpl {
         std::vector<std::pair<Req*, int>> sched;  // request, levels this step
         int64_t used = 0;
         for (auto& it : order) {
+            if ((int)sched.size() >= kMaxStepCircuits) break;
             Req* r = it.second;
             int L = 0;
+            double chain = 0.0;
             while (r->next_level + L < r->levels) {
                 const int64_t c = level_cost(r, r->next_level + L);
+                const double lat = level_latency_us(r, r->next_level + L);
+                if (L > 0 && opt.step_latency_us > 0 && chain + lat > opt.step_latency_us) break;
                 if (used + c > opt.step_tiles && (L > 0 || used > 0)) break;
                 used += c;
+                chain += lat;
                 L++;
             }
             if (L > 0) sched.push_back({r, L});
@@ -403,7 +463,9 @@ struct ServerImpl {
                         cnt[i]++;
                     };
                     if (a < r->npass) {
-                        for (uint32_t c0 = 0; c0 < r->ncos; c0 += chunk) add(BT_PASS, c0, std::min(r->ncos, c0 + chunk));
+                        // Small states: one coset per task, so a level spreads over several CTAs.
+                        const uint32_t ch = std::max<uint32_t>(1, std::min<uint32_t>(chunk, r->ncos / 64));
+                        for (uint32_t c0 = 0; c0 < r->ncos; c0 += ch) add(BT_PASS, c0, std::min(r->ncos, c0 + ch));
                     } else if (a == r->npass) {
                         for (uint32_t c0 = 0; c0 < r->nch; c0 += zch) add(BT_ZRED, c0, std::min(r->nch, c0 + zch));
                     } else if (a == r->npass + 1) {
@@ -415,65 +477,114 @@ struct ServerImpl {
             g0 = g1;
         }
         if (tasks.size() > (size_t)INT32_MAX) return "step has too many tasks";
-        std::string e = ensure((void**)&d_tasks, &tasks_cap, tasks.size() * sizeof(BatchTask));
-        if (e.empty()) e = ensure((void**)&d_circs, &circs_cap, circs.size() * sizeof(BatchCirc));
+        std::string e = ensure((void**)&S.d_tasks, &S.tasks_cap, tasks.size() * sizeof(BatchTask));
+        if (e.empty()) e = ensure((void**)&S.d_circs, &S.circs_cap, circs.size() * sizeof(BatchCirc));
         if (!e.empty()) return e;
-        if (tasks.size() > h_tasks_cap) {
-            if (h_tasks) cudaFreeHost(h_tasks);
-            h_tasks_cap = std::max(tasks.size(), 2 * h_tasks_cap);
-            cudaError_t ce = cudaHostAlloc((void**)&h_tasks, h_tasks_cap * sizeof(BatchTask), cudaHostAllocDefault);
+        if (tasks.size() > S.h_tasks_cap) {
+            // The slot's previous copy finished with its step.
+            if (S.h_tasks) cudaFreeHost(S.h_tasks);
+            S.h_tasks_cap = std::max(tasks.size(), 2 * S.h_tasks_cap);
+            cudaError_t ce = cudaHostAlloc((void**)&S.h_tasks, S.h_tasks_cap * sizeof(BatchTask), cudaHostAllocDefault);
             if (ce != cudaSuccess) {
-                h_tasks = nullptr;
-                h_tasks_cap = 0;
+                S.h_tasks = nullptr;
+                S.h_tasks_cap = 0;
                 return cuda_err("cudaHostAlloc(tasks)", ce);
             }
         }
-        std::memcpy(h_tasks, tasks.data(), tasks.size() * sizeof(BatchTask));
-        cudaMemcpyAsync(d_tasks, h_tasks, tasks.size() * sizeof(BatchTask), cudaMemcpyHostToDevice, stream);
-        cudaMemcpyAsync(d_circs, circs.data(), circs.size() * sizeof(BatchCirc), cudaMemcpyHostToDevice, stream);
-        cudaMemsetAsync(d_head, 0, sizeof(int), stream);
-        cudaMemsetAsync(d_done, 0, sizeof(int) * circs.size(), stream);
+        std::memcpy(S.h_tasks, tasks.data(), tasks.size() * sizeof(BatchTask));
+        cudaMemcpyAsync(S.d_tasks, S.h_tasks, tasks.size() * sizeof(BatchTask), cudaMemcpyHostToDevice, stream);
+        cudaMemcpyAsync(S.d_circs, circs.data(), circs.size() * sizeof(BatchCirc), cudaMemcpyHostToDevice, stream);
+        cudaMemsetAsync(S.d_ctr, 0, sizeof(int) * (2 + circs.size()), stream);
         const int g = (int)std::min<size_t>((size_t)grid, tasks.size());
-        cudaError_t le = launch_batch(d_state, precision, d_tasks, (int)tasks.size(), d_circs,
+        const double tb = now();
+        us_build += (int64_t)((tb - tnow) * 1e6);
+        cudaError_t le = launch_batch(d_state, precision, S.d_tasks, (int)tasks.size(), S.d_circs,
                                       reinterpret_cast<const BatchProg*>(d_aux), d_aux,
-                                      reinterpret_cast<const DevOp*>(d_aux), d_aux, d_head, d_done,
-                                      reinterpret_cast<double*>(d_aux), d_err, g, stream,
+                                      reinterpret_cast<const DevOp*>(d_aux), d_aux, S.d_ctr, S.d_ctr + 2,
+                                      reinterpret_cast<double*>(d_aux), S.d_ctr + 1, g, stream,
                                       reinterpret_cast<double*>(d_aux), reinterpret_cast<const double*>(d_aux),
                                       reinterpret_cast<uint64_t*>(d_aux));
         if (le != cudaSuccess) return cuda_err("launch_batch", le);
-        cudaError_t se = cudaStreamSynchronize(stream);
-        if (se != cudaSuccess) return cuda_err("cudaStreamSynchronize(step)", se);
-        int err = 0;
-        cudaMemcpy(&err, d_err, sizeof(int), cudaMemcpyDeviceToHost);
-        if (err) return "serving step: a dependency wait timed out";
-        n_steps++;
-        for (auto& s : sched) {
-            s.first->next_level += s.second;
-            if (s.first->next_level >= s.first->levels) finished.push_back(s.first);
+        cudaEventRecord(S.ev, stream);
+        S.t_launch = tb;
+        S.finishing.clear();
+        for (auto& x : sched) {
+            x.first->next_level += x.second;
+            if (x.first->next_level >= x.first->levels) S.finishing.push_back(x.first);
         }
+        inflight.push_back(si);
+        *launched = true;
         return "";
     }
 
-    void collect(Req* r) {
-        ServeResult res;
-        res.n = r->pack.n_out;
-        res.z.resize(res.n);
-        std::vector<uint64_t> phys(r->shots);
-        cudaMemcpy(res.z.data(), d_aux + 8 * r->zoff, 8 * res.n, cudaMemcpyDeviceToHost);
-        if (r->shots) cudaMemcpy(phys.data(), d_aux + 8 * r->soff, 8 * (size_t)r->shots, cudaMemcpyDeviceToHost);
-        res.samples.resize(r->shots);
-        for (int s = 0; s < r->shots; s++) {
-            uint64_t v = 0;
-            for (int x = 0; x < res.n; x++) v |= ((phys[s] >> r->pack.zbit[x]) & 1ull) << x;
-            res.samples[s] = v;
+    // Waits for the oldest queued step; returns the requests it finished.
+    std::string complete_oldest(std::vector<Req*>& finished) {
+        const int si = inflight.front();
+        inflight.pop_front();
+        Slot& S = slots[si];
+        cudaError_t ce = cudaEventSynchronize(S.ev);
+        us_kernel += (int64_t)((now() - std::max(S.t_launch, last_done)) * 1e6);
+        last_done = now();
+        if (ce != cudaSuccess) return cuda_err("cudaEventSynchronize(step)", ce);
+        cudaStreamWaitEvent(cstream, S.ev, 0);
+        cudaMemcpyAsync(S.h_err, S.d_ctr + 1, sizeof(int), cudaMemcpyDeviceToHost, cstream);
+        ce = cudaStreamSynchronize(cstream);
+        if (ce != cudaSuccess) return cuda_err("cudaStreamSynchronize(results)", ce);
+        if (*S.h_err) return "serving step: a dependency wait timed out";
+        n_steps++;
+        finished = S.finishing;
+        S.finishing.clear();
+        return "";
+    }
+    double last_done = 0;
+
+    std::vector<uint64_t> h_out;  // staging for results (pinned)
+    uint64_t* h_pinned = nullptr;
+    size_t h_pinned_cap = 0;
+
+    // Copies the finished requests' <Z> and samples with one asynchronous
+    // copy each and one synchronisation, then publishes the results.
+    void collect(const std::vector<Req*>& fin) {
+        size_t words = 0;
+        for (Req* r : fin) words += (size_t)r->pack.n_out + r->shots;
+        if (words > h_pinned_cap) {
+            if (h_pinned) cudaFreeHost(h_pinned);
+            h_pinned_cap = std::max(words, 2 * h_pinned_cap);
+            if (cudaHostAlloc((void**)&h_pinned, h_pinned_cap * 8, cudaHostAllocDefault) != cudaSuccess) {
+                h_pinned = nullptr;
+                h_pinned_cap = 0;
+            }
         }
-        res.t_submit = r->t_submit;
-        res.t_admit = r->t_admit;
-        res.t_done = now();
-        release(r);
-        std::lock_guard<std::mutex> lk(m);
-        results[r->id] = std::move(res);
-        n_completed++;
+        uint64_t* host = h_pinned;
+        if (!host) {
+            h_out.resize(words);
+            host = h_out.data();
+        }
+        size_t o = 0;
+        for (Req* r : fin) {
+            const size_t w = (size_t)r->pack.n_out + r->shots;
+            cudaMemcpyAsync(host + o, d_aux + 8 * r->zoff, 8 * w, cudaMemcpyDeviceToHost, cstream);
+            o += w;
+        }
+        cudaStreamSynchronize(cstream);
+        o = 0;
+        for (Req* r : fin) {
+            ServeResult res;
+            res.n = r->pack.n_out;
+            res.z.resize(res.n);
+            std::memcpy(res.z.data(), host + o, 8 * res.n);
+            const uint64_t* phys = host + o + res.n;
+            o += (size_t)res.n + r->shots;
+            res.samples.assign(phys, phys + r->shots);  // physical indices; wait() converts them
+            res.zbit = r->pack.zbit;
+            res.t_submit = r->t_submit;
+            res.t_admit = r->t_admit;
+            res.t_done = now();
+            release(r);
+            std::lock_guard<std::mutex> lk(m);
+            results[r->id] = std::move(res);
+            n_completed++;
+        }
     }
 
     void engine_loop() {
@@ -483,7 +594,7 @@ struct ServerImpl {
             std::vector<Req*> to_admit, failed;
             {
                 std::unique_lock<std::mutex> lk(m);
-                if (live.empty())
+                if (live.empty() && inflight.empty())
                     cv_engine.wait_for(lk, std::chrono::milliseconds(2), [&] {
                         if (stop) return true;
                         auto it = waiting.find(next_admit);
@@ -520,7 +631,10 @@ struct ServerImpl {
                     cv_done.notify_all();
                     continue;
                 }
-                if (resident + sbytes > opt.budget_bytes || !admit(r)) {
+                const double ta = now();
+                const bool admitted = resident + sbytes <= opt.budget_bytes && admit(r);
+                us_admit += (int64_t)((now() - ta) * 1e6);
+                if (!admitted) {
                     if (!live.empty()) break;  // wait for memory to free up
                     std::lock_guard<std::mutex> lk(m);
                     failures[r->id] = "request does not fit the device arenas";
@@ -537,11 +651,25 @@ struct ServerImpl {
                 next_admit++;
                 live.push_back(r);
             }
-            if (live.empty()) continue;
+            // Keep up to two steps queued: the next one is built while the
+            // current one runs.
+            std::string e;
+            while (e.empty() && inflight.size() < 2 && has_work()) {
+                bool launched = false;
+                e = launch_step(slot_next, &launched);
+                if (!launched) break;
+                slot_next ^= 1;
+            }
             std::vector<Req*> finished;
-            std::string e = step(finished);
+            if (e.empty()) {
+                if (inflight.empty()) continue;  // nothing to run: back to waiting for arrivals
+                e = complete_oldest(finished);
+            }
             if (!e.empty()) {
                 // Fail every live request; the engine keeps serving new ones.
+                cudaStreamSynchronize(stream);
+                inflight.clear();
+                for (Slot& S : slots) S.finishing.clear();
                 std::lock_guard<std::mutex> lk(m);
                 for (Req* r : live) {
                     failures[r->id] = e;
@@ -552,18 +680,19 @@ struct ServerImpl {
                     delete r;
                 }
                 live.clear();
-                cudaMemset(d_err, 0, sizeof(int));
                 cv_done.notify_all();
                 continue;
             }
+            const double tc = now();
+            if (!finished.empty()) collect(finished);
             for (Req* r : finished) {
-                collect(r);
                 {
                     std::lock_guard<std::mutex> lk(m);
                     live.erase(std::find(live.begin(), live.end(), r));
                 }
                 delete r;
             }
+            us_collect += (int64_t)((now() - tc) * 1e6);
             if (!finished.empty()) cv_done.notify_all();
         }
     }
@@ -579,9 +708,7 @@ std::string Server::create(int precision, int device, const ServeOptions& opt, S
     auto fail = [&](const std::string& e) {
         cudaFree(S->d_state);
         cudaFree(S->d_aux);
-        cudaFree(S->d_head);
-        cudaFree(S->d_done);
-        cudaFree(S->d_err);
+        S->free_slots();
         if (S->stream) cudaStreamDestroy(S->stream);
         delete S;
         return e;
@@ -597,11 +724,15 @@ std::string Server::create(int precision, int device, const ServeOptions& opt, S
     if (ce != cudaSuccess) return fail(cuda_err("cudaMalloc(state arena)", ce));
     ce = cudaMalloc((void**)&S->d_aux, opt.aux_bytes);
     if (ce != cudaSuccess) return fail(cuda_err("cudaMalloc(aux arena)", ce));
-    ce = cudaMalloc((void**)&S->d_head, sizeof(int));
-    if (ce == cudaSuccess) ce = cudaMalloc((void**)&S->d_done, sizeof(int) * 65536);
-    if (ce == cudaSuccess) ce = cudaMalloc((void**)&S->d_err, sizeof(int));
-    if (ce != cudaSuccess) return fail(cuda_err("cudaMalloc(counters)", ce));
-    cudaMemset(S->d_err, 0, sizeof(int));
+    ce = cudaStreamCreateWithFlags(&S->cstream, cudaStreamNonBlocking);
+    if (ce != cudaSuccess) return fail(cuda_err("cudaStreamCreate", ce));
+    for (auto& sl : S->slots) {
+        ce = cudaMalloc((void**)&sl.d_ctr, sizeof(int) * (2 + ServerImpl::kMaxStepCircuits));
+        if (ce == cudaSuccess) ce = cudaHostAlloc((void**)&sl.h_err, sizeof(int), cudaHostAllocDefault);
+        if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming);
+        if (ce != cudaSuccess) return fail(cuda_err("step slot allocation", ce));
+        cudaMemset(sl.d_ctr, 0, sizeof(int) * 2);
+    }
     S->states.init(budget, minb, 22);
     S->aux.init(opt.aux_bytes);
     S->grid = batch_grid(device, precision);
@@ -632,12 +763,8 @@ Server::~Server() {
     for (auto& kv : d_->waiting) delete kv.second;
     cudaFree(d_->d_state);
     cudaFree(d_->d_aux);
-    cudaFree(d_->d_tasks);
-    cudaFree(d_->d_circs);
-    cudaFree(d_->d_head);
-    cudaFree(d_->d_done);
-    cudaFree(d_->d_err);
-    if (d_->h_tasks) cudaFreeHost(d_->h_tasks);
+    d_->free_slots();
+    if (d_->h_pinned) cudaFreeHost(d_->h_pinned);
     cudaStreamDestroy(d_->stream);
     delete d_;
 }
@@ -674,6 +801,13 @@ std::string Server::wait(int64_t id, double timeout_s, ServeResult* out) {
         if (it != d_->results.end()) {
             *out = std::move(it->second);
             d_->results.erase(it);
+            lk.unlock();
+            // Physical amplitude index -> program-label order.
+            for (auto& v : out->samples) {
+                uint64_t w = 0;
+                for (int x = 0; x < out->n; x++) w |= ((v >> out->zbit[x]) & 1ull) << x;
+                v = w;
+            }
             return "";
         }
         auto f = d_->failures.find(id);
@@ -700,6 +834,10 @@ void Server::stats(int64_t* out) const {
     out[5] = (int64_t)d_->resident.load();
     out[6] = (int64_t)d_->peak_resident.load();
     out[7] = d_->n_failed;
+    out[8] = d_->us_admit.load();
+    out[9] = d_->us_build.load();
+    out[10] = d_->us_kernel.load();
+    out[11] = d_->us_collect.load();
 }
 
 double Server::now() const { return d_->now(); }

@@ -28,6 +28,7 @@ struct ServeOptions {
     uint64_t budget_bytes = 150ull << 30;  // resident states (the admission budget)
     uint64_t aux_bytes = 2ull << 30;       // programs, outputs, sums, uniforms
     int64_t step_tiles = 1 << 16;          // tile passes per step before requests wait for the next one
+    int step_latency_us = 1500;            // estimated critical path of one step (0: no limit)
     int chunk = 4;                         // cosets per pass task
     int zchunks = 4;                       // 2^16-amplitude chunks per <Z> task
     int schunks = 16;                      // chunks per sampling task
@@ -39,6 +40,7 @@ struct ServeResult {
     int n = 0;
     std::vector<double> z;          // <Z> per program label
     std::vector<uint64_t> samples;  // basis-state indices in label order, ascending CDF order
+    std::vector<uint8_t> zbit;      // internal: physical bit of each label (samples are converted on collection)
     double t_submit = 0, t_admit = 0, t_done = 0;  // seconds since the server started
 };
 
@@ -55,7 +57,9 @@ public:
     // Returns "timeout" when it is not done yet.
     std::string wait(int64_t id, double timeout_s, ServeResult* out);
     // Counters: [0] submitted [1] completed [2] live [3] queued [4] steps
-    // [5] resident bytes [6] peak resident bytes [7] failed.
+    // [5] resident bytes [6] peak resident bytes [7] failed; engine thread
+    // time in microseconds: [8] admission [9] step building [10] step
+    // launch to completion [11] result collection.
     void stats(int64_t* out) const;
     double now() const;  // seconds since the server started
 
