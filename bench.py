@@ -28,7 +28,8 @@ independent replicas, one per GPU (the path does not shard on one GPU).
 
 Other workloads (``--workload``), one JSON line each:
   precision  32-qubit complex64 brickwork of Haar SU(4) gates, 20 layers,
-             fused 5-qubit blocks on the tensor cores (3xTF32): layers/s,
+             fused 5-qubit blocks on the tensor cores (split-BF16 products,
+             FP32 accumulation): layers/s,
              speed-up over the complex128 path on the same circuit, and the
              infidelity against complex128 at n=28.
   batch      4096 hardware-efficient-ansatz circuits (n uniform in 10..22,
@@ -387,7 +388,7 @@ def run_precision(args):
     n, L = args.nqubits, args.layers
     gates = circuits.brickwork_su4(n, L, args.seed)
     cfg = {"workload": f"brickwork of Haar SU(4) gates, n={n}, {L} layers, complex64, gateScheduling + "
-                       f"gateFusion(5) into 5-qubit blocks on tensor cores (3xTF32); complex128 comparison on the "
+                       f"gateFusion(5) into 5-qubit blocks on tensor cores (split-BF16 x3); complex128 comparison on the "
                        f"unfused circuit (its faster plan)", "nqubits": n, "layers": L, "gates": len(gates),
            "seed": args.seed,
            "state_bytes": 8 << n, "l2": "state larger than L2; no flush needed", "parallelism": "replicas"}
@@ -474,13 +475,13 @@ def run_precision(args):
     cfg.update({"c128_ms_per_step": ms128, "speedup_vs_c128": ms128 / ms, "infidelity_vs_c128": infid,
                 "infidelity_nqubits": nf, "passes_per_step": len(passes), "fused_gates": fused.num_gates()})
     print(json.dumps(_common(
-        f"{n}q SU(4) brickwork layers/s (complex64)", "layers/s", L * 1000.0 / ms, args, ms, "c64 (tf32x3 / f32)",
+        f"{n}q SU(4) brickwork layers/s (complex64)", "layers/s", L * 1000.0 / ms, args, ms, "c64 (split-bf16 x3 products / f32 accumulation)",
         cfg,
         e2e={"value": L * 1000.0 / e2e_ms, "unit": "layers/s", "h2d_bytes_per_step": len(gates) * 16 * 16,
              "d2h_bytes_per_step": 2 * n * 8, "ms_per_step": e2e_ms},
         roofline={"bound": "hbm", "achieved": alg / (avg_pass / 1000) / 1e9, "peak": peak, "unit": "GB/s",
                   "frac": alg / (avg_pass / 1000) / 1e9 / peak, "traffic": None, "peak_source": peak_kind,
-                  "kernel": "k_block_c64 (tcgen05 kind::tf32, 3xTF32)", "alg_bytes_per_launch": alg,
+                  "kernel": "k_block_c64 (tcgen05 kind::f16, split-BF16 x3)", "alg_bytes_per_launch": alg,
                   "avg_launch_ms": avg_pass},
         gpu_launches=launches * args.steps, clocks=clk.summary(), cpu_baseline=cpu)))
 

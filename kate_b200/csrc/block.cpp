@@ -6,7 +6,8 @@
 // gate list, so no reordering is involved); each block's matrix is the FP64
 // product from the gate merger (the reference's CPUmergeGate arithmetic),
 // padded with identities to exactly five tile bits, then written as the
-// real 64x64 operand in TF32 hi + lo parts.
+// real 64x64 operand in BF16 hi + lo parts (split-BF16 products: the kernel
+// sums A_hi B_hi + A_hi B_lo + A_lo B_hi in FP32).
 #include <cmath>
 #include <cstring>
 
@@ -16,21 +17,25 @@ namespace kate {
 
 namespace {
 
-float tf32_rna(float x) {
+// BF16 bits of a float, rounded to nearest even (finite inputs).
+uint16_t bf16_bits(float x) {
     uint32_t u;
     std::memcpy(&u, &x, 4);
-    if ((u & 0x7f800000u) != 0x7f800000u) u = (u + 0x1000u) & 0xffffe000u;  // round half away from zero
+    u += 0x7fffu + ((u >> 16) & 1u);
+    return (uint16_t)(u >> 16);
+}
+float bf16_value(uint16_t h) {
+    const uint32_t u = (uint32_t)h << 16;
     float r;
     std::memcpy(&r, &u, 4);
     return r;
 }
 
-// Byte offset of element (row, k) in a K-major SWIZZLE_128B operand image
-// of `rows` rows and 64 fp32 columns (two K halves of rows x 128 bytes).
-size_t sw128_offset(int rows, int row, int k) {
-    const int khalf = k >> 5, kk = k & 31, chunk = kk >> 2, w = kk & 3;
-    return (size_t)khalf * rows * 128 + (size_t)(row >> 3) * 1024 + (size_t)(row & 7) * 128 +
-           (size_t)((chunk ^ (row & 7)) << 4) + (size_t)w * 4;
+// Byte offset of element (row, k) in a K-major SWIZZLE_128B operand image of
+// 64 BF16 columns: 128-byte rows, 16-byte chunks XORed with row & 7.
+size_t sw128_offset_bf16(int row, int k) {
+    const int chunk = k >> 3, w = k & 7;
+    return (size_t)(row >> 3) * 1024 + (size_t)(row & 7) * 128 + (size_t)((chunk ^ (row & 7)) << 4) + (size_t)w * 2;
 }
 
 // The pass's gates as kate::Gate on tile-bit qubits.
@@ -149,10 +154,10 @@ std::string build_block_program(const Plan& plan, const PlannedPass& pass, int n
         if (!e.empty()) return e;
         if (U.qbits.size() != 5) return "internal: block is not five qubits";
         for (int i = 0; i < 5; i++) out->btb[b][i] = (uint8_t)U.qbits[i];
-        // Real form and its TF32 split, as K-major SWIZZLE_128B images.
+        // Real form and its BF16 split, as K-major SWIZZLE_128B images.
         const size_t off = pool.size();
         pool.resize(off + KATE_BLOCK_IMG_BYTES, 0);
-        float* hi = reinterpret_cast<float*>(pool.data() + off);
+        uint8_t* hi_base = pool.data() + off;
         uint8_t* lo_base = pool.data() + off + KATE_BLOCK_IMG_BYTES / 2;
         for (int r = 0; r < 32; r++)
             for (int c = 0; c < 32; c++) {
@@ -162,11 +167,11 @@ std::string build_block_program(const Plan& plan, const PlannedPass& pass, int n
                     for (int bcol = 0; bcol < 2; bcol++) {
                         const int nrow = 2 * r + a, k = 2 * c + bcol;
                         const float f = (float)w[a][bcol];
-                        const float h = tf32_rna(f);
-                        const float l = tf32_rna(f - h);
-                        const size_t o = sw128_offset(64, nrow, k);
-                        std::memcpy(reinterpret_cast<uint8_t*>(hi) + o, &h, 4);
-                        std::memcpy(lo_base + o, &l, 4);
+                        const uint16_t h = bf16_bits(f);
+                        const uint16_t l = bf16_bits(f - bf16_value(h));
+                        const size_t o = sw128_offset_bf16(nrow, k);
+                        std::memcpy(hi_base + o, &h, 2);
+                        std::memcpy(lo_base + o, &l, 2);
                     }
             }
         out->bimg[b] = off;

@@ -107,11 +107,12 @@ typedef struct {
 // bit i of the block's local index is btb[b][i]); its 32x32 complex matrix
 // is stored as the real 64x64 matrix W (W[2r][2c] = Re U[r][c],
 // W[2r][2c+1] = -Im U[r][c], W[2r+1][2c] = Im U[r][c], W[2r+1][2c+1] =
-// Re U[r][c]) split into TF32 hi and lo parts, each laid out as the
-// K-major SWIZZLE_128B UMMA operand image (two K halves of 64 rows x 128 B):
-// KATE_BLOCK_IMG_BYTES per block at byte offset bimg[b] of the image pool.
+// Re U[r][c]) split into BF16 hi and lo parts (hi = bf16(w), lo =
+// bf16(w - hi)), each laid out as the K-major SWIZZLE_128B UMMA operand
+// image (64 rows x 128 B: 8 KiB), hi then lo: KATE_BLOCK_IMG_BYTES per block
+// at byte offset bimg[b] of the image pool.
 #define KATE_C64_MAX_BLOCKS 2
-#define KATE_BLOCK_IMG_BYTES 32768
+#define KATE_BLOCK_IMG_BYTES 16384
 
 typedef struct {
     int32_t m, ncb, nblocks, pad;

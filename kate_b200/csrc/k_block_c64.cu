@@ -1,25 +1,32 @@
 // Complex64 group pass with 5-qubit dense blocks on the tensor cores
-// (tcgen05, kind::tf32, 3xTF32 compensated products, FP32 accumulation in
-// TMEM).
+// (tcgen05, kind::f16 with BF16 operands, split-BF16 products, FP32
+// accumulation in TMEM).
 //
-// Each CTA (256 threads, one per SM) processes 4096-amplitude coset tiles
-// in a grid-stride loop; the next tile is prefetched with cp.async into a
-// second staging buffer while the current one is processed. For each block
-// of the pass:
-//   1. the tile (staging buffer S, natural tile order) is rearranged into
-//      the MMA A operand: 128 rows (the values of the 7 non-block tile
-//      bits) x 64 reals (the 32 complex amplitudes of the block's index,
-//      re/im interleaved), K-major with the 128-byte swizzle, as a TF32 hi
-//      part and the FP32 remainder (lo);
-//   2. one elected thread issues 8 K-steps x 3 products (A_hi.B_hi,
-//      A_hi.B_lo, A_lo.B_hi; M = 128, N = 64, K = 8) into one TMEM
+// Each CTA (256 threads; two CTAs per SM, ~97 KiB of shared memory each, so
+// one CTA's loads and CUDA-core phases overlap the other's tensor-core work)
+// processes 4096-amplitude coset tiles in a grid-stride loop. Per tile:
+//   0. the tile is copied global -> staging buffer S with 16-byte cp.async
+//      (an amplitude pair per copy: tile bit 0 is physical bit 0);
+//   for each block of the pass:
+//   1. S is rearranged into the MMA A operand: 128 rows (the values of the
+//      7 non-block tile bits) x 64 reals (the 32 complex amplitudes of the
+//      block's index, re/im interleaved), K-major with the 128-byte swizzle,
+//      as a BF16 hi part and the BF16 remainder (lo);
+//   2. one elected thread issues 4 K-steps x 3 products (A_hi.B_hi,
+//      A_hi.B_lo, A_lo.B_hi; M = 128, N = 64, K = 16) into one TMEM
 //      accumulator and commits to an mbarrier;
 //   3. every thread reads its row's 32 results back from TMEM and writes
-//      them to S at the amplitudes' tile positions.
-// The tile is then written back to global with the pass's remap permutation.
+//      them to S at the amplitudes' tile positions;
+//   4. the tile is written back to global with the pass's remap permutation
+//      (16-byte stores of amplitude pairs).
 // The block matrices (B operands, hi and lo) are staged in shared memory
 // once per CTA. All waits are bounded: on timeout the kernel records an
 // error flag for the host and returns after freeing its TMEM.
+//
+// Accuracy: hi + lo keeps ~16 bits of each FP32 operand and the dropped
+// lo.lo product is ~2^-16 relative, so one block's relative error is about
+// 1e-5 per amplitude; infidelity stays orders of magnitude below 1e-6 over
+// the circuit (checked against complex128 by the tests and the bench).
 #include <cuda_runtime.h>
 
 #include "device_types.h"
@@ -32,13 +39,13 @@ namespace {
 constexpr int NT = 256;
 constexpr int TB = KATE_TILE_BITS;  // 12 tile bits
 constexpr int TS = 1 << TB;
-constexpr uint32_t A_BYTES = 128 * 64 * 4;   // 32 KiB per operand (hi or lo)
+constexpr uint32_t A_BYTES = 128 * 64 * 2;   // 16 KiB per operand part (hi or lo), BF16
 constexpr uint32_t S_BYTES = TS * 8;         // 32 KiB staging tile (float2)
 constexpr uint32_t OFF_A = 0;
 constexpr uint32_t OFF_AL = OFF_A + A_BYTES;
 constexpr uint32_t OFF_B = OFF_AL + A_BYTES;                                   // blocks' B images
-constexpr uint32_t OFF_S = OFF_B + KATE_C64_MAX_BLOCKS * KATE_BLOCK_IMG_BYTES;  // two staging tiles
-constexpr uint32_t OFF_MISC = OFF_S + 2 * S_BYTES;
+constexpr uint32_t OFF_S = OFF_B + KATE_C64_MAX_BLOCKS * KATE_BLOCK_IMG_BYTES;  // staging tile
+constexpr uint32_t OFF_MISC = OFF_S + S_BYTES;
 constexpr uint32_t SMEM_BYTES = OFF_MISC + 64 + 1024;  // + alignment slack
 constexpr uint32_t TMEM_COLS = 64;
 constexpr long WAIT_LIMIT = 1L << 24;
@@ -50,11 +57,13 @@ __device__ __forceinline__ uint32_t sswz(uint32_t i) { return i ^ ((((i >> 4) ^ 
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-__device__ __forceinline__ float tf32_rna(float x) {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return __uint_as_float(r);
+// BF16 bits of x rounded to nearest even, and the value they encode.
+__device__ __forceinline__ uint32_t bf16_rn(float x) {
+    uint32_t u = __float_as_uint(x);
+    u += 0x7fffu + ((u >> 16) & 1u);
+    return u >> 16;
 }
+__device__ __forceinline__ float bf16_val(uint32_t h) { return __uint_as_float(h << 16); }
 
 // UMMA shared-memory descriptor, K-major, 128-byte swizzle: 8-row groups
 // 1024 bytes apart (SBO), version 1.
@@ -68,14 +77,14 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
     return d;
 }
 
-// Instruction descriptor: D F32, A/B TF32, both K-major, N = 64, M = 128.
-constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+// Instruction descriptor: D F32, A/B BF16, both K-major, N = 64, M = 128.
+constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
 
-__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
         "l"(adesc), "l"(bdesc), "r"(IDESC), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
 }
 
@@ -94,7 +103,12 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
     return false;
 }
 
-__global__ void __launch_bounds__(NT, 1)
+// Byte offset of (row, k) in a K-major SWIZZLE_128B image of 64 BF16 columns.
+__device__ __forceinline__ uint32_t a_off(uint32_t row, uint32_t chunk) {
+    return (row >> 3) * 1024u + (row & 7u) * 128u + ((chunk ^ (row & 7u)) << 4);
+}
+
+__global__ void __launch_bounds__(NT, 2)
     k_block_c64(float2* __restrict__ st, const __grid_constant__ BlockProg P, const uint8_t* __restrict__ bimg,
                 int* __restrict__ err) {
     extern __shared__ uint8_t smem_raw[];
@@ -105,6 +119,8 @@ __global__ void __launch_bounds__(NT, 1)
     const uint32_t mbar = base + OFF_MISC;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(gbase + OFF_MISC + 8);
     int* abort_flag = reinterpret_cast<int*>(gbase + OFF_MISC + 16);
+    float2* S = reinterpret_cast<float2*>(gbase + OFF_S);
+    const uint32_t sb = base + OFF_S;
 
     if (t == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
@@ -130,90 +146,81 @@ __global__ void __launch_bounds__(NT, 1)
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
 
-    // Global offsets: tile element t + 256 j lives at dT(t) + dH(j).
+    // Copy j of thread t moves the amplitude pair e, e + 1 with e = 2t + 512 j
+    // (tile bit 0 is physical bit 0): global offset dT + dH[j]; on write-back
+    // the pair reads the tile at pT | oH[j] and (pT | oH[j]) | o1.
     uint64_t dT = 0;
-    for (int i = 0; i < 8; i++) dT |= (uint64_t)((t >> i) & 1u) << P.tphys[i];
-    uint64_t dH[16];
-    uint32_t oH[16];
     uint32_t pT = 0;
-    for (int i = 0; i < 8; i++) pT |= ((t >> i) & 1u) << P.outsrc[i];
+    for (int i = 0; i < 8; i++) {
+        dT |= (uint64_t)((t >> i) & 1u) << P.tphys[i + 1];
+        pT |= ((t >> i) & 1u) << P.outsrc[i + 1];
+    }
+    uint64_t dH[8];
+    uint32_t oH[8];
 #pragma unroll
-    for (int j = 0; j < 16; j++) {
+    for (int j = 0; j < 8; j++) {
         uint64_t g = 0;
         uint32_t o = 0;
-        for (int i = 0; i < 4; i++)
+        for (int i = 0; i < 3; i++)
             if ((j >> i) & 1) {
-                g |= 1ull << P.tphys[8 + i];
-                o |= 1u << P.outsrc[8 + i];
+                g |= 1ull << P.tphys[9 + i];
+                o |= 1u << P.outsrc[9 + i];
             }
         dH[j] = g;
         oH[j] = o;
     }
+    const uint32_t o1 = 1u << P.outsrc[0];
     auto coset_base = [&](uint64_t c) {
         uint64_t b = 0;
         for (int i = 0; i < P.ncb; i++) b |= ((c >> i) & 1ull) << P.cphys[i];
         return b;
     };
-    auto prefetch = [&](uint64_t c, uint32_t sbuf) {
-        const float2* src = st + coset_base(c) + dT;
-#pragma unroll
-        for (int j = 0; j < 16; j++) {
-            const uint32_t d = sbuf + sswz(t + ((uint32_t)j << 8)) * 8u;
-            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src + dH[j]) : "memory");
-        }
-        asm volatile("cp.async.commit_group;\n" ::: "memory");
-    };
 
     const uint64_t ncos = 1ull << P.ncb;
     uint32_t phase = 0;
-    if ((uint64_t)blockIdx.x < ncos) prefetch(blockIdx.x, base + OFF_S);
-    int it = 0;
-    for (uint64_t c = blockIdx.x; c < ncos; c += gridDim.x, it++) {
-        const uint32_t sb = base + OFF_S + (uint32_t)(it & 1) * S_BYTES;
-        float2* S = reinterpret_cast<float2*>(gbase + OFF_S + (it & 1) * S_BYTES);
-        if (c + gridDim.x < ncos) {
-            prefetch(c + gridDim.x, base + OFF_S + (uint32_t)((it + 1) & 1) * S_BYTES);
-            asm volatile("cp.async.wait_group 1;\n" ::: "memory");
-        } else {
+    for (uint64_t c = blockIdx.x; c < ncos; c += gridDim.x) {
+        const uint64_t cb = coset_base(c);
+        {
+            const float2* src = st + cb + dT;
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                const uint32_t d = sb + sswz(2u * t + ((uint32_t)j << 9)) * 8u;
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src + dH[j]) : "memory");
+            }
+            asm volatile("cp.async.commit_group;\n" ::: "memory");
             asm volatile("cp.async.wait_group 0;\n" ::: "memory");
         }
         __syncthreads();
-        (void)sb;
 
         for (int blk = 0; blk < P.nblocks; blk++) {
-            // Non-block tile bits (ascending): row index bits.
             uint32_t bmask = 0;
             for (int i = 0; i < 5; i++) bmask |= 1u << P.btb[blk][i];
             // 1. A operand (hi, lo) from the staging tile. Thread t: row
-            //    r = t & 127, K half h = t >> 7 (block indices 16h..16h+15).
+            //    r = t & 127, K half h = t >> 7 (block indices 16h..16h+15,
+            //    16-byte chunks 4h..4h+3 of 4 amplitudes each).
             {
                 const uint32_t r = t & 127u, h = t >> 7;
                 uint32_t rbase = 0;
                 for (int i = 0, q = 0; i < TB; i++)
                     if (!((bmask >> i) & 1u)) rbase |= ((r >> q++) & 1u) << i;
-                const uint32_t rowoff = h * 16384u + (r >> 3) * 1024u + (r & 7u) * 128u;
 #pragma unroll
-                for (int cpair = 0; cpair < 8; cpair++) {
-                    float v[4];
+                for (int q = 0; q < 4; q++) {
+                    uint32_t hw[4], lw[4];
 #pragma unroll
-                    for (int e = 0; e < 2; e++) {
-                        const uint32_t b = h * 16u + (uint32_t)(2 * cpair + e);
+                    for (int e = 0; e < 4; e++) {
+                        const uint32_t b = h * 16u + (uint32_t)(4 * q + e);
                         uint32_t idx = rbase;
 #pragma unroll
                         for (int i = 0; i < 5; i++) idx |= ((b >> i) & 1u) << P.btb[blk][i];
                         const float2 a = S[sswz(idx)];
-                        v[2 * e] = a.x;
-                        v[2 * e + 1] = a.y;
+                        const uint32_t hr = bf16_rn(a.x), hi = bf16_rn(a.y);
+                        const uint32_t lr = bf16_rn(a.x - bf16_val(hr)), li = bf16_rn(a.y - bf16_val(hi));
+                        hw[e] = hr | (hi << 16);
+                        lw[e] = lr | (li << 16);
                     }
-                    float hi[4], lo[4];
-#pragma unroll
-                    for (int e = 0; e < 4; e++) {
-                        hi[e] = tf32_rna(v[e]);
-                        lo[e] = v[e] - hi[e];
-                    }
-                    const uint32_t off = rowoff + (((uint32_t)cpair ^ (r & 7u)) << 4);
-                    *reinterpret_cast<float4*>(gbase + OFF_A + off) = make_float4(hi[0], hi[1], hi[2], hi[3]);
-                    *reinterpret_cast<float4*>(gbase + OFF_AL + off) = make_float4(lo[0], lo[1], lo[2], lo[3]);
+                    const uint32_t off = a_off(r, h * 4u + (uint32_t)q);
+                    *reinterpret_cast<uint4*>(gbase + OFF_A + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+                    *reinterpret_cast<uint4*>(gbase + OFF_AL + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
                 }
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -223,14 +230,13 @@ __global__ void __launch_bounds__(NT, 1)
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const uint32_t bb = base + OFF_B + blk * KATE_BLOCK_IMG_BYTES;
 #pragma unroll 1
-                for (int s = 0; s < 8; s++) {
-                    const uint32_t ka = (uint32_t)(s >> 2) * 16384u + (uint32_t)(s & 3) * 32u;
-                    const uint32_t kb = (uint32_t)(s >> 2) * 8192u + (uint32_t)(s & 3) * 32u;
-                    const uint64_t a_hi = sw128_desc(base + OFF_A + ka), a_lo = sw128_desc(base + OFF_AL + ka);
-                    const uint64_t b_hi = sw128_desc(bb + kb), b_lo = sw128_desc(bb + 16384u + kb);
-                    mma_tf32(tmem, a_hi, b_hi, s > 0 ? 1u : 0u);
-                    mma_tf32(tmem, a_hi, b_lo, 1u);
-                    mma_tf32(tmem, a_lo, b_hi, 1u);
+                for (int s = 0; s < 4; s++) {
+                    const uint32_t k = (uint32_t)s * 32u;  // K = 16 BF16 = 32 bytes per step
+                    const uint64_t a_hi = sw128_desc(base + OFF_A + k), a_lo = sw128_desc(base + OFF_AL + k);
+                    const uint64_t b_hi = sw128_desc(bb + k), b_lo = sw128_desc(bb + KATE_BLOCK_IMG_BYTES / 2 + k);
+                    mma_bf16(tmem, a_hi, b_hi, s > 0 ? 1u : 0u);
+                    mma_bf16(tmem, a_hi, b_lo, 1u);
+                    mma_bf16(tmem, a_lo, b_hi, 1u);
                 }
                 asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
                              : "memory");
@@ -275,14 +281,19 @@ __global__ void __launch_bounds__(NT, 1)
             __syncthreads();
         }
         if (*abort_flag) break;
-        // Write back with the remap permutation.
-        float2* dst = st + coset_base(c) + dT;
+        // 4. Write back with the remap permutation, an amplitude pair per store.
+        {
+            float2* dst = st + cb + dT;
 #pragma unroll
-        for (int j = 0; j < 16; j++) dst[dH[j]] = S[sswz(pT | oH[j])];
+            for (int j = 0; j < 8; j++) {
+                const uint32_t src = pT | oH[j];
+                const float2 v0 = S[sswz(src)], v1 = S[sswz(src | o1)];
+                *reinterpret_cast<float4*>(dst + dH[j]) = make_float4(v0.x, v0.y, v1.x, v1.y);
+            }
+        }
         __syncthreads();
     }
     if (*abort_flag && t == 0) atomicExch(err, 1);
-    // Drain any outstanding prefetch before the CTA exits.
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -299,9 +310,17 @@ int block_c64_grid(int n, int device) {
     if (device < 0 || device >= 64) device = 0;
     if (!cached[device]) {
         cudaFuncSetAttribute(k_block_c64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES);
-        int sms = 148;
+        cudaFuncSetAttribute(k_block_c64, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int)cudaSharedmemCarveoutMaxShared);
+        int sms = 148, smem_sm = 0, reserved = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-        cached[device] = sms;
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device);
+        cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, device);
+        // Registers allow two CTAs (__launch_bounds__); shared memory decides.
+        int occ = smem_sm / (int)(SMEM_BYTES + reserved);
+        if (occ < 1) occ = 1;
+        if (occ > 2) occ = 2;
+        cached[device] = sms * occ;
     }
     const uint64_t ncos = 1ull << (n - TB);
     return (int)(ncos < (uint64_t)cached[device] ? ncos : (uint64_t)cached[device]);
@@ -309,6 +328,7 @@ int block_c64_grid(int n, int device) {
 
 cudaError_t launch_block_c64(void* st, const BlockProg& prog, const void* bimg, int* err, int grid, cudaStream_t s) {
     if (prog.m != TB || prog.nblocks < 1 || prog.nblocks > KATE_C64_MAX_BLOCKS) return cudaErrorInvalidValue;
+    if (prog.tphys[0] != 0) return cudaErrorInvalidValue;  // amplitude pairs must be contiguous
     k_block_c64<<<grid, NT, SMEM_BYTES, s>>>((float2*)st, prog, (const uint8_t*)bimg, err);
     return cudaGetLastError();
 }

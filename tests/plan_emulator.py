@@ -39,13 +39,12 @@ BLOCK_DTYPE = np.dtype([("m", "<i4"), ("ncb", "<i4"), ("nblocks", "<i4"), ("pad"
                         ("outsrc", "u1", 16), ("cphys", "u1", 48), ("btb", "u1", (2, 8)), ("bimg", "<u8", 2)])
 
 
-def _sw128_offsets(rows):
-    """Byte offset of (row, k) in a K-major SWIZZLE_128B image, 64 columns."""
+def _sw128_offsets_bf16(rows):
+    """Byte offset of (row, k) in a K-major SWIZZLE_128B image of 64 BF16 columns."""
     r = np.arange(rows)[:, None]
     k = np.arange(64)[None, :]
-    khalf, kk = k >> 5, k & 31
-    chunk, w = kk >> 2, kk & 3
-    return khalf * rows * 128 + (r >> 3) * 1024 + (r & 7) * 128 + ((chunk ^ (r & 7)) << 4) + w * 4
+    chunk, w = k >> 3, k & 7
+    return (r >> 3) * 1024 + (r & 7) * 128 + ((chunk ^ (r & 7)) << 4) + w * 2
 
 
 def _swz(i):
@@ -131,11 +130,13 @@ class PlanView:
         L.kate_plan_block_images(h, self.bimg.ctypes.data_as(ctypes.c_void_p), self.bimg.size, ctypes.byref(size))
 
     def block_matrix(self, off):
-        """The real 64x64 W = hi + lo read back from a block's operand images."""
-        o = _sw128_offsets(64)
-        hi = self.bimg[off:off + 16384].view(np.float32)
-        lo = self.bimg[off + 16384:off + 32768].view(np.float32)
-        return hi[o // 4].astype(np.float64) + lo[o // 4].astype(np.float64)
+        """The real 64x64 W = hi + lo read back from a block's BF16 operand images."""
+        o = _sw128_offsets_bf16(64)
+        def dec(b):
+            return (b.view(np.uint16).astype(np.uint32) << 16).view(np.float32)
+        hi = dec(self.bimg[off:off + 8192])
+        lo = dec(self.bimg[off + 8192:off + 16384])
+        return hi[o // 2].astype(np.float64) + lo[o // 2].astype(np.float64)
 
     def run_blocks(self, state):
         """Executes complex64 block programs (the others generically): each

@@ -1,6 +1,7 @@
-"""Complex64 path: 5-qubit dense blocks on the tensor cores (3xTF32, FP32
-accumulation) and the complex64 generic kernel, against the oracle's FP64
-states. Bar: infidelity 1 - |<psi64|psi128>|^2 <= 1e-6 per circuit."""
+"""Complex64 path: 5-qubit dense blocks on the tensor cores (split-BF16
+products, FP32 accumulation) and the complex64 generic kernel, against the
+oracle's FP64 states. Bar: infidelity 1 - |<psi64|psi128>|^2 <= 1e-6 per
+circuit; amplitudes and <Z> within 1e-4 (about 16 bits kept per operand)."""
 import numpy as np
 import pytest
 
@@ -27,7 +28,7 @@ def test_c64_random_circuits(oracle, n):
     ref = oracle.simulate(n, gates)
     got = sim.state()
     assert infidelity(got, ref) <= 1e-6
-    assert np.abs(got - ref).max() <= 1e-5
+    assert np.abs(got - ref).max() <= 1e-4
 
 
 def test_c64_brickwork_su4_fused_blocks(oracle):
@@ -52,4 +53,4 @@ def test_c64_layered_and_measurements(oracle):
     p = np.abs(ref) ** 2
     z = np.array([p[((np.arange(1 << n) >> q) & 1) == 0].sum() - p[((np.arange(1 << n) >> q) & 1) == 1].sum()
                   for q in range(n)])
-    assert np.abs(sim.expect_z() - z).max() <= 1e-5
+    assert np.abs(sim.expect_z() - z).max() <= 1e-4

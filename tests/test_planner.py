@@ -141,3 +141,23 @@ def test_multi_qubit_diagonals_become_register_ops(oracle, seed):
     assert all(p is not None for p in pv.programs)
     assert pv.smem_ops == [] or len(pv.smem_ops) == 0
     assert np.abs(pv.run_staged(zero_state(n)) - oracle.simulate(n, gates)).max() <= 1e-12
+
+
+@pytest.mark.parametrize("seed", range(3))
+def test_c64_block_programs_match_oracle(oracle, seed):
+    """Complex64 plans: each pass's 5-qubit blocks, read back from their BF16
+    hi/lo operand images and applied as the tensor-core kernel does, give the
+    oracle's state (the image split keeps about 16 bits per entry)."""
+    rng = np.random.default_rng(700 + seed)
+    n = 13 + seed
+    gates = circuits.brickwork_su4(n, 6, seed=seed) + random_circuit(n, 40, rng, kinds=("h", "cnot", "crk", "d1", "d2"))
+    c = K.Circuit(n, gates)
+    c.gateScheduling()
+    c.gateFusion(5, 1e-6)
+    pv = PlanView(c, 12, 4, 4)
+    assert any(bp is not None for bp in pv.block_programs)
+    got = pv.run_blocks(zero_state(n))
+    ref = oracle.simulate(n, gates)
+    a, b = got / np.linalg.norm(got), ref / np.linalg.norm(ref)
+    assert 1 - abs(np.vdot(a, b)) ** 2 <= 1e-8
+    assert np.abs(got - ref).max() <= 1e-4
