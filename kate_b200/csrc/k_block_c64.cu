@@ -45,8 +45,9 @@ constexpr uint32_t OFF_A = 0;
 constexpr uint32_t OFF_AL = OFF_A + A_BYTES;
 constexpr uint32_t OFF_B = OFF_AL + A_BYTES;                                   // blocks' B images
 constexpr uint32_t OFF_S = OFF_B + KATE_C64_MAX_BLOCKS * KATE_BLOCK_IMG_BYTES;  // staging tile
-constexpr uint32_t OFF_MISC = OFF_S + S_BYTES;
-constexpr uint32_t SMEM_BYTES = OFF_MISC + 64 + 1024;  // + alignment slack
+constexpr uint32_t OFF_MISC = OFF_S + S_BYTES;           // mbarrier, TMEM slot, abort flag
+constexpr uint32_t OFF_TAB = OFF_MISC + 64;              // per block: swizzled tile offset of block index b
+constexpr uint32_t SMEM_BYTES = OFF_TAB + KATE_C64_MAX_BLOCKS * 32 * 2 + 1024;  // + alignment slack
 constexpr uint32_t TMEM_COLS = 64;
 constexpr long WAIT_LIMIT = 1L << 24;
 
@@ -57,13 +58,13 @@ __device__ __forceinline__ uint32_t sswz(uint32_t i) { return i ^ ((((i >> 4) ^ 
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-// BF16 bits of x rounded to nearest even, and the value they encode.
-__device__ __forceinline__ uint32_t bf16_rn(float x) {
-    uint32_t u = __float_as_uint(x);
-    u += 0x7fffu + ((u >> 16) & 1u);
-    return u >> 16;
+// Two floats rounded to BF16 (nearest even) and packed: lo in bits 0..15,
+// hi in bits 16..31.
+__device__ __forceinline__ uint32_t bf16x2_rn(float lo, float hi) {
+    uint32_t d;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
+    return d;
 }
-__device__ __forceinline__ float bf16_val(uint32_t h) { return __uint_as_float(h << 16); }
 
 // UMMA shared-memory descriptor, K-major, 128-byte swizzle: 8-row groups
 // 1024 bytes apart (SBO), version 1.
@@ -146,6 +147,36 @@ __global__ void __launch_bounds__(NT, 2)
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
 
+    // Per block: tab[b] = sswz of block index b deposited into the block's
+    // tile bits, and for this thread the sswz of its A row (r = t & 127) and
+    // of its TMEM row (r = 32 (warp & 3) + lane) deposited into the other
+    // bits. sswz is linear over GF(2), so a tile offset is rsw ^ tab[b].
+    uint16_t* tab = reinterpret_cast<uint16_t*>(gbase + OFF_TAB);
+    uint32_t rsa[KATE_C64_MAX_BLOCKS], rsr[KATE_C64_MAX_BLOCKS];
+#pragma unroll
+    for (int blk = 0; blk < KATE_C64_MAX_BLOCKS; blk++) {
+        rsa[blk] = rsr[blk] = 0;
+        if (blk >= P.nblocks) continue;
+        uint32_t bmask = 0;
+        for (int i = 0; i < 5; i++) bmask |= 1u << P.btb[blk][i];
+        const uint32_t ra = t & 127u, rr = (warp & 3u) * 32u + lane;
+        uint32_t da = 0, dr = 0;
+        for (int i = 0, q = 0; i < TB; i++)
+            if (!((bmask >> i) & 1u)) {
+                da |= ((ra >> q) & 1u) << i;
+                dr |= ((rr >> q) & 1u) << i;
+                q++;
+            }
+        rsa[blk] = sswz(da);
+        rsr[blk] = sswz(dr);
+        if (t < 32) {
+            uint32_t idx = 0;
+            for (int i = 0; i < 5; i++) idx |= ((t >> i) & 1u) << P.btb[blk][i];
+            tab[blk * 32 + t] = (uint16_t)sswz(idx);
+        }
+    }
+    __syncthreads();
+
     // Copy j of thread t moves the amplitude pair e, e + 1 with e = 2t + 512 j
     // (tile bit 0 is physical bit 0): global offset dT + dH[j]; on write-back
     // the pair reads the tile at pT | oH[j] and (pT | oH[j]) | o1.
@@ -193,30 +224,24 @@ __global__ void __launch_bounds__(NT, 2)
         __syncthreads();
 
         for (int blk = 0; blk < P.nblocks; blk++) {
-            uint32_t bmask = 0;
-            for (int i = 0; i < 5; i++) bmask |= 1u << P.btb[blk][i];
+            const uint16_t* tb = tab + blk * 32;
+            const uint32_t ra_sw = blk == 0 ? rsa[0] : rsa[KATE_C64_MAX_BLOCKS - 1];
+            const uint32_t rr_sw = blk == 0 ? rsr[0] : rsr[KATE_C64_MAX_BLOCKS - 1];
             // 1. A operand (hi, lo) from the staging tile. Thread t: row
             //    r = t & 127, K half h = t >> 7 (block indices 16h..16h+15,
             //    16-byte chunks 4h..4h+3 of 4 amplitudes each).
             {
                 const uint32_t r = t & 127u, h = t >> 7;
-                uint32_t rbase = 0;
-                for (int i = 0, q = 0; i < TB; i++)
-                    if (!((bmask >> i) & 1u)) rbase |= ((r >> q++) & 1u) << i;
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
                     uint32_t hw[4], lw[4];
 #pragma unroll
                     for (int e = 0; e < 4; e++) {
-                        const uint32_t b = h * 16u + (uint32_t)(4 * q + e);
-                        uint32_t idx = rbase;
-#pragma unroll
-                        for (int i = 0; i < 5; i++) idx |= ((b >> i) & 1u) << P.btb[blk][i];
-                        const float2 a = S[sswz(idx)];
-                        const uint32_t hr = bf16_rn(a.x), hi = bf16_rn(a.y);
-                        const uint32_t lr = bf16_rn(a.x - bf16_val(hr)), li = bf16_rn(a.y - bf16_val(hi));
-                        hw[e] = hr | (hi << 16);
-                        lw[e] = lr | (li << 16);
+                        const float2 a = S[ra_sw ^ tb[h * 16u + (uint32_t)(4 * q + e)]];
+                        const uint32_t hp = bf16x2_rn(a.x, a.y);
+                        const float hre = __uint_as_float(hp << 16), him = __uint_as_float(hp & 0xffff0000u);
+                        hw[e] = hp;
+                        lw[e] = bf16x2_rn(a.x - hre, a.y - him);
                     }
                     const uint32_t off = a_off(r, h * 4u + (uint32_t)q);
                     *reinterpret_cast<uint4*>(gbase + OFF_A + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
@@ -251,7 +276,6 @@ __global__ void __launch_bounds__(NT, 2)
             //    columns 32(w>>2)..+31 (block indices 16(w>>2)..+15).
             {
                 const uint32_t sub = warp & 3u, ch = warp >> 2;
-                const uint32_t r = sub * 32u + lane;
                 uint32_t d[32];
                 const uint32_t taddr = tmem + ((sub * 32u) << 16) + ch * 32u;
                 asm volatile(
@@ -265,17 +289,10 @@ __global__ void __launch_bounds__(NT, 2)
                       "=r"(d[29]), "=r"(d[30]), "=r"(d[31])
                     : "r"(taddr));
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                uint32_t rbase = 0;
-                for (int i = 0, q = 0; i < TB; i++)
-                    if (!((bmask >> i) & 1u)) rbase |= ((r >> q++) & 1u) << i;
 #pragma unroll
-                for (int e = 0; e < 16; e++) {
-                    const uint32_t b = ch * 16u + (uint32_t)e;
-                    uint32_t idx = rbase;
-#pragma unroll
-                    for (int i = 0; i < 5; i++) idx |= ((b >> i) & 1u) << P.btb[blk][i];
-                    S[sswz(idx)] = make_float2(__uint_as_float(d[2 * e]), __uint_as_float(d[2 * e + 1]));
-                }
+                for (int e = 0; e < 16; e++)
+                    S[rr_sw ^ tb[ch * 16u + (uint32_t)e]] =
+                        make_float2(__uint_as_float(d[2 * e]), __uint_as_float(d[2 * e + 1]));
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncthreads();
