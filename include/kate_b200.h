@@ -59,7 +59,7 @@ typedef enum {
 
 typedef enum {
     KATE_C128 = 0, /* complex128 state, FP64 arithmetic (the reference's only form) */
-    KATE_C64 = 1   /* complex64 state; fused dense blocks on tensor cores (3xTF32) */
+    KATE_C64 = 1   /* complex64 state; fused dense blocks on tensor cores (split-BF16 products, FP32 accumulation) */
 } kate_precision;
 
 /* Gate identifiers, as the reference defines them (backendagnosticcode/agnosticpreprocessor.hpp:28-33). */
