@@ -166,6 +166,25 @@ def committed_traffic(n):
         return None
 
 
+def max_over_ranks(ms, device=None):
+    """The slowest rank's time (torch.distributed all-reduce MAX; the group
+    may be NCCL on GPUs or gloo on CPU). Returns ms unchanged without a
+    process group."""
+    import torch
+    import torch.distributed as tdist
+    if not (tdist.is_available() and tdist.is_initialized()):
+        return ms
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(units_per_rank, ms_max, world):
+    """Whole-job throughput of N independent replicas: all ranks' units over
+    the slowest rank's time."""
+    return world * units_per_rank / (ms_max / 1000.0)
+
+
 def cpu_reference_sample(n, seed):
     """Times one layer of the n-qubit circuit on the reference's CPU simulator."""
     from kate_b200 import circuits
@@ -283,11 +302,9 @@ def main():
     torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1)
     if dist:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(ms, dev)
     ms_per_step = ms / args.steps
-    value = world * args.steps * L / (ms / 1000.0)
+    value = replica_rate(args.steps * L, ms, world)
 
     # Per-launch times of the group-pass kernel (events between launches).
     init_ms, pass_ms = sim.profile_passes()
@@ -306,9 +323,7 @@ def main():
         s2.close()
     e2e_ms = (time.perf_counter() - t0) * 1000.0 / e2e_steps
     if dist:
-        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+        e2e_ms = max_over_ranks(e2e_ms, dev)
     n_ops = sum(ng for _, ng in passes)
     h2d = n_ops * 112 + 16 * (4 ** 1) * n_ops + 2 * n * 8
     d2h = 2 * n * 8 + 16 * (1 + 2 * (12 + 4)) * (1 << 14)
