@@ -31,6 +31,12 @@ __device__ __forceinline__ void cfma(double2& acc, double2 a, double2 b) {
 }
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) { return cmulf(a, b); }
+// Complex products for the register stages: complex64 in packed FP32
+// (sm_100), b.re * a + b.im * (i a); complex128 as cmul.
+__device__ __forceinline__ float2 cmul_r(float2 a, float2 b) {
+    return __ffma2_rn(make_float2(b.y, b.y), make_float2(-a.y, a.x), __fmul2_rn(make_float2(b.x, b.x), a));
+}
+__device__ __forceinline__ double2 cmul_r(double2 a, double2 b) { return cmul(a, b); }
 __device__ __forceinline__ void cfma(float2& acc, float2 a, float2 b) {
     acc.x = fmaf(a.x, b.x, acc.x);
     acc.x = fmaf(-a.y, b.y, acc.x);

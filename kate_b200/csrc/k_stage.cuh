@@ -48,6 +48,10 @@ struct Amp<float2> {
     static constexpr int SH = 3;
     static constexpr int NCP = 8;  // each 16-byte copy moves an adjacent pair of amplitudes
     __device__ __forceinline__ static R fm(R a, R b, R c) { return fmaf(a, b, c); }
+    // Packed FP32 (sm_100): s * v, s * v + w, and i * v.
+    __device__ __forceinline__ static float2 mul_s(R s, float2 v) { return __fmul2_rn(make_float2(s, s), v); }
+    __device__ __forceinline__ static float2 fma_s(R s, float2 v, float2 w) { return __ffma2_rn(make_float2(s, s), v, w); }
+    __device__ __forceinline__ static float2 rot(float2 v) { return make_float2(-v.y, v.x); }
     __device__ __forceinline__ static float2 mk(R x, R y) { return make_float2(x, y); }
     __device__ __forceinline__ static float2 lds(uint32_t addr) {
         float2 v;
@@ -59,7 +63,12 @@ struct Amp<float2> {
     }
 };
 
-// r = u0 * x + u1 * y (complex): 8 FMA-class ops.
+// r = u0 * x + u1 * y (complex): 8 FMA-class ops (complex64: 4 packed ops
+// on x, y and their i-rotations).
+__device__ __forceinline__ float2 row2(float2 u0, float2 u1, float2 x, float2 y) {
+    using A = Amp<float2>;
+    return A::fma_s(u1.y, A::rot(y), A::fma_s(u1.x, y, A::fma_s(u0.y, A::rot(x), A::mul_s(u0.x, x))));
+}
 template <typename C2>
 __device__ __forceinline__ C2 row2(C2 u0, C2 u1, C2 x, C2 y) {
     using A = Amp<C2>;
@@ -95,9 +104,15 @@ __device__ __forceinline__ void reg_h(C2 (&a)[16]) {
         if ((j >> B) & 1) continue;
         const int k = j | (1 << B);
         const C2 x = a[j], y = a[k];
-        const C2 n0 = Amp<C2>::mk((x.x + y.x) * (R)KATE_SQRT2INV, (x.y + y.y) * (R)KATE_SQRT2INV);
-        a[j] = n0;
-        a[k] = Amp<C2>::mk(n0.x - y.x * (R)KATE_SQRT2, n0.y - y.y * (R)KATE_SQRT2);
+        if constexpr (sizeof(C2) == 8) {
+            const float2 n0 = Amp<float2>::mul_s((R)KATE_SQRT2INV, __fadd2_rn(x, y));
+            a[j] = n0;
+            a[k] = Amp<float2>::fma_s(-(R)KATE_SQRT2, y, n0);
+        } else {
+            const C2 n0 = Amp<C2>::mk((x.x + y.x) * (R)KATE_SQRT2INV, (x.y + y.y) * (R)KATE_SQRT2INV);
+            a[j] = n0;
+            a[k] = Amp<C2>::mk(n0.x - y.x * (R)KATE_SQRT2, n0.y - y.y * (R)KATE_SQRT2);
+        }
     }
 }
 
@@ -123,8 +138,13 @@ __device__ __forceinline__ void reg_ur(C2 (&a)[16], R u00, R u01, R u10, R u11) 
         if ((j >> B) & 1) continue;
         const int k = j | (1 << B);
         const C2 x = a[j], y = a[k];
-        a[j] = A::mk(A::fm(u01, y.x, u00 * x.x), A::fm(u01, y.y, u00 * x.y));
-        a[k] = A::mk(A::fm(u11, y.x, u10 * x.x), A::fm(u11, y.y, u10 * x.y));
+        if constexpr (sizeof(C2) == 8) {
+            a[j] = Amp<float2>::fma_s(u01, y, Amp<float2>::mul_s(u00, x));
+            a[k] = Amp<float2>::fma_s(u11, y, Amp<float2>::mul_s(u10, x));
+        } else {
+            a[j] = A::mk(A::fm(u01, y.x, u00 * x.x), A::fm(u01, y.y, u00 * x.y));
+            a[k] = A::mk(A::fm(u11, y.x, u10 * x.x), A::fm(u11, y.y, u10 * x.y));
+        }
     }
 }
 
@@ -137,8 +157,14 @@ __device__ __forceinline__ void reg_ux(C2 (&a)[16], R u00, R u01i, R u10i, R u11
         if ((j >> B) & 1) continue;
         const int k = j | (1 << B);
         const C2 x = a[j], y = a[k];
-        a[j] = A::mk(A::fm(-u01i, y.y, u00 * x.x), A::fm(u01i, y.x, u00 * x.y));
-        a[k] = A::mk(A::fm(-u10i, x.y, u11 * y.x), A::fm(u10i, x.x, u11 * y.y));
+        if constexpr (sizeof(C2) == 8) {
+            using F = Amp<float2>;
+            a[j] = F::fma_s(u01i, F::rot(y), F::mul_s(u00, x));
+            a[k] = F::fma_s(u10i, F::rot(x), F::mul_s(u11, y));
+        } else {
+            a[j] = A::mk(A::fm(-u01i, y.y, u00 * x.x), A::fm(u01i, y.x, u00 * x.y));
+            a[k] = A::mk(A::fm(-u10i, x.y, u11 * y.x), A::fm(u10i, x.x, u11 * y.y));
+        }
     }
 }
 
@@ -461,7 +487,7 @@ __device__ __forceinline__ void run_program(const TileTables<C2>& T, int nops, u
             const C2 ph = T.mats[op.idx];
 #pragma unroll
             for (int j = 0; j < 16; j++)
-                if (((uint32_t)j & op.creg) == op.creg) a[j] = cmul(a[j], ph);
+                if (((uint32_t)j & op.creg) == op.creg) a[j] = cmul_r(a[j], ph);
             break;
         }
         case SOP_D1: {
@@ -469,12 +495,12 @@ __device__ __forceinline__ void run_program(const TileTables<C2>& T, int nops, u
             const bool b = op.src == SRC_THR ? ((t >> op.a) & 1u) : (uint32_t)((cbase >> op.a) & 1ull);
             const C2 d = b ? d1 : d0;
 #pragma unroll
-            for (int j = 0; j < 16; j++) a[j] = cmul(a[j], d);
+            for (int j = 0; j < 16; j++) a[j] = cmul_r(a[j], d);
             break;
         }
         case SOP_DR: {
 #pragma unroll
-            for (int j = 0; j < 16; j++) a[j] = cmul(a[j], T.mats[op.idx + j]);
+            for (int j = 0; j < 16; j++) a[j] = cmul_r(a[j], T.mats[op.idx + j]);
             break;
         }
         default:
