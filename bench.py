@@ -21,6 +21,10 @@ pass = 20 layers). Metric: layers per second of the gate phase.
             headers into oracle/_ref) on a bounded sample: one layer of the
             same 30-qubit circuit, compiled as the reference's best CPU
             configuration (scheduling, fusion(5), grouping(12)).
+  ref_gpu_baseline  the reference's own GPU path (its HIPcode headers built
+            with nvcc into oracle/_ref) on the same GPU and circuit, with
+            scheduling, fusion(5) and grouping(9), gate phase on the wall
+            clock; its proba_state is compared with this library's.
 
 ``--impl reference`` times the reference's CPU implementation alone on this
 workload (same metric), rank 0 only. ``--gpus N`` (torchrun) runs N
@@ -74,6 +78,7 @@ def parse():
     ap.add_argument("--step-us", type=int, default=0, help="serve: step latency target in us (0: default)")
     ap.add_argument("--seed", type=int, default=1234)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true", help="layers: skip the reference's own GPU path")
     ap.add_argument("--no-autotune", action="store_true", help="batch: default plan choices")
     ap.add_argument("--no-baseline", action="store_true", help="batch/serve: skip the one-at-a-time baseline")
     a = ap.parse_args()
@@ -214,6 +219,46 @@ def cpu_reference_sample(n, seed):
             "sample": f"1 layer at n={nn} on the C restatement, scaled by 2^{n - nn}", "ms_per_layer": ms}
 
 
+def reference_gpu_sample(n, L, seed, kate_proba=None, budget_s=90.0):
+    """The reference's own GPU path on this GPU (oracle/_ref/libkate_ref_gpu.so,
+    built from its HIPcode headers): the same circuit through gateScheduling,
+    gateFusion(5, 1e-6), gateGrouping(9) (the largest group its kernel keeps
+    inside its shared memory) and compileDefault(0). Its gate phase
+    (executeCommand per group, each ending in a device synchronise) is timed
+    on the wall clock: one warm-up run, then up to 3 runs within budget_s.
+    Its proba_state is compared with this library's (kate_proba)."""
+    import numpy as np
+    from kate_b200 import circuits
+    from oracle import ref_gpu
+
+    if not ref_gpu.available():
+        return {"value": None, "unavailable": "oracle/_ref/libkate_ref_gpu.so was not built"}
+    c = ref_gpu.RefGpuCircuit(n, circuits.layered(n, L, seed))
+    t0 = time.perf_counter()
+    c.compile(fuse=5, mtm=1e-6, group=ref_gpu.MAX_GROUP_QUBITS)
+    plan_s = time.perf_counter() - t0
+    s = c.session()
+    try:
+        t0 = time.perf_counter()
+        runs = [s.run()]
+        while len(runs) < 4 and time.perf_counter() - t0 < budget_s / 2:
+            runs.append(s.run())
+        proba = s.proba_state()
+    finally:
+        s.close()
+    timed = runs[1:] if len(runs) > 1 else runs
+    ms = sum(timed) / len(timed)
+    out = {"value": L / (ms / 1000.0), "unit": UNIT, "ms_per_step": ms, "runs_timed": len(timed),
+           "plan": "gateScheduling + gateFusion(5, 1e-6) + gateGrouping(9) + compileDefault(0)",
+           "plan_s": plan_s, "gates": c.num_gates(), "groups": c.num_groups(), "max_group": c.max_group(),
+           "timing": "wall clock of the reference's instruction loop (it synchronises after every group)"}
+    if kate_proba is not None:
+        d = np.abs(np.asarray(kate_proba) - proba)
+        d[:, 1] = np.minimum(d[:, 1], 2 * np.pi - d[:, 1])
+        out["proba_state_max_abs_diff_vs_kate_b200"] = float(d.max())
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -328,6 +373,16 @@ def main():
     h2d = n_ops * 112 + 16 * (4 ** 1) * n_ops + 2 * n * 8
     d2h = 2 * n * 8 + 16 * (1 + 2 * (12 + 4)) * (1 << 14)
 
+    ref_gpu = None
+    if rank == 0 and world == 1 and not args.no_ref_gpu:
+        kate_proba = sim.execute().as_array()
+        try:
+            ref_gpu = reference_gpu_sample(n, L, args.seed, kate_proba)
+        except Exception as e:  # reported, not fatal
+            ref_gpu = {"value": None, "unavailable": f"failed: {e}"}
+        if ref_gpu.get("value"):
+            ref_gpu["value_speedup"] = value / ref_gpu["value"]
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         del sim
@@ -352,7 +407,7 @@ def main():
                                                   "mean": sum(pass_ms) / len(pass_ms)}},
                 "passes_per_step": len(passes), "passes_per_layer": len(passes) / L,
                 "gpu_launches": launches * args.steps, "clocks": clk.summary(),
-                "cpu_baseline": cpu}
+                "cpu_baseline": cpu, "ref_gpu_baseline": ref_gpu}
         print(json.dumps(line))
     if dist:
         tdist.barrier()

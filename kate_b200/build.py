@@ -82,10 +82,11 @@ def build(verbose: bool = False) -> str:
 
 def build_oracle(with_ref: bool = True, verbose: bool = False) -> None:
     """Compiles oracle/libkate_oracle.so and, when the reference headers are
-    present, oracle/_ref/libkate_ref.so (test infrastructure)."""
+    present, oracle/_ref/libkate_ref.so and oracle/_ref/libkate_ref_gpu.so
+    (test and measurement infrastructure)."""
     targets = ["oracle"]
     if with_ref and os.path.exists("/root/reference/Kate.hpp"):
-        targets.append("ref")
+        targets += ["ref", "refgpu"]
     r = subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), *targets], capture_output=True, text=True)
     if verbose:
         print(r.stdout, r.stderr)
