@@ -632,6 +632,8 @@ def run_batch(args):
     b2 = K.Batch(circs, precision=K.C64, options=b.options)
     b2.run()
     b2.expect_z_flat()
+    create_ms = b2.create_times()
+    h2d = b2.upload_bytes()
     b2.close()
     e2e_s = time.perf_counter() - t0
     # Baseline: one Simulator launch per circuit (plans and states prepared beforehand).
@@ -661,9 +663,9 @@ def run_batch(args):
         w_s = statistics.mean(2.0 ** n for n in ns[:cnt])
         cpu = {"value": cnt / tot * (w_s / w_all), "unit": "circuits/s", "cores": cores, "kind": "reference",
                "sample": f"first {cnt} circuits on the reference CPUSimulator (complex128), rate scaled by mean 2^n"}
-    h2d = info["programs"] * 6000
     cfg.update({"autotuned": tune, "tasks": info["tasks"], "pass_programs": info["programs"],
                 "arena_bytes": info["arena_bytes"], "ctas": info["ctas"], "create_s": create_s,
+                "e2e_create_ms": create_ms, "host_cpus": os.cpu_count(),
                 "baseline_one_launch_per_circuit_cps": plain,
                 "speedup_vs_one_launch_per_circuit": value / plain if plain else None})
     print(json.dumps(_common(

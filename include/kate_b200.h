@@ -327,6 +327,13 @@ KATE_API kate_status kate_batch_info(const kate_batch* b, long long* info);
 KATE_API kate_status kate_batch_circuit_info(const kate_batch* b, int* programs, int* resident_qubits);
 /* Average device time of `runs` back-to-back runs (CUDA events). */
 KATE_API kate_status kate_batch_time(kate_batch* b, int runs, float* ms);
+/* Host wall time of kate_batch_create in ms, ms[0..3]: planning (host
+ * threads), assembly of the task queue, device buffers and uploads, graph
+ * capture and instantiation. */
+KATE_API kate_status kate_batch_create_times(const kate_batch* b, double* ms);
+/* Bytes kate_batch_create copied from host to device (task queue, circuit
+ * and program tables, program data, matrices). */
+KATE_API kate_status kate_batch_upload_bytes(const kate_batch* b, long long* bytes);
 
 /* ---- serving: a request stream with continuous batching ----
  * Replaces a caller's loop that blocks on `Simulator(circuit).execute()`

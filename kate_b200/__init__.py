@@ -456,6 +456,18 @@ class Batch:
         _check(self._lib.kate_batch_info(self._h, v))
         return {"tasks": v[0], "programs": v[1], "arena_bytes": v[2], "ctas": v[3]}
 
+    def create_times(self) -> dict:
+        """Host wall time of the batch's creation, in ms, per phase."""
+        v = (ctypes.c_double * 4)()
+        _check(self._lib.kate_batch_create_times(self._h, v))
+        return {"plan": v[0], "assemble": v[1], "upload": v[2], "graph": v[3]}
+
+    def upload_bytes(self) -> int:
+        """Host-to-device bytes copied when the batch was created."""
+        v = ctypes.c_longlong()
+        _check(self._lib.kate_batch_upload_bytes(self._h, ctypes.byref(v)))
+        return v.value
+
     def circuit_info(self):
         """(pass programs, resident qubits) per circuit; resident qubits is 0
         for circuits run in shared memory."""

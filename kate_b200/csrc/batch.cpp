@@ -7,6 +7,8 @@
 #include <atomic>
 #include <cstring>
 #include <map>
+#include <chrono>
+#include <memory>
 #include <thread>
 
 #include "launch.hpp"
@@ -121,32 +123,41 @@ std::string pack_circuit(const Program& in, const BatchTune& tune, bool resident
         header(nullptr, bp);
         out.progs.push_back(bp);
     }
+    // Register-staged programs carry their own matrices; only shared-memory
+    // ops and generic passes read the pool, so without them it is not sent.
+    if (out.sops.empty() && out.generic.empty()) std::vector<Cx>().swap(out.pool);
     return "";
 }
 
 namespace {
 
-// Plans every circuit on host threads.
-std::vector<CircPack> pack_all(const std::vector<const Program*>& circuits, const BatchOptions& opt) {
-    std::vector<CircPack> packs(circuits.size());
+// Runs f(i) for i in [0, count) on up to 32 host threads (one below 8 items).
+template <typename F>
+void for_each_item(size_t count, F f) {
     std::atomic<size_t> next{0};
     auto work = [&]() {
-        for (size_t i; (i = next.fetch_add(1)) < circuits.size();) {
-            const BatchTune& tu = opt.for_n(circuits[i]->nqbits);
-            try {
-                packs[i].err = pack_circuit(*circuits[i], tu, false, packs[i]);
-            } catch (const std::exception& ex) {
-                packs[i].err = ex.what();
-            }
-        }
+        for (size_t i; (i = next.fetch_add(1)) < count;) f(i);
     };
     unsigned nt = std::thread::hardware_concurrency();
     nt = std::max(1u, std::min(nt, 32u));
-    if (circuits.size() < 8) nt = 1;
+    if (count < 8) nt = 1;
     std::vector<std::thread> th;
     for (unsigned k = 1; k < nt; k++) th.emplace_back(work);
     work();
     for (auto& x : th) x.join();
+}
+
+// Plans every circuit on host threads.
+std::vector<CircPack> pack_all(const std::vector<const Program*>& circuits, const BatchOptions& opt) {
+    std::vector<CircPack> packs(circuits.size());
+    for_each_item(circuits.size(), [&](size_t i) {
+        const BatchTune& tu = opt.for_n(circuits[i]->nqbits);
+        try {
+            packs[i].err = pack_circuit(*circuits[i], tu, false, packs[i]);
+        } catch (const std::exception& ex) {
+            packs[i].err = ex.what();
+        }
+    });
     return packs;
 }
 
@@ -168,7 +179,8 @@ struct BatchImpl {
     std::vector<BatchCirc> circs;
     std::vector<int> cprogs, cres;  // per circuit: programs, resident qubits
     std::vector<BatchProg> progs;
-    std::vector<uint8_t> blob;
+    std::unique_ptr<uint8_t[]> blob;  // concatenated program blobs (host copy, freed after upload)
+    uint64_t blob_bytes = 0;
     std::vector<DevOp> sops;
     std::vector<Cx> pool;
     void* d_arena = nullptr;
@@ -185,6 +197,8 @@ struct BatchImpl {
     cudaStream_t stream = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    double create_ms[4] = {0, 0, 0, 0};  // planning, assembly, device buffers + uploads, graph
+    uint64_t upload_bytes = 0;           // host-to-device bytes copied by create()
 
     size_t amp_bytes() const { return precision == 0 ? 16 : 8; }
 
@@ -230,7 +244,12 @@ std::string Batch::create(const std::vector<const Program*>& circuits, int preci
     for (const Program* p : circuits)
         if (!p) return "null circuit";
     const int chunk = std::max(1, opt.chunk), zchunks = std::max(1, opt.zchunks);
+    using clk = std::chrono::steady_clock;
+    auto ms_since = [](clk::time_point t) { return std::chrono::duration<double, std::milli>(clk::now() - t).count(); };
+    clk::time_point t0 = clk::now();
     std::vector<CircPack> packs = pack_all(circuits, opt);
+    const double plan_ms = ms_since(t0);
+    t0 = clk::now();
     for (size_t i = 0; i < packs.size(); i++)
         if (!packs[i].err.empty()) return "circuit " + std::to_string(i) + ": " + packs[i].err;
 
@@ -243,60 +262,121 @@ std::string Batch::create(const std::vector<const Program*>& circuits, int preci
     S->device = device;
     S->precision = precision;
     S->ncirc = (int)circuits.size();
+    S->create_ms[0] = plan_ms;
 
-    // Concatenate the packs; lay the large states out in the arena.
-    std::vector<int> prog0(packs.size());
-    for (size_t i = 0; i < packs.size(); i++) {
+    // Concatenate the packs: offsets first, then every pack copied in
+    // parallel into buffers allocated once (uninitialised, so each page is
+    // first touched by the thread that fills it). Large states are laid out
+    // in the arena in circuit order.
+    const size_t np = packs.size();
+    std::vector<uint64_t> boff(np), poff(np), soff(np);
+    std::vector<int> prog0(np);
+    {
+        uint64_t bsz = 0, psz = 0, ssz = 0, gsz = 0;
+        S->circs.resize(np);
+        S->cprogs.resize(np);
+        S->cres.resize(np);
+        for (size_t i = 0; i < np; i++) {
+            const CircPack& P = packs[i];
+            bsz = (bsz + 15) & ~uint64_t(15);
+            boff[i] = bsz;
+            bsz += P.blob.size();
+            poff[i] = psz;
+            psz += P.pool.size();
+            soff[i] = ssz;
+            ssz += P.sops.size();
+            prog0[i] = (int)gsz;
+            gsz += P.progs.size();
+            BatchCirc bc{};
+            bc.n = P.n_out;
+            bc.zoff = S->nout;
+            bc.poff = -1;
+            S->nout += P.n_out;
+            for (int x = 0; x < P.n_out; x++) bc.zbit[x] = P.zbit[x];
+            if (!P.small) {
+                bc.off = S->arena_amps;
+                S->arena_amps += 1ull << P.n_sim;
+            }
+            S->circs[i] = bc;
+            S->cprogs[i] = (int)P.progs.size();
+            S->cres[i] = P.small ? 0 : P.n_sim;
+        }
+        if (ssz > (uint64_t)INT32_MAX || gsz > (uint64_t)INT32_MAX) return fail("too many programs or shared-memory ops");
+        S->blob_bytes = std::max<uint64_t>(16, bsz);
+        S->blob.reset(new uint8_t[S->blob_bytes]);
+        S->pool.resize(psz);
+        S->sops.resize(ssz);
+        S->progs.resize(gsz);
+    }
+    for_each_item(np, [&](size_t i) {
         CircPack& P = packs[i];
-        const uint64_t bbase = (S->blob.size() + 15) & ~uint64_t(15);
-        S->blob.resize(bbase);
-        S->blob.insert(S->blob.end(), P.blob.begin(), P.blob.end());
-        const int64_t pbase = (int64_t)S->pool.size();
-        const int sbase = (int)S->sops.size();
+        uint8_t* bl = S->blob.get() + boff[i];
+        const uint64_t end = i + 1 < np ? boff[i + 1] : S->blob_bytes;
+        if (!P.blob.empty()) std::memcpy(bl, P.blob.data(), P.blob.size());
+        std::memset(bl + P.blob.size(), 0, end - boff[i] - P.blob.size());  // alignment padding
+        const int64_t pbase = (int64_t)poff[i];
         for (auto& g : P.generic) {
-            DevOp* ops = reinterpret_cast<DevOp*>(S->blob.data() + bbase + g.first);
+            DevOp* ops = reinterpret_cast<DevOp*>(bl + g.first);
             for (int k = 0; k < g.second; k++) ops[k].mat += pbase;
         }
-        for (DevOp d : P.sops) {
-            d.mat += pbase;
-            S->sops.push_back(d);
+        DevOp* so = S->sops.data() + soff[i];
+        for (size_t k = 0; k < P.sops.size(); k++) {
+            so[k] = P.sops[k];
+            so[k].mat += pbase;
         }
-        S->pool.insert(S->pool.end(), P.pool.begin(), P.pool.end());
-        prog0[i] = (int)S->progs.size();
-        for (BatchProg bp : P.progs) {
-            bp.ops_off += bbase;
-            bp.mats_off += bbase;
-            bp.stab_off += bbase;
-            bp.sop0 += sbase;
-            S->progs.push_back(bp);
+        std::copy(P.pool.begin(), P.pool.end(), S->pool.begin() + (ptrdiff_t)poff[i]);
+        BatchProg* pr = S->progs.data() + prog0[i];
+        for (size_t k = 0; k < P.progs.size(); k++) {
+            BatchProg bp = P.progs[k];
+            bp.ops_off += boff[i];
+            bp.mats_off += boff[i];
+            bp.stab_off += boff[i];
+            bp.sop0 += (int)soff[i];
+            pr[k] = bp;
         }
-        BatchCirc bc{};
-        bc.n = P.n_out;
-        bc.zoff = S->nout;
-        bc.poff = -1;
-        S->nout += P.n_out;
-        for (int x = 0; x < P.n_out; x++) bc.zbit[x] = P.zbit[x];
-        if (!P.small) {
-            bc.off = S->arena_amps;
-            S->arena_amps += 1ull << P.n_sim;
-        }
-        S->circs.push_back(bc);
-        S->cprogs.push_back((int)P.progs.size());
-        S->cres.push_back(P.small ? 0 : P.n_sim);
         std::vector<uint8_t>().swap(P.blob);
         std::vector<Cx>().swap(P.pool);
         std::vector<DevOp>().swap(P.sops);
-    }
-    if (S->sops.size() > (size_t)INT32_MAX) return fail("too many shared-memory ops");
+    });
 
     // Task queue. Large circuits, window by window, level by level; small
     // circuits spread evenly between them (they depend on nothing, so they
-    // fill the waits at level boundaries).
+    // fill the waits at level boundaries): small circuit s goes right after
+    // the first L*s/Sn large tasks, L large tasks in all.
     std::vector<int> large, small;
-    for (size_t i = 0; i < packs.size(); i++) (packs[i].small ? small : large).push_back((int)i);
-    std::vector<BatchTask> ltasks;
+    for (size_t i = 0; i < np; i++) (packs[i].small ? small : large).push_back((int)i);
+    auto pass_tasks = [&](const CircPack& P) -> uint64_t {
+        const uint32_t ncos = 1u << (P.n_sim - KATE_TILE_BITS);
+        const uint32_t cch = std::max<uint32_t>(1, std::min<uint32_t>(chunk, ncos / 16));
+        return (ncos + cch - 1) / cch;
+    };
+    auto zred_tasks = [&](const CircPack& P) -> uint64_t {
+        const uint64_t nch = std::max<uint64_t>(1, (1ull << P.n_sim) >> 16);
+        return (nch + zchunks - 1) / zchunks;
+    };
+    uint64_t L = 0;
+    for (int ci : large) L += pass_tasks(packs[ci]) * packs[ci].progs.size() + zred_tasks(packs[ci]);
+    const uint64_t Sn = small.size();
+    if (L + Sn > (uint64_t)INT32_MAX) return fail("too many tasks");
+    S->tasks.reserve(L + Sn);
+    uint64_t li = 0, si = 0;
+    auto push_small = [&]() {
+        BatchTask st{};
+        st.kind = BT_SMALL;
+        st.circ = small[si];
+        st.prog = prog0[small[si]];
+        st.nprog = (int)packs[small[si]].progs.size();
+        S->tasks.push_back(st);
+        si++;
+    };
+    auto push_large = [&](const BatchTask& t) {
+        while (si < Sn && L * si / Sn <= li) push_small();
+        S->tasks.push_back(t);
+        li++;
+    };
     {
         size_t w0 = 0;
+        std::vector<int> need(large.size(), 0);
         while (w0 < large.size()) {
             size_t w1 = w0;
             uint64_t bytes = 0;
@@ -305,17 +385,16 @@ std::string Batch::create(const std::vector<const Program*>& circuits, int preci
                 w1++;
             } while (w1 < large.size() && (opt.window_bytes == 0 ||
                                            bytes + (1ull << packs[large[w1]].n_sim) * S->amp_bytes() <= opt.window_bytes));
-            std::vector<int> need(large.size(), 0);
             size_t maxlev = 0;
             for (size_t k = w0; k < w1; k++) maxlev = std::max(maxlev, packs[large[k]].progs.size() + 1);
             for (size_t lev = 0; lev < maxlev; lev++)
                 for (size_t k = w0; k < w1; k++) {
                     const int ci = large[k];
                     const CircPack& P = packs[ci];
-                    const size_t np = P.progs.size();
-                    if (lev > np) continue;
+                    const size_t nprog = P.progs.size();
+                    if (lev > nprog) continue;
                     const int before = need[k];
-                    if (lev < np) {
+                    if (lev < nprog) {
                         const uint32_t ncos = 1u << (P.n_sim - KATE_TILE_BITS);
                         // Small states: fewer cosets per task, so a level spreads over several CTAs.
                         const uint32_t cch = std::max<uint32_t>(1, std::min<uint32_t>(chunk, ncos / 16));
@@ -328,7 +407,7 @@ std::string Batch::create(const std::vector<const Program*>& circuits, int preci
                             t.c1 = std::min<uint32_t>(ncos, c0 + cch);
                             t.need = before;
                             t.first = lev == 0;
-                            ltasks.push_back(t);
+                            push_large(t);
                             need[k]++;
                         }
                     } else {
@@ -340,31 +419,18 @@ std::string Batch::create(const std::vector<const Program*>& circuits, int preci
                             t.c0 = c0;
                             t.c1 = std::min<uint32_t>(nch, c0 + zchunks);
                             t.need = before;
-                            ltasks.push_back(t);
+                            push_large(t);
                             need[k]++;
                         }
                     }
                 }
             w0 = w1;
         }
+        while (si < Sn) push_small();  // only when there are no large circuits
     }
-    {
-        const size_t L = ltasks.size(), Sn = small.size();
-        size_t li = 0;
-        for (size_t s = 0; s < Sn; s++) {
-            // Large tasks due before small task s.
-            const size_t upto = L * s / Sn;
-            while (li < upto) S->tasks.push_back(ltasks[li++]);
-            BatchTask t{};
-            t.kind = BT_SMALL;
-            t.circ = small[s];
-            t.prog = prog0[small[s]];
-            t.nprog = (int)packs[small[s]].progs.size();
-            S->tasks.push_back(t);
-        }
-        while (li < L) S->tasks.push_back(ltasks[li++]);
-    }
-    if (S->tasks.size() > (size_t)INT32_MAX) return fail("too many tasks");
+    if (li != L) return fail("internal: task count mismatch");
+    S->create_ms[1] = ms_since(t0);
+    t0 = clk::now();
 
     // Device side.
     cudaError_t ce = cudaSetDevice(device);
@@ -377,9 +443,10 @@ std::string Batch::create(const std::vector<const Program*>& circuits, int preci
     if ((e = S->upload(&S->d_progs, S->progs, "cudaMalloc(programs)")) != "") return fail(e);
     if ((e = S->upload(&S->d_sops, S->sops, "cudaMalloc(smem ops)")) != "") return fail(e);
     {
-        uint8_t* b = nullptr;
-        if ((e = S->upload(&b, S->blob, "cudaMalloc(program blob)")) != "") return fail(e);
-        S->d_blob = b;
+        ce = cudaMalloc(&S->d_blob, S->blob_bytes);
+        if (ce != cudaSuccess) return fail(cuda_err("cudaMalloc(program blob)", ce));
+        ce = cudaMemcpy(S->d_blob, S->blob.get(), S->blob_bytes, cudaMemcpyHostToDevice);
+        if (ce != cudaSuccess) return fail(cuda_err("cudaMemcpy(program blob)", ce));
         Cx* p = nullptr;
         if ((e = S->upload(&p, S->pool, "cudaMalloc(matrix pool)")) != "") return fail(e);
         S->d_pool = p;
@@ -396,8 +463,13 @@ std::string Batch::create(const std::vector<const Program*>& circuits, int preci
     if (ce != cudaSuccess) return fail(cuda_err("cudaMalloc(error flag)", ce));
     ce = cudaMemset(S->d_err, 0, sizeof(int));
     if (ce != cudaSuccess) return fail(cuda_err("cudaMemset(error flag)", ce));
+    S->upload_bytes = S->tasks.size() * sizeof(BatchTask) + S->circs.size() * sizeof(BatchCirc) +
+                      S->progs.size() * sizeof(BatchProg) + S->sops.size() * sizeof(DevOp) + S->blob_bytes +
+                      S->pool.size() * sizeof(Cx);
     S->grid = batch_grid(device, precision);
     const int grid = (int)std::min<size_t>((size_t)S->grid, S->tasks.size());
+    S->create_ms[2] = ms_since(t0);
+    t0 = clk::now();
 
     // One graph: reset queue, counters and outputs, then the kernel.
     ce = cudaStreamBeginCapture(S->stream, cudaStreamCaptureModeThreadLocal);
@@ -413,8 +485,9 @@ std::string Batch::create(const std::vector<const Program*>& circuits, int preci
     if (ce != cudaSuccess) return fail(cuda_err("cudaStreamEndCapture", ce));
     ce = cudaGraphInstantiate(&S->exec, S->graph, 0);
     if (ce != cudaSuccess) return fail(cuda_err("cudaGraphInstantiate", ce));
+    S->create_ms[3] = ms_since(t0);
     // Host copies are no longer needed.
-    std::vector<uint8_t>().swap(S->blob);
+    S->blob.reset();
     std::vector<Cx>().swap(S->pool);
     std::vector<DevOp>().swap(S->sops);
     auto* b = new Batch();
@@ -484,6 +557,10 @@ int64_t Batch::num_outputs() const { return d_->nout; }
 int64_t Batch::num_tasks() const { return (int64_t)d_->tasks.size(); }
 uint64_t Batch::arena_bytes() const { return d_->arena_amps * d_->amp_bytes(); }
 int Batch::grid() const { return d_->grid; }
+void Batch::create_times(double* ms4) const {
+    for (int k = 0; k < 4; k++) ms4[k] = d_->create_ms[k];
+}
+uint64_t Batch::upload_bytes() const { return d_->upload_bytes; }
 int64_t Batch::num_programs() const { return (int64_t)d_->progs.size(); }
 void Batch::circuit_info(int i, int* programs, int* resident_qubits) const {
     *programs = d_->cprogs[i];

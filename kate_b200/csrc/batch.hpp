@@ -70,6 +70,10 @@ public:
     uint64_t arena_bytes() const;
     int grid() const;
     int64_t num_programs() const;
+    // Host wall time of create() in ms: planning, assembly of the task queue,
+    // device buffers and uploads, graph capture and instantiation.
+    void create_times(double* ms4) const;
+    uint64_t upload_bytes() const;  // host-to-device bytes copied by create()
     // Per circuit: pass programs and qubits simulated (0 for circuits run in shared memory).
     void circuit_info(int i, int* programs, int* resident_qubits) const;
 

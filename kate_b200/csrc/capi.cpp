@@ -741,6 +741,18 @@ kate_status kate_batch_info(const kate_batch* b, long long* info) {
     return KATE_OK;
 }
 
+kate_status kate_batch_create_times(const kate_batch* b, double* ms) {
+    REQUIRE(b && ms, "null pointer");
+    b->b->create_times(ms);
+    return KATE_OK;
+}
+
+kate_status kate_batch_upload_bytes(const kate_batch* b, long long* bytes) {
+    REQUIRE(b && bytes, "null pointer");
+    *bytes = (long long)b->b->upload_bytes();
+    return KATE_OK;
+}
+
 kate_status kate_batch_circuit_info(const kate_batch* b, int* programs, int* resident_qubits) {
     REQUIRE(b && programs && resident_qubits, "null pointer");
     for (int i = 0; i < b->ncirc; i++) b->b->circuit_info(i, programs + i, resident_qubits + i);
