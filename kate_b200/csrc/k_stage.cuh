@@ -296,6 +296,82 @@ __device__ __forceinline__ void setup_io(TileTables<C2>& T, const ProgView& P, u
     T.tls[t] = ops::tsw<C2>(t << E) << SH;
 }
 
+// Direct global I/O of the first and the last register stage (complex128):
+// the first stage loads its registers straight from global memory and the
+// last stores them straight back, instead of copying the tile through
+// shared memory (a 16-byte store and load per amplitude each way). Usable
+// when the stage's thread bits 0..3 address physical bits 0..3 (every warp
+// access then still covers runs of 256 contiguous bytes) and no
+// shared-memory op comes before (after) that stage.
+//   ml / mh  physical offset, in amplitudes, of the low / high 6 bits of a
+//            tile slot (swizzled byte offset >> 4) as the tile is read;
+//   sl / sh  the same as the tile is written back (qubit remap applied);
+//   lr / sr  offset of register j in the first / last stage.
+// Every map is linear over GF(2), so offsets of XOR-combined slots XOR.
+struct DirectIO {
+    uint64_t ml[64], mh[64], sl[64], sh[64];
+    uint64_t lr[16], sr[16];
+    int okL, okS;
+};
+
+// Physical offset of tile slot x (byte offset >> 4 in the complex128
+// layout) when tile bit k sits at physical bit pos[k].
+__device__ __forceinline__ uint64_t slot_phys(uint32_t x, const uint8_t* pos) {
+    const uint32_t e = ops::swz(x);
+    uint64_t o = 0;
+    for (int k = 0; k < TB; k++)
+        if ((e >> k) & 1u) o |= 1ull << pos[k];
+    return o;
+}
+
+// Builds D from the program (no barrier needed before; one after).
+__device__ __forceinline__ void setup_direct(DirectIO& D, const ProgView& P, uint32_t t) {
+    uint8_t in[TB], out[TB];
+    for (int k = 0; k < TB; k++) in[k] = P.tphys[k], out[k] = P.tphys[k];
+    for (int i = 0; i < TB; i++) out[P.outsrc[i]] = P.tphys[i];
+    if (t < 64) D.ml[t] = slot_phys(t, in);
+    else if (t < 128) D.mh[t - 64] = slot_phys((t - 64) << 6, in);
+    else if (t < 192) D.sl[t - 128] = slot_phys(t - 128, out);
+    else D.sh[t - 192] = slot_phys((t - 192) << 6, out);
+    int first = -1, last = -1, smem_before = 0, smem_after = 0;
+    for (int k = 0; k < P.nops; k++) {
+        const int kind = P.ops[k].kind;
+        if (kind == SOP_STAGE) {
+            if (first < 0) first = P.ops[k].idx;
+            last = P.ops[k].idx;
+            smem_after = 0;
+        } else if (kind == SOP_SMEM) {
+            if (first < 0) smem_before = 1;
+            smem_after = 1;
+        }
+    }
+    if (t < 32) {
+        const bool ld = t < 16;
+        const int st = ld ? first : last;
+        uint32_t w = 0;
+        if (st >= 0)
+            for (int i = 0; i < 4; i++)
+                if (((t & 15u) >> i) & 1u) w ^= P.stab[st][(ld ? 32 : 36) + i];
+        (ld ? D.lr : D.sr)[t & 15u] = st >= 0 ? slot_phys(w >> 4, ld ? in : out) : 0;
+    }
+    if (t == 0) {
+        // Lanes 0..15 of a warp differ in thread bits 0..3: their slots
+        // differ by stab[st][1 << b] ^ stab[st][0].
+        auto lanes_ok = [&](int st, const uint8_t* pos) {
+            if (st < 0) return false;
+            uint64_t acc = 0;
+            for (int b = 0; b < 4; b++) {
+                const uint64_t d = slot_phys((uint32_t)(P.stab[st][1 << b] ^ P.stab[st][0]) >> 4, pos);
+                if (d == 0 || (d & (d - 1)) != 0) return false;
+                acc |= d;
+            }
+            return acc == 15;
+        };
+        D.okL = !smem_before && lanes_ok(first, in);
+        D.okS = !smem_after && lanes_ok(last, out);
+    }
+}
+
 template <typename C2>
 __device__ __forceinline__ uint64_t coset_base(const TileTables<C2>& T, uint32_t c) {
     return T.cb[0][c & 255u] | T.cb[1][(c >> 8) & 255u] | T.cb[2][c >> 16];
@@ -363,14 +439,19 @@ __device__ __forceinline__ void store_tile(const TileTables<C2>& T, C2* __restri
 // Runs the program in T on the tile at shared address tb (generic pointer
 // tile), for coset base cbase. Ends with the last stage's registers stored;
 // no trailing barrier. SM: whether the program may hold shared-memory ops.
+// D (complex128 only, may be null): with D->okL the first stage loads from
+// the state gst at coset base cbase, with D->okS the last stage stores there
+// (DirectIO); the caller then skips the tile copy in or out.
 template <typename C2, bool SM, int MAXK = 5>
 __device__ __forceinline__ void run_program(const TileTables<C2>& T, int nops, uint32_t tb, C2* tile, uint64_t cbase,
                                             const DevOp* __restrict__ sops, int sop0,
-                                            const double2* __restrict__ pool, uint32_t t) {
+                                            const double2* __restrict__ pool, uint32_t t,
+                                            const DirectIO* D = nullptr, C2* __restrict__ gst = nullptr) {
     using A = Amp<C2>;
     using R = typename A::R;
     C2 a[16];
     bool open = false;
+    bool started = false;  // a stage has been loaded
     uint32_t s0s = 0;    // store offset base of the open stage (flipped by SOP_XF)
     uint32_t lflip = 0;  // load offset flips for the next stage (SOP_XL)
     int si = 0;          // open stage's table
@@ -385,14 +466,30 @@ __device__ __forceinline__ void run_program(const TileTables<C2>& T, int nops, u
         switch (op.kind) {
         case SOP_STAGE: {
             if (open) store_regs();
-            __syncthreads();
             si = op.idx;
             const uint16_t* tab = T.stab[si];
             const uint32_t s0 = (uint32_t)tab[t & 15u] ^ (uint32_t)tab[16 + (t >> 4)];
-            const uint32_t w0 = tab[32], w1 = tab[33], w2 = tab[34], w3 = tab[35];
             const uint32_t sl = s0 ^ lflip;
+            if constexpr (sizeof(C2) == 16) {
+                if (D != nullptr && !started && D->okL) {
+                    // Register and thread vectors may share tile bits (folded
+                    // CNOTs), so offsets combine by XOR, never by addition.
+                    const uint32_t x = sl >> 4;
+                    const uint64_t base = cbase ^ D->ml[x & 63u] ^ D->mh[x >> 6];
+#pragma unroll
+                    for (int j = 0; j < 16; j++) a[j] = __ldcg(gst + (base ^ D->lr[j]));
+                    started = true;
+                    s0s = s0;
+                    lflip = 0;
+                    open = true;
+                    break;
+                }
+            }
+            __syncthreads();
+            const uint32_t w0 = tab[32], w1 = tab[33], w2 = tab[34], w3 = tab[35];
 #pragma unroll
             for (int j = 0; j < 16; j++) a[j] = A::lds(tb + reg_off(j, sl, w0, w1, w2, w3));
+            started = true;
             s0s = s0;
             lflip = 0;
             open = true;
@@ -507,7 +604,18 @@ __device__ __forceinline__ void run_program(const TileTables<C2>& T, int nops, u
             break;
         }
     }
-    if (open) store_regs();
+    if (open) {
+        if constexpr (sizeof(C2) == 16) {
+            if (D != nullptr && D->okS) {
+                const uint32_t x = s0s >> 4;
+                const uint64_t base = cbase ^ D->sl[x & 63u] ^ D->sh[x >> 6];
+#pragma unroll
+                for (int j = 0; j < 16; j++) gst[base ^ D->sr[j]] = a[j];
+                return;
+            }
+        }
+        store_regs();
+    }
 }
 
 }  // namespace

@@ -29,9 +29,16 @@ namespace {
 
 using namespace stage;
 
+// Complex128 with one buffer also keeps the DirectIO tables (first-stage
+// loads and last-stage stores straight to global memory).
+template <typename C2, int NBUF>
+constexpr bool tile_direct() {
+    return sizeof(C2) == 16 && NBUF == 1;
+}
+
 template <typename C2, int NBUF>
 constexpr size_t tile_smem_bytes() {
-    return (size_t)NBUF * TS * sizeof(C2) + sizeof(TileTables<C2>);
+    return (size_t)NBUF * TS * sizeof(C2) + sizeof(TileTables<C2>) + (tile_direct<C2, NBUF>() ? sizeof(DirectIO) : 0);
 }
 
 // SM: whether the program has shared-memory ops (the variant without them
@@ -48,11 +55,13 @@ __global__ void __launch_bounds__(NT, NBUF == 1 ? 2 : 1)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C2* bufs = reinterpret_cast<C2*>(smem_raw);
     TileTables<C2>& T = *reinterpret_cast<TileTables<C2>*>(bufs + NBUF * TS);
+    DirectIO* D = tile_direct<C2, NBUF>() ? reinterpret_cast<DirectIO*>(&T + 1) : nullptr;
     const uint32_t t = threadIdx.x;
     {
         const ProgView v = view(P);
         setup_program(T, v, t);
         setup_io(T, v, t);
+        if constexpr (tile_direct<C2, NBUF>()) setup_direct(*D, v, t);
     }
     const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(bufs);
     __syncthreads();
@@ -73,6 +82,10 @@ __global__ void __launch_bounds__(NT, NBUF == 1 ? 2 : 1)
             else asm volatile("cp.async.commit_group;\n" ::: "memory");
         }
     }
+    // Tile copies through shared memory unless the first (last) stage reads
+    // (writes) global memory itself.
+    const bool copy_in = !tile_direct<C2, NBUF>() || !D->okL;
+    const bool copy_out = !tile_direct<C2, NBUF>() || !D->okS;
     int it = 0;
     for (uint32_t c = c_begin; c < c_end; c += c_step, it++) {
         const int slot = NBUF == 1 ? 0 : it % NBUF;
@@ -85,15 +98,17 @@ __global__ void __launch_bounds__(NT, NBUF == 1 ? 2 : 1)
             if (cn < c_end) load_async(T, st, cn, sbase + (uint32_t)((it + NBUF - 1) % NBUF) * BUF_BYTES, t);
             else asm volatile("cp.async.commit_group;\n" ::: "memory");
             asm volatile("cp.async.wait_group %0;\n" ::"n"(NBUF - 1) : "memory");
-        } else {
+        } else if (copy_in) {
             load_async(T, st, c, sbase, t);
             asm volatile("cp.async.wait_group 0;\n" ::: "memory");
         }
-        __syncthreads();
-        run_program<C2, SM>(T, nops, tb, tile, coset_base(T, c), sops, sop0, pool, t);
-        __syncthreads();
-        store_tile<C2, false>(T, st, c, tb, t);
-        // The buffer is refilled by a later load.
+        if (copy_in) __syncthreads();
+        run_program<C2, SM>(T, nops, tb, tile, coset_base(T, c), sops, sop0, pool, t, D, st);
+        if (copy_out) {
+            __syncthreads();
+            store_tile<C2, false>(T, st, c, tb, t);
+        }
+        // The buffer is rewritten by the next coset.
         __syncthreads();
     }
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
