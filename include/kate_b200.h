@@ -298,6 +298,9 @@ typedef struct {
     int zchunks;               /* 65536-amplitude chunks per <Z> task; 0: default */
     unsigned long long window_bytes; /* queue large circuits in windows of this many state bytes; 0: one window */
     kate_batch_tuning tune[KATE_BATCH_MAX_QUBITS + 1]; /* by qubit count */
+    int wait_ms;               /* a dependency wait in the kernel gives up after this long; 0: 5000 */
+    long long fault_task;      /* test hook, 1-based: that task waits for a count never reached, so the
+                                  bounded wait runs out and kate_batch_synchronize reports it; 0: none */
 } kate_batch_options;
 
 /* Defaults (no window, default tuning for every qubit count). */

@@ -107,7 +107,8 @@ class BatchTuning(_c.Structure):
 class BatchOptions(_c.Structure):
     """kate_batch_options (include/kate_b200.h)."""
     _fields_ = [("chunk", _c.c_int), ("zchunks", _c.c_int), ("window_bytes", _c.c_ulonglong),
-                ("tune", BatchTuning * (KATE_BATCH_MAX_QUBITS + 1))]
+                ("tune", BatchTuning * (KATE_BATCH_MAX_QUBITS + 1)), ("wait_ms", _c.c_int),
+                ("fault_task", _c.c_longlong)]
 _RET = {"kate_last_error": _c.c_char_p, "kate_version": _c.c_char_p}
 
 

@@ -199,6 +199,7 @@ struct BatchImpl {
     cudaGraphExec_t exec = nullptr;
     double create_ms[4] = {0, 0, 0, 0};  // planning, assembly, device buffers + uploads, graph
     uint64_t upload_bytes = 0;           // host-to-device bytes copied by create()
+    uint64_t wait_ns = 5000000000ull;    // a dependency wait in the kernel gives up after this long
 
     size_t amp_bytes() const { return precision == 0 ? 16 : 8; }
 
@@ -429,6 +430,10 @@ std::string Batch::create(const std::vector<const Program*>& circuits, int preci
         while (si < Sn) push_small();  // only when there are no large circuits
     }
     if (li != L) return fail("internal: task count mismatch");
+    // Test hook: one task waits for a count its circuit never reaches, so the
+    // kernel's bounded wait runs out (the failure is made on the host).
+    if (opt.fault_task >= 0 && (size_t)opt.fault_task < S->tasks.size()) S->tasks[opt.fault_task].need = INT32_MAX;
+    S->wait_ns = 1000000ull * (uint64_t)std::max(1, opt.wait_ms);
     S->create_ms[1] = ms_since(t0);
     t0 = clk::now();
 
@@ -479,7 +484,7 @@ std::string Batch::create(const std::vector<const Program*>& circuits, int preci
     cudaMemsetAsync(S->d_zout, 0, sizeof(double) * std::max<int64_t>(1, S->nout), S->stream);
     cudaError_t le = launch_batch(S->d_arena, precision, S->d_tasks, (int)S->tasks.size(), S->d_circs, S->d_progs,
                                   S->d_blob, S->d_sops, S->d_pool, S->d_head, S->d_done, S->d_zout, S->d_err, grid,
-                                  S->stream);
+                                  S->stream, nullptr, nullptr, nullptr, S->wait_ns);
     ce = cudaStreamEndCapture(S->stream, &S->graph);
     if (le != cudaSuccess) return fail(cuda_err("launch_batch", le));
     if (ce != cudaSuccess) return fail(cuda_err("cudaStreamEndCapture", ce));

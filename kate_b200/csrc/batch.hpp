@@ -30,6 +30,8 @@ struct BatchOptions {
     int zchunks = 4;              // 2^16-amplitude chunks per ZRED task
     uint64_t window_bytes = 0;    // queue large circuits in windows of this many state bytes (0: one window)
     std::vector<BatchTune> tune;  // by qubit count (index n); missing entries use the defaults
+    int wait_ms = 5000;           // a dependency wait in the kernel gives up after this long
+    int64_t fault_task = -1;      // test hook: this task waits for a count its circuit never reaches
     const BatchTune& for_n(int n) const;
 };
 

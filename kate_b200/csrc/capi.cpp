@@ -624,6 +624,8 @@ kate::BatchOptions to_options(const kate_batch_options* o) {
     if (o->chunk > 0) r.chunk = o->chunk;
     if (o->zchunks > 0) r.zchunks = o->zchunks;
     r.window_bytes = o->window_bytes;
+    if (o->wait_ms > 0) r.wait_ms = o->wait_ms;
+    r.fault_task = o->fault_task > 0 ? o->fault_task - 1 : -1;
     r.tune.resize(KATE_BATCH_MAX_QUBITS + 1);
     for (int n = 0; n <= KATE_BATCH_MAX_QUBITS; n++) {
         r.tune[n].fusion = o->tune[n].fusion;
@@ -645,6 +647,7 @@ kate_status kate_batch_options_default(kate_batch_options* opt) {
     kate::BatchOptions d;
     opt->chunk = d.chunk;
     opt->zchunks = d.zchunks;
+    opt->wait_ms = d.wait_ms;
     return KATE_OK;
 }
 

@@ -33,7 +33,6 @@ namespace {
 
 using namespace stage;
 
-constexpr unsigned long long WAIT_NS = 5000000000ull;  // a dependency wait gives up after 5 s
 
 __device__ __forceinline__ unsigned long long now_ns() {
     unsigned long long v;
@@ -315,7 +314,7 @@ __global__ void __launch_bounds__(NT, sizeof(C2) == 8 ? 2 : 1)
             const BatchProg* __restrict__ progs, const unsigned char* __restrict__ blob, const DevOp* __restrict__ sops,
             const double2* __restrict__ pool, int* __restrict__ head, int* __restrict__ done,
             double* __restrict__ zout, int* __restrict__ err, double* __restrict__ psum,
-            const double* __restrict__ unif, uint64_t* __restrict__ sout) {
+            const double* __restrict__ unif, uint64_t* __restrict__ sout, unsigned long long wait_ns) {
     // Two tile buffers (a pass task prefetches its next coset into the
     // other one), then the program tables.
     C2* tile = reinterpret_cast<C2*>(batch_smem_raw);
@@ -340,7 +339,7 @@ __global__ void __launch_bounds__(NT, sizeof(C2) == 8 ? 2 : 1)
         if (t == 0 && K.need > 0) {
             const unsigned long long t0 = now_ns();
             while (*((volatile int*)(done + K.circ)) < K.need) {
-                if (now_ns() - t0 > WAIT_NS || *((volatile int*)err)) {
+                if (now_ns() - t0 > wait_ns || *((volatile int*)err)) {
                     s_abort = 1;
                     atomicExch(err, 1);
                     break;
@@ -453,15 +452,15 @@ int batch_grid(int device, int prec) {
 cudaError_t launch_batch(void* arena, int prec, const BatchTask* tasks, int ntasks, const BatchCirc* circs,
                          const BatchProg* progs, const void* blob, const DevOp* sops, const void* pool, int* head,
                          int* done, double* zout, int* err, int grid, cudaStream_t s, double* psum,
-                         const double* unif, uint64_t* sout) {
+                         const double* unif, uint64_t* sout, unsigned long long wait_ns) {
     const unsigned char* b = (const unsigned char*)blob;
     const double2* pl = (const double2*)pool;
     if (prec == 1)
         k_batch<float2><<<grid, NT, batch_smem<float2>(), s>>>((float2*)arena, tasks, ntasks, circs, progs, b, sops, pl,
-                                                               head, done, zout, err, psum, unif, sout);
+                                                               head, done, zout, err, psum, unif, sout, wait_ns);
     else
         k_batch<double2><<<grid, NT, batch_smem<double2>(), s>>>((double2*)arena, tasks, ntasks, circs, progs, b, sops,
-                                                                 pl, head, done, zout, err, psum, unif, sout);
+                                                                 pl, head, done, zout, err, psum, unif, sout, wait_ns);
     return cudaGetLastError();
 }
 

@@ -44,12 +44,14 @@ int block_c64_grid(int n, int device);
 
 // Persistent batch kernel (k_batch.cu). head, done[circuits], zout (large
 // circuits' outputs) must be zero at launch; err is set to 1 when a
-// dependency wait gave up (the kernel then stops). psum / unif / sout: chunk
-// sums, uniforms and samples of circuits that sample (may be null otherwise).
+// dependency wait gave up after wait_ns (the kernel then stops). psum /
+// unif / sout: chunk sums, uniforms and samples of circuits that sample (may
+// be null otherwise).
 cudaError_t launch_batch(void* arena, int prec, const BatchTask* tasks, int ntasks, const BatchCirc* circs,
                          const BatchProg* progs, const void* blob, const DevOp* sops, const void* pool, int* head,
                          int* done, double* zout, int* err, int grid, cudaStream_t s, double* psum = nullptr,
-                         const double* unif = nullptr, uint64_t* sout = nullptr);
+                         const double* unif = nullptr, uint64_t* sout = nullptr,
+                         unsigned long long wait_ns = 5000000000ull);
 int batch_grid(int device, int prec);
 
 // Bit sums: per CTA, for every local bit, the sum over amplitudes with the

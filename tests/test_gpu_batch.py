@@ -106,3 +106,29 @@ def test_hea_batch_of_many_circuits(oracle):
     for i in range(0, len(specs), 37):
         n, g = specs[i]
         assert np.abs(got[i] - zexp(n, oracle.simulate(n, g))).max() <= 2e-5
+
+
+def test_dependency_wait_runs_out_and_reports(oracle):
+    """A task made (on the host) to wait for a count its circuit never
+    reaches: the kernel's bounded wait gives up after wait_ms, every CTA stops
+    at its next task, the run reports the timeout, and the device stays
+    usable for the next batch."""
+    specs = [(14, circuits.hea(14, 8, seed=3)), (16, circuits.hea(16, 8, seed=4)), (10, circuits.hea(10, 4, seed=5))]
+    circs = [K.Circuit(n, g) for n, g in specs]
+    o = _lib.BatchOptions()
+    K._lib.lib().kate_batch_options_default(ctypes_ref(o))
+    o.wait_ms = 200
+    b = K.Batch(circs, precision=K.C64, options=o)
+    ntasks = b.info()["tasks"]
+    b.close()
+    o.fault_task = ntasks  # 1-based: the last task, a <Z> reduction that waits on the passes
+    bad = K.Batch(circs, precision=K.C64, options=o)
+    with pytest.raises(K.KateError, match="timed out"):
+        bad.run()
+    bad.close()
+    o.fault_task = 0
+    good = K.Batch(circs, precision=K.C64, options=o)
+    good.run()
+    for (n, g), z in zip(specs, good.expect_z()):
+        assert np.abs(z - zexp(n, oracle.simulate(n, g))).max() <= 2e-5
+    good.close()
