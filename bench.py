@@ -371,7 +371,14 @@ def main():
         e2e_ms = max_over_ranks(e2e_ms, dev)
     n_ops = sum(ng for _, ng in passes)
     h2d = n_ops * 112 + 16 * (4 ** 1) * n_ops + 2 * n * 8
-    d2h = 2 * n * 8 + 16 * (1 + 2 * (12 + 4)) * (1 << 14)
+    # proba_state: per-CTA partial sums of the bit-sum kernel (2^g CTAs,
+    # 1 + 2 (12 + r) complex sums each, g = min(n - 12, 10), r = the rest up
+    # to 8), then the (theta, phi) pairs.
+    g_bits = min(n - 12, 10)
+    r_bits = n - 12 - g_bits
+    if r_bits > 8:
+        g_bits, r_bits = n - 12 - 8, 8
+    d2h = 2 * n * 8 + 16 * (1 + 2 * (12 + r_bits)) * (1 << g_bits)
 
     ref_gpu = None
     if rank == 0 and world == 1 and not args.no_ref_gpu:

@@ -80,6 +80,36 @@ __global__ void k_init_product(A* __restrict__ st, int n, const ProductInit P) {
     }
 }
 
+// The same product state for n >= 10 in one write pass: amplitude
+// (c << 10) | i is L[i] * H(c), L the products of the low 10 qubits' factors
+// (a shared table built once per CTA) and H the product of the high ones
+// (per 1024-amplitude chunk, the same for the whole block, so its factor
+// loads are uniform). The product is taken in another order than the
+// reference's left-to-right one: the amplitudes agree to a few ulp.
+template <typename A>
+__global__ void __launch_bounds__(256) k_init_product_split(A* __restrict__ st, int n, const ProductInit P) {
+    __shared__ double2 L[1024];
+    for (int i = threadIdx.x; i < 1024; i += blockDim.x) {
+        double2 v = make_double2(1.0, 0.0);
+        for (int j = 0; j < 10; j++) {
+            const int b = (i >> j) & 1;
+            v = cmul(v, make_double2(P.v[b][j][0], P.v[b][j][1]));
+        }
+        L[i] = v;
+    }
+    __syncthreads();
+    const uint64_t nchunks = 1ull << (n - 10);
+    for (uint64_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
+        double2 h = make_double2(1.0, 0.0);
+        for (int j = 10; j < n; j++) {
+            const int b = (int)((c >> (j - 10)) & 1ull);
+            h = cmul(h, make_double2(P.v[b][j][0], P.v[b][j][1]));
+        }
+        A* dst = st + (c << 10);
+        for (int i = threadIdx.x; i < 1024; i += blockDim.x) narrow(dst + i, cmul(L[i], h));
+    }
+}
+
 }  // namespace
 
 cudaError_t launch_set_basis0(void* st, uint64_t dim, int prec, cudaStream_t s) {
@@ -93,6 +123,13 @@ cudaError_t launch_set_basis0(void* st, uint64_t dim, int prec, cudaStream_t s) 
 cudaError_t launch_set_basis0_c128(void* st, uint64_t dim, cudaStream_t s) { return launch_set_basis0(st, dim, 0, s); }
 
 cudaError_t launch_init_product(void* st, int n, const ProductInit& P, int prec, cudaStream_t s) {
+    if (n >= 10) {
+        const uint64_t nchunks = 1ull << (n - 10);
+        const unsigned blocks = (unsigned)(nchunks < 148 * 8 ? nchunks : 148 * 8);
+        if (prec == 0) k_init_product_split<double2><<<blocks, 256, 0, s>>>((double2*)st, n, P);
+        else k_init_product_split<float2><<<blocks, 256, 0, s>>>((float2*)st, n, P);
+        return cudaGetLastError();
+    }
     uint64_t dim = 1ull << n;
     uint64_t blocks = (dim + 255) / 256;
     if (blocks > 148 * 16) blocks = 148 * 16;

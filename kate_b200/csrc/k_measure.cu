@@ -158,8 +158,14 @@ BitSumShape bitsum_shape(int n) {
         s.g = 0;
         s.nr = 0;
     } else {
-        s.g = n - 12 < 14 ? n - 12 : 14;
+        // About a thousand CTAs (seven per SM), each summing up to 2^MAXR
+        // rounds in registers: few partials to add on the host.
+        s.g = n - 12 < 10 ? n - 12 : 10;
         s.nr = n - 12 - s.g;
+        if (s.nr > MAXR) {
+            s.nr = MAXR;
+            s.g = n - 12 - MAXR;
+        }
     }
     s.grid = 1 << s.g;
     s.nout = 1 + 2 * (12 + s.nr);
