@@ -276,6 +276,19 @@ KATE_API kate_status kate_plan_final_layout(const kate_plan* p, int* phys, int* 
 KATE_API kate_status kate_proba_state_noalloc(const void* d_state, int nqbits, const int* phys_of_label,
                                               const int* final_inverse_permutation, double* theta_phi, void* stream);
 
+/* ---- device memory held for reuse ----
+ * No counterpart in the reference, which allocates the state in every
+ * Simulator constructor and frees it in the destructor
+ * (HIPcode/simulator.hpp:243-300, 407-425). Here a destroyed simulator's
+ * state (and a destroyed batch's arena), if at least 64 MiB, stays allocated
+ * and is reused by the next simulator or batch on that device that it covers
+ * (up to 4x its size), which saves the cudaMalloc / cudaFree of the whole
+ * state in a loop of Simulator(circuit).execute(). At most one such buffer
+ * is held per device; kate_server_create frees it before taking its budget.
+ * This call frees it (device -1: on every device), e.g. before handing the
+ * memory to another library. */
+KATE_API kate_status kate_release_cached_memory(int device);
+
 /* ---- batches of independent circuits ----
  * Replaces a caller's loop of `Simulator(circuit).execute()` over many
  * independent circuits (CPUcode/simulator.hpp:120-200 per circuit; the GPU

@@ -268,6 +268,12 @@ class Circuit:
         return Gate(d[: 2 * dim * dim].view(np.complex128).reshape(dim, dim).copy(), [int(x) for x in q[: k.value]])
 
 
+def release_cached_memory(device: int = -1):
+    """Frees the device buffer kept for reuse after a simulator or batch was
+    destroyed (kate_release_cached_memory); device -1: every device."""
+    _check(_lib.lib().kate_release_cached_memory(int(device)))
+
+
 def mergeGate(gates: Sequence[Gate]) -> Gate:
     """CPUmergeGate / mergeGate (CPUcode/GateMerger.hpp:8-55): FP64 product
     of the gates on the sorted union of their qubits."""
@@ -384,7 +390,7 @@ class Simulator:
         return out
 
 
-__all__ = ["Gate", "Circuit", "Simulator", "mergeGate", "proba_state", "KateError", "Hadamard", "CNOT", "CRk",
+__all__ = ["Gate", "Circuit", "Simulator", "mergeGate", "release_cached_memory", "proba_state", "KateError", "Hadamard", "CNOT", "CRk",
            "TOFFOLI", "RX", "RZ", "DENSE", "C128", "C64"]
 
 

@@ -87,6 +87,7 @@ SIGNATURES = {
     "kate_batch_time": [_vp, _i, _c.POINTER(_c.c_float)],
     "kate_batch_circuit_info": [_vp, _ip, _ip],
     "kate_batch_create_times": [_vp, _dp],
+    "kate_release_cached_memory": [_i],
     "kate_batch_upload_bytes": [_vp, _c.POINTER(_c.c_longlong)],
     "kate_server_options_default": [_vp],
     "kate_server_create": [_i, _i, _vp, _vpp],

@@ -11,6 +11,7 @@
 #include <memory>
 #include <thread>
 
+#include "devcache.hpp"
 #include "launch.hpp"
 #include "plan.hpp"
 
@@ -208,7 +209,7 @@ struct BatchImpl {
         if (stream) cudaStreamSynchronize(stream);
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
-        cudaFree(d_arena);
+        cached_free(d_arena, device);
         cudaFree(d_tasks);
         cudaFree(d_circs);
         cudaFree(d_progs);
@@ -456,7 +457,7 @@ std::string Batch::create(const std::vector<const Program*>& circuits, int preci
         if ((e = S->upload(&p, S->pool, "cudaMalloc(matrix pool)")) != "") return fail(e);
         S->d_pool = p;
     }
-    ce = cudaMalloc(&S->d_arena, std::max<uint64_t>(16, S->arena_amps * S->amp_bytes()));
+    ce = cached_malloc(&S->d_arena, std::max<uint64_t>(16, S->arena_amps * S->amp_bytes()), device);
     if (ce != cudaSuccess) return fail(cuda_err("cudaMalloc(state arena)", ce));
     ce = cudaMalloc((void**)&S->d_head, sizeof(int));
     if (ce != cudaSuccess) return fail(cuda_err("cudaMalloc(queue head)", ce));

@@ -26,7 +26,7 @@ struct BatchTune {
 };
 
 struct BatchOptions {
-    int chunk = 4;                // cosets per PASS task
+    int chunk = 16;               // cosets per PASS task (at most 1/16 of a circuit's cosets)
     int zchunks = 4;              // 2^16-amplitude chunks per ZRED task
     uint64_t window_bytes = 0;    // queue large circuits in windows of this many state bytes (0: one window)
     std::vector<BatchTune> tune;  // by qubit count (index n); missing entries use the defaults

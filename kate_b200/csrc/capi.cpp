@@ -1,4 +1,5 @@
 // C ABI (include/kate_b200.h) over the C++ circuit, passes and simulator.
+#include "devcache.hpp"
 #include "kate_b200.h"
 
 #include <cstring>
@@ -640,6 +641,13 @@ std::vector<const kate::Program*> programs(const kate_circuit* const* c, int cou
     return v;
 }
 }  // namespace
+
+kate_status kate_release_cached_memory(int device) {
+    return guarded([&] {
+        kate::release_cached(device);
+        return KATE_OK;
+    });
+}
 
 kate_status kate_batch_options_default(kate_batch_options* opt) {
     REQUIRE(opt, "null pointer");

@@ -15,6 +15,7 @@
 #include <thread>
 #include <unordered_map>
 
+#include "devcache.hpp"
 #include "launch.hpp"
 
 namespace kate {
@@ -720,6 +721,7 @@ std::string Server::create(int precision, int device, const ServeOptions& opt, S
     const uint64_t minb = (1ull << KATE_TILE_BITS) * S->amp_bytes();
     const uint64_t budget = opt.budget_bytes / minb * minb;
     if (budget < minb) return fail("admission budget below one 12-qubit state");
+    release_cached(device);  // the budget is one allocation: no simulator state held back for reuse
     ce = cudaMalloc(&S->d_state, budget);
     if (ce != cudaSuccess) return fail(cuda_err("cudaMalloc(state arena)", ce));
     ce = cudaMalloc((void**)&S->d_aux, opt.aux_bytes);

@@ -10,6 +10,7 @@
 #include <numeric>
 #include <random>
 
+#include "devcache.hpp"
 #include "launch.hpp"
 
 namespace kate {
@@ -180,7 +181,7 @@ std::string Simulator::create(const Program& prog_in, int precision, int device,
     impl->part_bytes = (size_t)sh.grid * sh.nout * 2 * sizeof(double);
     ce = cudaMalloc(&impl->d_part, impl->part_bytes);
     if (ce != cudaSuccess) return fail(cuda_err("cudaMalloc(partials)", ce));
-    ce = cudaMalloc(&impl->d_state, impl->dim() * impl->amp_bytes());
+    ce = cached_malloc(&impl->d_state, impl->dim() * impl->amp_bytes(), device);
     if (ce != cudaSuccess) return fail(cuda_err("cudaMalloc(state)", ce));
     impl->grid = generic_pass_grid(impl->n, std::min(impl->opt.max_tile, impl->n), device);
     if (const char* e = std::getenv("KATE_TILE_NBUF")) {
@@ -203,7 +204,7 @@ Simulator::~Simulator() {
     if (!d_) return;
     cudaSetDevice(d_->device);
     if (d_->stream) cudaStreamSynchronize(d_->stream);
-    cudaFree(d_->d_state);
+    cached_free(d_->d_state, d_->device);
     cudaFree(d_->d_ops);
     cudaFree(d_->d_sops);
     cudaFree(d_->d_pool);
