@@ -44,6 +44,15 @@ typedef struct {
 #define SOP_DR 10    // diagonal over the register bits: multiply register j by mats[idx + j]
 #define SOP_XF 11    // fold a NOT into the stage's store: store offset ^= idx where controls cthr/ccos are 1
 #define SOP_XL 12    // fold a NOT into the next stage's load: load offset ^= idx where controls cthr/ccos are 1
+// Rotations with a common factor taken out of the matrix (one FMA-class op
+// per real component of an amplitude instead of two). mats[idx] = (t0, t1);
+// the factors of a pass are multiplied together and applied once, folded
+// into one diagonal or full 2x2 op of the same pass (a scalar commutes with
+// every op). On register bit a, x0 / x1 the pair's amplitudes:
+#define SOP_URA 13   // x0' = x0 + t0 x1,     x1' = t1 x0 + x1      (real [[a, b], [c, a]] / a)
+#define SOP_URB 14   // x0' = t0 x0 + x1,     x1' = t1 x1 - x0      (real [[a, b], [-b, d]] / b)
+#define SOP_UXA 15   // x0' = x0 + i t0 x1,   x1' = x1 + i t1 x0    ([[a, ib], [ic, a]] / a)
+#define SOP_UXB 16   // x0' = x1 - i t0 x0,   x1' = x0 - i t1 x1    ([[a, ib], [ib, d]] / (ib))
 
 #define SRC_REG 0
 #define SRC_THR 1

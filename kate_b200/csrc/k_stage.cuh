@@ -168,6 +168,63 @@ __device__ __forceinline__ void reg_ux(C2 (&a)[16], R u00, R u01i, R u10i, R u11
     }
 }
 
+// Rotations with their common factor taken out (SOP_URA/URB/UXA/UXB): one
+// FMA-class op per real component (one packed FMA per complex64 amplitude).
+//   F = 0 (URA): x0 + t0 x1,    t1 x0 + x1
+//   F = 1 (URB): t0 x0 + x1,    t1 x1 - x0
+//   F = 2 (UXA): x0 + i t0 x1,  x1 + i t1 x0
+//   F = 3 (UXB): x1 - i t0 x0,  x0 - i t1 x1
+template <int F, int B, typename C2, typename R>
+__device__ __forceinline__ void reg_rot(C2 (&a)[16], R t0, R t1) {
+    using A = Amp<C2>;
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+        if ((j >> B) & 1) continue;
+        const int k = j | (1 << B);
+        const C2 x = a[j], y = a[k];
+        if constexpr (sizeof(C2) == 8) {
+            using Fp = Amp<float2>;
+            if constexpr (F == 0) {
+                a[j] = Fp::fma_s(t0, y, x);
+                a[k] = Fp::fma_s(t1, x, y);
+            } else if constexpr (F == 1) {
+                a[j] = Fp::fma_s(t0, x, y);
+                a[k] = Fp::fma_s(t1, y, make_float2(-x.x, -x.y));
+            } else if constexpr (F == 2) {
+                a[j] = Fp::fma_s(t0, Fp::rot(y), x);
+                a[k] = Fp::fma_s(t1, Fp::rot(x), y);
+            } else {
+                a[j] = Fp::fma_s(-t0, Fp::rot(x), y);
+                a[k] = Fp::fma_s(-t1, Fp::rot(y), x);
+            }
+        } else {
+            if constexpr (F == 0) {
+                a[j] = A::mk(A::fm(t0, y.x, x.x), A::fm(t0, y.y, x.y));
+                a[k] = A::mk(A::fm(t1, x.x, y.x), A::fm(t1, x.y, y.y));
+            } else if constexpr (F == 1) {
+                a[j] = A::mk(A::fm(t0, x.x, y.x), A::fm(t0, x.y, y.y));
+                a[k] = A::mk(A::fm(t1, y.x, -x.x), A::fm(t1, y.y, -x.y));
+            } else if constexpr (F == 2) {
+                a[j] = A::mk(A::fm(-t0, y.y, x.x), A::fm(t0, y.x, x.y));
+                a[k] = A::mk(A::fm(-t1, x.y, y.x), A::fm(t1, x.x, y.y));
+            } else {
+                a[j] = A::mk(A::fm(t0, x.y, y.x), A::fm(-t0, x.x, y.y));
+                a[k] = A::mk(A::fm(t1, y.y, x.x), A::fm(-t1, y.x, x.y));
+            }
+        }
+    }
+}
+
+template <int F, typename C2, typename R>
+__device__ __forceinline__ void reg_rot_bit(C2 (&a)[16], int b, R t0, R t1) {
+    switch (b) {
+    case 0: reg_rot<F, 0>(a, t0, t1); break;
+    case 1: reg_rot<F, 1>(a, t0, t1); break;
+    case 2: reg_rot<F, 2>(a, t0, t1); break;
+    default: reg_rot<F, 3>(a, t0, t1); break;
+    }
+}
+
 // Controlled NOT with a per-thread condition: selects, no branches.
 template <int B, typename C2>
 __device__ __forceinline__ void reg_xs(C2 (&a)[16], uint32_t creg, bool go) {
@@ -548,6 +605,18 @@ __device__ __forceinline__ void run_program(const TileTables<C2>& T, int nops, u
             case 2: reg_ux<2>(a, u00, u01, u10, u11); break;
             default: reg_ux<3>(a, u00, u01, u10, u11); break;
             }
+            break;
+        }
+        case SOP_URA:
+        case SOP_URB:
+        case SOP_UXA:
+        case SOP_UXB: {
+            const C2 tt = T.mats[op.idx];
+            const R t0 = tt.x, t1 = tt.y;
+            if (op.kind == SOP_URA) reg_rot_bit<0>(a, op.a, t0, t1);
+            else if (op.kind == SOP_URB) reg_rot_bit<1>(a, op.a, t0, t1);
+            else if (op.kind == SOP_UXA) reg_rot_bit<2>(a, op.a, t0, t1);
+            else reg_rot_bit<3>(a, op.a, t0, t1);
             break;
         }
         case SOP_H: {

@@ -9,6 +9,7 @@
 // through shared memory, so the scheduler first takes ready ops whose target
 // is already a register bit, then grows the register set (up to four bits),
 // and closes the stage only when neither is possible.
+#include <cmath>
 #include <algorithm>
 #include <cstring>
 
@@ -53,6 +54,68 @@ bool diag_factors(const std::vector<Cx>& table, int k, std::vector<Cx>* h) {
 }
 
 }  // namespace
+
+// Rewrites real and RX-form 2x2 ops whose matrix is a common factor f times
+// a matrix with a unit entry in each row (SOP_URA/URB/UXA/UXB), picking the
+// factor of larger magnitude so that |t0|, |t1| <= 1, and applies the
+// product F of the factors once: F multiplies the entries of the pass's
+// first diagonal (DR, D1) or general 2x2 (U) op, or, when the pass has none,
+// the first rewritten op goes back to a general 2x2 carrying F.
+void scale_rotations(std::vector<SOp>& ops, std::vector<Cx>& mats) {
+    Cx F(1.0, 0.0);
+    int first = -1;
+    std::vector<Cx> orig;  // matrix of the first rewritten op
+    for (size_t k = 0; k < ops.size(); k++) {
+        SOp& o = ops[k];
+        if (o.kind != SOP_UR && o.kind != SOP_UX) continue;
+        const Cx* m = &mats[o.idx];
+        double a, b, c, d;
+        const bool ux = o.kind == SOP_UX;
+        if (ux) {
+            a = m[0].re, b = m[1].im, c = m[2].im, d = m[3].re;
+        } else {
+            a = m[0].re, b = m[1].re, c = m[2].re, d = m[3].re;
+        }
+        const bool formA = a == d && a != 0.0;
+        const bool formB = b != 0.0 && (ux ? c == b : c == -b);
+        if (!formA && !formB) continue;
+        const bool useA = formA && (!formB || std::fabs(a) >= std::fabs(b));
+        if (first < 0) {
+            first = (int)k;
+            orig.assign(m, m + 4);
+        }
+        Cx f, t;
+        if (useA) {
+            f = Cx(a, 0.0);
+            t = Cx(b / a, c / a);
+            o.kind = ux ? SOP_UXA : SOP_URA;
+        } else {
+            f = ux ? Cx(0.0, b) : Cx(b, 0.0);
+            t = Cx(a / b, d / b);
+            o.kind = ux ? SOP_UXB : SOP_URB;
+        }
+        F = F * f;
+        // The op keeps its 4-entry slot; entry 0 holds (t0, t1), entry 1 the factor.
+        mats[o.idx] = t;
+        mats[o.idx + 1] = f;
+    }
+    if (first < 0) return;
+    for (SOp& o : ops) {
+        int cnt = o.kind == SOP_DR ? 16 : o.kind == SOP_D1 ? 2 : o.kind == SOP_U ? 4 : 0;
+        if (!cnt) continue;
+        for (int i = 0; i < cnt; i++) mats[o.idx + i] = mats[o.idx + i] * F;
+        return;
+    }
+    // No op to absorb F: the first rewritten op becomes a general 2x2 with
+    // its own factor replaced by F.
+    SOp& o = ops[first];
+    const Cx f = mats[o.idx + 1];
+    // G = F / f (f is real or purely imaginary and nonzero).
+    const double n2 = f.re * f.re + f.im * f.im;
+    const Cx G = F * Cx(f.re / n2, -f.im / n2);
+    for (int i = 0; i < 4; i++) mats[o.idx + i] = orig[i] * G;
+    o.kind = SOP_U;
+}
 
 int classify_2x2(const Cx* m) {
     bool real = true, rx = true;
@@ -480,6 +543,7 @@ std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n,
         dr_flush();
         ops.insert(ops.end(), folds.begin(), folds.end());
     }
+    scale_rotations(ops, mats);
     if ((int)ops.size() > KATE_MAX_SOPS || (int)mats.size() > KATE_MAX_MATS)
         return "pass program too large for the kernel parameter";
     out->nops = (int)ops.size();

@@ -281,6 +281,21 @@ class PlanView:
                             continue
                         if kind in (8, 9):  # real / RX-form 2x2: same arithmetic as U here
                             kind = 3
+                        if kind in (13, 14, 15, 16):  # rotations with their factor taken out
+                            tt = mats[int(op["idx"])]
+                            t0, t1 = tt.real, tt.imag
+                            lo = jj[((jj >> B) & 1) == 0]
+                            hi = lo | (1 << B)
+                            x, y = a[:, :, lo].copy(), a[:, :, hi].copy()
+                            if kind == 13:
+                                a[:, :, lo], a[:, :, hi] = x + t0 * y, t1 * x + y
+                            elif kind == 14:
+                                a[:, :, lo], a[:, :, hi] = t0 * x + y, t1 * y - x
+                            elif kind == 15:
+                                a[:, :, lo], a[:, :, hi] = x + 1j * t0 * y, y + 1j * t1 * x
+                            else:
+                                a[:, :, lo], a[:, :, hi] = y - 1j * t0 * x, x - 1j * t1 * y
+                            continue
                         if kind in (3, 4, 5):
                             lo = jj[((jj >> B) & 1) == 0]
                             if kind == 5:
