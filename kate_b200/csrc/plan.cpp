@@ -108,7 +108,12 @@ void matrix_2x2(const PGate& g, Cx m[4]) {
 int cost_2x2(const Cx m[4]) {
     if (m[1].re == 0.0 && m[1].im == 0.0 && m[2].re == 0.0 && m[2].im == 0.0) return 1;
     int k = classify_2x2(m);
-    return k == SOP_U ? 8 : 4;
+    if (k == SOP_U) return 8;
+    // Real or RX-form: 2 when a factor can be taken out (a = d, or c = +-b).
+    const double a = m[0].re, d = m[3].re;
+    const double b = k == SOP_UX ? m[1].im : m[1].re, c = k == SOP_UX ? m[2].im : m[2].re;
+    const bool scalable = (a == d && a != 0.0) || (b != 0.0 && (k == SOP_UX ? c == b : c == -b));
+    return scalable ? 2 : 4;
 }
 
 PGate make_1q(int q, const Cx m[4], int src) {
