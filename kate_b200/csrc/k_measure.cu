@@ -51,7 +51,7 @@ __device__ __forceinline__ double2 ld_amp(const float2* p) {
 
 // S: stored amplitude type (double2 or float2); sums are FP64 either way.
 template <typename V, typename S = double2>
-__global__ void __launch_bounds__(NT) k_bitsums(const S* __restrict__ st, int n, int g, int nr,
+__global__ void __launch_bounds__(NT, 2) k_bitsums(const S* __restrict__ st, int n, int g, int nr,
                                                 V* __restrict__ part) {
     using A = Acc<V>;
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
