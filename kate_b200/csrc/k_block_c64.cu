@@ -5,8 +5,8 @@
 // Each CTA (256 threads; two CTAs per SM, ~97 KiB of shared memory each, so
 // one CTA's loads and CUDA-core phases overlap the other's tensor-core work)
 // processes 4096-amplitude coset tiles in a grid-stride loop. Per tile:
-//   0. the tile is copied global -> staging buffer S, an amplitude pair per
-//      16-byte load and shared store (tile bit 0 is physical bit 0);
+//   0. the tile is copied global -> staging buffer S with 16-byte cp.async
+//      (an amplitude pair per copy: tile bit 0 is physical bit 0);
 //   for each block of the pass:
 //   1. S is rearranged into the MMA A operand: 128 rows (the values of the
 //      7 non-block tile bits) x 64 reals (the 32 complex amplitudes of the
@@ -51,23 +51,10 @@ constexpr uint32_t SMEM_BYTES = OFF_TAB + KATE_C64_MAX_BLOCKS * 32 * 2 + 1024;  
 constexpr uint32_t TMEM_COLS = 64;
 constexpr long WAIT_LIMIT = 1L << 24;
 
-// Swizzle of the staging tile (float2 elements), linear over GF(2): bit
-// 4 + b of the element index XORs the fixed 4-bit column c[b] into bits
-// 0..3 (the bank pair of an 8-byte element). The columns were chosen by a
-// search over the block programs of brickwork, layered and random circuits
-// so that the 32 rows a warp reads or writes at one block index, and the 32
-// output pairs of a write-back, fall on distinct bank pairs (1.03-1.08
-// times the conflict-free wavefront count, against 1.8-2.0 for a swizzle
-// that keeps element pairs in place). Elements 2m and 2m + 1 stay in one
-// aligned 16-byte slot, in either order: sswz(i ^ 1) = sswz(i) ^ 1.
-__device__ __forceinline__ uint32_t sswz(uint32_t i) {
-    constexpr uint32_t col[8] = {14, 11, 15, 13, 1, 7, 13, 2};
-    uint32_t m = 0;
-#pragma unroll
-    for (int b = 0; b < 8; b++)
-        if ((i >> (4 + b)) & 1u) m ^= col[b];
-    return i ^ m;
-}
+// Pair-preserving swizzle of the staging tile (float2 elements): XORs bits
+// 1..3 of the index with bits 4..6 and 8..10, spreading strided 8-byte
+// accesses over the banks while keeping element pairs 16-byte contiguous.
+__device__ __forceinline__ uint32_t sswz(uint32_t i) { return i ^ ((((i >> 4) ^ (i >> 8)) & 7u) << 1); }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -134,6 +121,7 @@ __global__ void __launch_bounds__(NT, 2)
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(gbase + OFF_MISC + 8);
     int* abort_flag = reinterpret_cast<int*>(gbase + OFF_MISC + 16);
     float2* S = reinterpret_cast<float2*>(gbase + OFF_S);
+    const uint32_t sb = base + OFF_S;
 
     if (t == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
@@ -213,16 +201,6 @@ __global__ void __launch_bounds__(NT, 2)
         oH[j] = o;
     }
     const uint32_t o1 = 1u << P.outsrc[0];
-    // Swizzled slots, by linearity: copy j writes element 2t + 512 j at
-    // sT ^ sJ[j] (and its partner at that ^ 1); write-back pair j reads
-    // sP ^ sO[j] and that ^ sO1.
-    const uint32_t sT = sswz(2u * t), sP = sswz(pT), sO1 = sswz(o1);
-    uint32_t sJ[8], sO[8];
-#pragma unroll
-    for (int j = 0; j < 8; j++) {
-        sJ[j] = sswz((uint32_t)j << 9);
-        sO[j] = sswz(oH[j]);
-    }
     auto coset_base = [&](uint64_t c) {
         uint64_t b = 0;
         for (int i = 0; i < P.ncb; i++) b |= ((c >> i) & 1ull) << P.cphys[i];
@@ -234,17 +212,14 @@ __global__ void __launch_bounds__(NT, 2)
     for (uint64_t c = blockIdx.x; c < ncos; c += gridDim.x) {
         const uint64_t cb = coset_base(c);
         {
-            // An amplitude pair per 16-byte load, stored as one 16-byte slot
-            // (its two halves swapped when the swizzle puts the pair's first
-            // element at the odd position).
             const float2* src = st + cb + dT;
 #pragma unroll
             for (int j = 0; j < 8; j++) {
-                const float4 v = __ldcg(reinterpret_cast<const float4*>(src + dH[j]));
-                const uint32_t sl = sT ^ sJ[j];
-                const float4 w = (sl & 1u) ? make_float4(v.z, v.w, v.x, v.y) : v;
-                *reinterpret_cast<float4*>(S + (sl & ~1u)) = w;
+                const uint32_t d = sb + sswz(2u * t + ((uint32_t)j << 9)) * 8u;
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src + dH[j]) : "memory");
             }
+            asm volatile("cp.async.commit_group;\n" ::: "memory");
+            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
         }
         __syncthreads();
 
@@ -328,8 +303,8 @@ __global__ void __launch_bounds__(NT, 2)
             float2* dst = st + cb + dT;
 #pragma unroll
             for (int j = 0; j < 8; j++) {
-                const uint32_t sl = sP ^ sO[j];
-                const float2 v0 = S[sl], v1 = S[sl ^ sO1];
+                const uint32_t src = pT | oH[j];
+                const float2 v0 = S[sswz(src)], v1 = S[sswz(src | o1)];
                 *reinterpret_cast<float4*>(dst + dH[j]) = make_float4(v0.x, v0.y, v1.x, v1.y);
             }
         }
