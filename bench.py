@@ -361,6 +361,11 @@ def main():
     # End to end through the C ABI with host buffers.
     e2e_steps = max(1, min(args.steps, 3))
     tp_in = np.zeros((n, 2))
+    # One untimed step first: the process's first state allocation of this
+    # size is a one-time cost (later simulators reuse the released buffer).
+    s2 = K.Simulator(circ, 1, K.C128, local)
+    s2.execute(K.proba_state(tp_in))
+    s2.close()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         s2 = K.Simulator(circ, 1, K.C128, local)
@@ -537,12 +542,17 @@ def run_precision(args):
     ov = np.vdot(psi128, psi64)
     infid = float(1.0 - abs(ov) ** 2 / (np.vdot(psi64, psi64).real * np.vdot(psi128, psi128).real))
     del psi64, psi128
-    # End to end: plan + upload + |0> init + passes + proba_state readback.
-    t0 = time.perf_counter()
-    e = K.Simulator(fused, 1, K.C64, 0)
-    e.execute()
-    e.close()
-    e2e_ms = (time.perf_counter() - t0) * 1000
+    # End to end: plan + upload + |0> init + passes + proba_state readback,
+    # after one untimed step (the first state allocation of this size is a
+    # one-time cost; later simulators reuse the released buffer).
+    e2e_steps = 2
+    for i in range(1 + e2e_steps):
+        if i == 1:
+            t0 = time.perf_counter()
+        e = K.Simulator(fused, 1, K.C64, 0)
+        e.execute()
+        e.close()
+    e2e_ms = (time.perf_counter() - t0) * 1000 / e2e_steps
     cpu = None
     if not args.no_cpu_baseline and not _reference_unavailable():
         nn = 24
