@@ -54,6 +54,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -100,7 +101,9 @@ class Clocks:
     def __init__(self, index: int):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        # KATE_CLOCKS_DIR keeps the samples where the caller wants them.
+        d = os.environ.get("KATE_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(d, f"kate_clocks_{os.getpid()}_{index}.csv")
 
     def __enter__(self):
         os.makedirs(os.path.dirname(self.path), exist_ok=True)
