@@ -32,7 +32,7 @@ typedef struct {
 // whose target is a register bit run on registers; controls and diagonal
 // bits may be register, thread or coset bits. Anything else runs as a
 // shared-memory op between register stages.
-#define SOP_STAGE 1  // store registers (if a stage is open), sync, load with rb/tb
+#define SOP_STAGE 1  // store registers (if a stage is open), sync (a warp barrier when src = 1), load with rb/tb
 #define SOP_SMEM 2   // generic op on the shared-memory tile (DevOp index idx)
 #define SOP_U 3      // 2x2 on register bit a; matrix mats[idx .. idx+3] (row-major)
 #define SOP_H 4      // Hadamard on register bit a (the reference's arithmetic)

@@ -369,6 +369,7 @@ struct DirectIO {
     uint64_t ml[64], mh[64], sl[64], sh[64];
     uint64_t lr[16], sr[16];
     int okL, okS;
+    int wl;  // every shared-memory exchange of a coset stays within a warp (see setup_direct)
 };
 
 // Physical offset of tile slot x (byte offset >> 4 in the complex128
@@ -390,16 +391,18 @@ __device__ __forceinline__ void setup_direct(DirectIO& D, const ProgView& P, uin
     else if (t < 128) D.mh[t - 64] = slot_phys((t - 64) << 6, in);
     else if (t < 192) D.sl[t - 128] = slot_phys(t - 128, out);
     else D.sh[t - 192] = slot_phys((t - 192) << 6, out);
-    int first = -1, last = -1, smem_before = 0, smem_after = 0;
+    int first = -1, last = -1, smem_before = 0, smem_after = 0, smem_any = 0, wide = 0;
     for (int k = 0; k < P.nops; k++) {
         const int kind = P.ops[k].kind;
         if (kind == SOP_STAGE) {
+            if (first >= 0 && P.ops[k].src != 1) wide = 1;  // a boundary that needs the whole CTA
             if (first < 0) first = P.ops[k].idx;
             last = P.ops[k].idx;
             smem_after = 0;
         } else if (kind == SOP_SMEM) {
             if (first < 0) smem_before = 1;
             smem_after = 1;
+            smem_any = 1;
         }
     }
     if (t < 32) {
@@ -426,6 +429,11 @@ __device__ __forceinline__ void setup_direct(DirectIO& D, const ProgView& P, uin
         };
         D.okL = !smem_before && lanes_ok(first, in);
         D.okS = !smem_after && lanes_ok(last, out);
+        // With both ends in HBM, no shared-memory op and every boundary
+        // warp-local (so every stage gives the warp index the same tile
+        // bits), a coset's shared-memory slots are only touched by one warp:
+        // the next coset then needs a warp barrier, not a CTA one.
+        D.wl = D.okL && D.okS && !smem_any && !wide;
     }
 }
 
@@ -542,7 +550,10 @@ __device__ __forceinline__ void run_program(const TileTables<C2>& T, int nops, u
                     break;
                 }
             }
-            __syncthreads();
+            // src = 1: both stages give the same tile bits to the warp index,
+            // so each warp reloads only the slots it stored.
+            if (op.src == 1) __syncwarp();
+            else __syncthreads();
             const uint32_t w0 = tab[32], w1 = tab[33], w2 = tab[34], w3 = tab[35];
 #pragma unroll
             for (int j = 0; j < 16; j++) a[j] = A::lds(tb + reg_off(j, sl, w0, w1, w2, w3));

@@ -108,8 +108,10 @@ __global__ void __launch_bounds__(NT, NBUF == 1 ? 2 : 1)
             __syncthreads();
             store_tile<C2, false>(T, st, c, tb, t);
         }
-        // The buffer is rewritten by the next coset.
-        __syncthreads();
+        // The buffer is rewritten by the next coset (only in the same warps'
+        // slots when every exchange is warp-local).
+        if (tile_direct<C2, NBUF>() && D->wl) __syncwarp();
+        else __syncthreads();
     }
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }

@@ -258,11 +258,10 @@ std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n,
     std::vector<SOp> ops;
     std::vector<Cx> mats;
 
-    int scheduled = 0;
-    while (scheduled < N) {
-        // Tentative register stage.
-        std::vector<char> d2(done);
-        std::vector<int> R, list;
+    // Greedy register stage from the ops not yet done: its register bits R
+    // (at most 4 targets) and its op list in order.
+    auto select = [&](const std::vector<char>& base, std::vector<int>& R, std::vector<int>& list) {
+        std::vector<char> d2(base);
         for (;;) {
             int pick = -1;
             for (int i = 0; i < N && pick < 0; i++)
@@ -279,6 +278,24 @@ std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n,
             d2[pick] = 1;
             list.push_back(pick);
         }
+    };
+    auto pad = [&](std::vector<int>& R) {
+        for (int t = 0; t < m && R.size() < 4; t++)
+            if (std::find(R.begin(), R.end(), t) == R.end()) R.push_back(t);
+    };
+    // Warp bits (thread bits 5..7) of the previous stage, when its registers
+    // are still open (no shared-memory op since): a stage that keeps them,
+    // on tile bits outside both stages' registers, exchanges the tile only
+    // within each warp (every warp stores and reloads the slots whose warp
+    // bits are its index), so its boundary needs a warp barrier only.
+    std::vector<int> prevW;
+    bool prev_open = false;
+
+    int scheduled = 0;
+    while (scheduled < N) {
+        // Tentative register stage.
+        std::vector<int> R, list;
+        select(done, R, list);
         if (list.empty()) {
             int first = -1;
             for (int i = 0; i < N && first < 0; i++)
@@ -290,24 +307,60 @@ std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n,
             ops.push_back(s);
             done[first] = 1;
             scheduled++;
+            prev_open = false;
             continue;
         }
-        for (int t = 0; t < m && R.size() < 4; t++)
-            if (std::find(R.begin(), R.end(), t) == R.end()) R.push_back(t);
-        // Thread map: three low thread bits on tile bits of distinct residue
-        // mod 3 (conflict-free 16-byte accesses under the XOR swizzle of
-        // k_tile.cu), then the other non-register bits ascending.
-        std::vector<int> nonR, tb;
+        pad(R);
+        std::vector<int> nonR;
         for (int t = 0; t < m; t++)
             if (std::find(R.begin(), R.end(), t) == R.end()) nonR.push_back(t);
-        bool res_used[3] = {false, false, false};
+        auto is_nonR = [&](int t) { return std::find(nonR.begin(), nonR.end(), t) != nonR.end(); };
+        // Warp bits: the previous stage's when they are not register bits
+        // here (warp-local boundary), else three non-register bits that the
+        // next stage (looked ahead) does not take as registers either. Only
+        // bits above 3 qualify while there are enough: tile bits 0..3 are
+        // physical bits 0..3 and stay lanes, which keeps the first and last
+        // stages' HBM accesses in 256-byte runs (worth more than a warp-local
+        // boundary).
+        bool local_in = prev_open && prevW.size() == 3;
+        for (int t : prevW)
+            if (!is_nonR(t) || t < 4) local_in = false;
+        std::vector<int> Wb;
+        if (local_in) {
+            Wb = prevW;
+        } else {
+            std::vector<char> dn(done);
+            for (int i : list) dn[i] = 1;
+            std::vector<int> Rn, ln;
+            select(dn, Rn, ln);
+            if (!ln.empty()) pad(Rn);
+            auto in_Rn = [&](int t) { return std::find(Rn.begin(), Rn.end(), t) != Rn.end(); };
+            for (int pass2 = 0; pass2 < 3 && Wb.size() < 3; pass2++)
+                for (int k = (int)nonR.size() - 1; k >= 0 && Wb.size() < 3; k--) {
+                    const int t = nonR[k];
+                    if (std::find(Wb.begin(), Wb.end(), t) != Wb.end()) continue;
+                    const bool ok = pass2 == 0 ? (t >= 4 && !in_Rn(t)) : pass2 == 1 ? t >= 4 : true;
+                    if (ok) Wb.push_back(t);
+                }
+        }
+        // Thread map: lanes first — three low thread bits on tile bits of
+        // distinct residue mod 3 (conflict-free 16-byte accesses under the
+        // XOR swizzle of k_tile.cu), then the other lane bits ascending —
+        // then the warp bits.
+        std::vector<int> lanes, tb;
         for (int t : nonR)
+            if (std::find(Wb.begin(), Wb.end(), t) == Wb.end()) lanes.push_back(t);
+        bool res_used[3] = {false, false, false};
+        for (int t : lanes)
             if (tb.size() < 3 && !res_used[t % 3]) {
                 res_used[t % 3] = true;
                 tb.push_back(t);
             }
-        for (int t : nonR)
+        for (int t : lanes)
             if (std::find(tb.begin(), tb.end(), t) == tb.end()) tb.push_back(t);
+        for (int t : Wb) tb.push_back(t);
+        prevW = Wb;
+        prev_open = true;
         auto regpos = [&](int t) { return (int)(std::find(R.begin(), R.end(), t) - R.begin()); };
         auto thrpos = [&](int t) { return (int)(std::find(tb.begin(), tb.end(), t) - tb.begin()); };
         auto in_R = [&](int t) { return std::find(R.begin(), R.end(), t) != R.end(); };
@@ -447,6 +500,7 @@ std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n,
         SOp st{};
         st.kind = SOP_STAGE;
         st.idx = (uint16_t)si;
+        st.src = local_in ? 1 : 0;  // boundary needs a warp barrier only
         ops.push_back(st);
         for (int i : prefix) done[i] = 1;
         for (int i : suffix) done[i] = 1;

@@ -161,3 +161,51 @@ def test_c64_block_programs_match_oracle(oracle, seed):
     a, b = got / np.linalg.norm(got), ref / np.linalg.norm(ref)
     assert 1 - abs(np.vdot(a, b)) ** 2 <= 1e-8
     assert np.abs(got - ref).max() <= 1e-4
+
+
+def _warp_local_violations(prog):
+    """Stage boundaries marked warp-local (STAGE op src = 1) must give the
+    warp index (thread bits 5..7) the same tile bits in both stages, those
+    bits must be register bits in neither, and no shared-memory op may sit
+    between the two stages."""
+    bad = []
+    prev = None
+    for k in range(int(prog["nops"])):
+        op = prog["ops"][k]
+        kind = int(op["kind"])
+        if kind == 2:
+            prev = None
+        elif kind == 1:
+            si = int(op["idx"])
+            if int(op["src"]) == 1:
+                if prev is None:
+                    bad.append((k, "no open stage before"))
+                else:
+                    w0 = [int(x) for x in prog["stb"][prev][5:8]]
+                    w1 = [int(x) for x in prog["stb"][si][5:8]]
+                    regs = set(int(x) for x in prog["srb"][prev]) | set(int(x) for x in prog["srb"][si])
+                    if w0 != w1 or regs & set(w1):
+                        bad.append((k, w0, w1, sorted(regs)))
+            prev = si
+    return bad
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_warp_local_stage_boundaries_are_safe(oracle, seed):
+    rng = np.random.default_rng(900 + seed)
+    n = 18
+    g = random_circuit(n, 200, rng)
+    for c in (K.Circuit(n, g), K.Circuit(30, circuits.layered(30, 20, 1234))):
+        pv = PlanView(c)
+        marked = 0
+        for prog in pv.programs:
+            if prog is None:
+                continue
+            assert _warp_local_violations(prog) == []
+            marked += sum(1 for k in range(int(prog["nops"])) if int(prog["ops"][k]["kind"]) == 1 and
+                          int(prog["ops"][k]["src"]) == 1)
+        if c.nqbits == 30:
+            assert marked > 0
+    st0 = np.zeros(1 << n, dtype=np.complex128)
+    st0[0] = 1
+    assert np.abs(PlanView(K.Circuit(n, g)).run_staged(st0) - oracle.simulate(n, g)).max() <= 1e-12
