@@ -209,3 +209,28 @@ def test_warp_local_stage_boundaries_are_safe(oracle, seed):
     st0 = np.zeros(1 << n, dtype=np.complex128)
     st0[0] = 1
     assert np.abs(PlanView(K.Circuit(n, g)).run_staged(st0) - oracle.simulate(n, g)).max() <= 1e-12
+
+
+def test_factored_rotations_at_edge_angles(oracle):
+    """RX / RY at angles where one factor vanishes or dominates (0, pi/2,
+    pi, 3pi/2, and a random spread) run as factored rotations; the emulated
+    program matches the oracle."""
+    n = 13
+    angles = [0.0, np.pi / 2, np.pi, 1.5 * np.pi, 2 * np.pi, 1e-9, np.pi - 1e-9]
+    rng = np.random.default_rng(77)
+    angles += list(rng.uniform(0, 2 * np.pi, 12))
+    g = []
+    for i, th in enumerate(angles):
+        q = i % n
+        g.append((0, [q], 0, circuits.rx(th)))
+        g.append((0, [(q + 5) % n], 0, circuits.ry(th)))
+        g.append((3, [q, (q + 1) % n], 0, None))
+    pv = PlanView(K.Circuit(n, g))
+    kinds = set()
+    for prog in pv.programs:
+        if prog is not None:
+            kinds |= {int(prog["ops"][k]["kind"]) for k in range(int(prog["nops"]))}
+    assert kinds & {13, 14, 15, 16}
+    st0 = np.zeros(1 << n, dtype=np.complex128)
+    st0[0] = 1
+    assert np.abs(pv.run_staged(st0) - oracle.simulate(n, g)).max() <= 1e-12
