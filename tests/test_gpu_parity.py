@@ -97,3 +97,25 @@ def test_sampling_follows_probabilities(oracle):
     hist = np.bincount(s.astype(np.int64), minlength=1 << n) / len(s)
     assert np.abs(hist - p).max() < 0.01
     assert np.array_equal(s[:100], sim.sample(100, seed=42)[:100])
+
+
+def test_factored_rotations_at_edge_angles_complex128_and_complex64(oracle):
+    """RX / RY at angles where a rotation's factor vanishes or dominates run as
+    factored register ops on the GPU: complex128 within 1e-12 of the oracle,
+    complex64 within 1e-5."""
+    n = 14
+    angles = [0.0, np.pi / 2, np.pi, 1.5 * np.pi, 2 * np.pi, 1e-9, np.pi - 1e-9]
+    rng = np.random.default_rng(78)
+    angles += list(rng.uniform(0, 2 * np.pi, 20))
+    g = []
+    for i, th in enumerate(angles):
+        q = i % n
+        g.append((0, [q], 0, circuits.rx(th)))
+        g.append((0, [(q + 5) % n], 0, circuits.ry(th)))
+        g.append((3, [q, (q + 1) % n], 0, None))
+    ref = oracle.simulate(n, g)
+    s128, _ = run(n, g)
+    assert np.abs(s128.state() - ref).max() <= TOL
+    s64 = K.Simulator(K.Circuit(n, g), 1, K.C64, 0)
+    s64.execute()
+    assert np.abs(s64.state() - ref).max() <= 1e-5
