@@ -44,6 +44,10 @@ Other workloads (``--workload``), one JSON line each:
              through the continuous-batching server under a 150 GB
              admission budget, rates swept: circuits/s and p50/p99 latency,
              against one-at-a-time plain launches.
+  qulacs     the reference's own benchmark circuit (QulacsBench, 25 qubits,
+             complex128): ms per execution, lower is better, against its
+             published 1x MI200 time (vs_baseline), its CPU simulator and its
+             GPU path on the same GPU.
 """
 from __future__ import annotations
 
@@ -70,7 +74,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="kate_b200", choices=["kate_b200", "reference"])
-    ap.add_argument("--workload", default="layers", choices=["layers", "precision", "batch", "serve"])
+    ap.add_argument("--workload", default="layers", choices=["layers", "precision", "batch", "serve", "qulacs"])
     ap.add_argument("--nqubits", type=int, default=None)
     ap.add_argument("--layers", type=int, default=20)
     ap.add_argument("--circuits", type=int, default=4096, help="batch: circuits in the batch")
@@ -84,7 +88,7 @@ def parse():
     ap.add_argument("--no-baseline", action="store_true", help="batch/serve: skip the one-at-a-time baseline")
     a = ap.parse_args()
     if a.nqubits is None:
-        a.nqubits = 32 if a.workload == "precision" else 30
+        a.nqubits = {"precision": 32, "qulacs": 25}.get(a.workload, 30)
     return a
 
 
@@ -302,7 +306,8 @@ def run_reference(args):
 def main():
     args = parse()
     if args.workload != "layers":
-        {"precision": run_precision, "batch": run_batch, "serve": run_serve}[args.workload](args)
+        {"precision": run_precision, "batch": run_batch, "serve": run_serve,
+         "qulacs": run_qulacs}[args.workload](args)
         return
     if args.impl == "reference":
         run_reference(args)
@@ -574,6 +579,165 @@ def run_precision(args):
                   "kernel": "k_block_c64 (tcgen05 kind::f16, split-BF16 x3)", "alg_bytes_per_launch": alg,
                   "avg_launch_ms": avg_pass},
         gpu_launches=launches * args.steps, clocks=clk.summary(), cpu_baseline=cpu)))
+
+
+QULACS_PUBLISHED_MS = 1035.41  # README.md:29 of the reference: QulacsBench 25q on 1x AMD MI200
+
+
+def run_qulacs(args):
+    """The reference's own benchmark circuit (BenchCircuits.hpp:8-42,
+    QulacsBench: 41 n Hadamard and CNOT-ring gates) at n qubits, complex128,
+    |0..0>; one step = one execution (initialisation + every group pass).
+    Metric: wall time per execution in ms (lower is better), the figure the
+    reference publishes for 25 qubits (README.md:23-31)."""
+    import numpy as np
+    from kate_b200 import circuits
+
+    n = args.nqubits
+    gates = circuits.qulacs_bench(n)
+    cfg = {"workload": f"QulacsBench circuit (H / CNOT-ring layers), n={n}, complex128, |0..0>",
+           "nqubits": n, "gates": len(gates), "state_bytes": 16 << n,
+           "l2": "state larger than L2 (126 MB); no flush needed" if (16 << n) > (126 << 20)
+           else "state fits L2: steps run back to back", "parallelism": "replicas"}
+    metric, unit = f"QulacsBench {n}q wall time", "ms"
+    published = QULACS_PUBLISHED_MS if n == 25 else None
+
+    def line(value, ms_per_step, dtype, **extra):
+        out = _common(metric, unit, value, args, ms_per_step, dtype, cfg, **extra)
+        out["higher_is_better"] = False
+        out["data"] = "synthetic (the benchmark's fixed gate structure, generated in code)"
+        if published is not None:
+            out["vs_baseline"] = value / published
+            out["vs_baseline_note"] = ("value / 1035.41 ms, the reference's published 1x MI200 time "
+                                       "(README.md:29); below 1 is faster")
+        return out
+
+    def cpu_run():
+        """The reference's CPU simulator on the whole circuit, compiled as its
+        main.cpp does (gateScheduling + gateGrouping(12) + compileDefault)."""
+        from oracle.oracle import Ref
+        ref = Ref()
+        c = ref.circuit(n, gates)
+        c.schedule()
+        c.group(min(12, n))
+        c.compile_default(0)
+        sess = c.session()
+        try:
+            return sess.run(), ref.hw_threads()
+        finally:
+            sess.close()
+
+    if args.impl == "reference":
+        if int(os.environ.get("RANK", "0")) != 0:
+            return
+        if _reference_unavailable():
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built"}))
+            return
+        for _ in range(args.warmup):
+            cpu_run()
+        runs = [cpu_run() for _ in range(args.steps)]
+        ms = sum(r[0] for r in runs) / len(runs)
+        cores = runs[0][1]
+        print(json.dumps(line(ms, ms, "c128 (f64)", impl="reference",
+                              cpu_baseline={"value": ms, "unit": unit, "cores": cores, "kind": "reference",
+                                            "sample": f"each step = the whole n={n} circuit on the reference "
+                                                      f"CPUSimulator (gateScheduling + gateGrouping(12)), gate "
+                                                      f"phase only, {cores} threads"},
+                              e2e={"value": ms, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})))
+        return
+
+    import torch
+    import kate_b200 as K
+
+    torch.cuda.set_device(0)
+    circ = K.Circuit(n, gates)
+    sim = K.Simulator(circ, 1, K.C128, 0)
+    passes = sim.passes()
+    launches = sim.launches_per_run()
+    stream = torch.cuda.Stream()
+    for _ in range(args.warmup):
+        sim.run_async(stream.cuda_stream)
+    stream.synchronize()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(0) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            sim.run_async(stream.cuda_stream)
+        ev1.record(stream)
+        ev1.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    init_ms, pass_ms = sim.profile_passes()
+    avg_pass = (ms - init_ms) / max(1, len(passes))
+    alg = 2.0 * 16.0 * 2 ** n
+    peak, peak_kind = measured_hbm_peak()
+    kate_proba = sim.execute().as_array()
+    sim.close()
+    del sim
+
+    # End to end through the public API: Simulator(circuit) (plan + upload)
+    # + execute() with the proba_state copied to the host, after one untimed
+    # step (first allocation of the state).
+    e2e_steps = max(1, min(args.steps, 5))
+    for i in range(1 + e2e_steps):
+        if i == 1:
+            t0 = time.perf_counter()
+        e = K.Simulator(circ, 1, K.C128, 0)
+        e.execute()
+        e.close()
+    e2e_ms = (time.perf_counter() - t0) * 1000.0 / e2e_steps
+    n_ops = sum(ng for _, ng in passes)
+    h2d = n_ops * 112 + 16 * 4 * n_ops
+    g_bits = min(n - 12, 10)
+    r_bits = n - 12 - g_bits
+    if r_bits > 8:
+        g_bits, r_bits = n - 12 - 8, 8
+    d2h = 2 * n * 8 + 16 * (1 + 2 * (12 + r_bits)) * (1 << g_bits)
+
+    ref_gpu = None
+    if not args.no_ref_gpu:
+        try:
+            from oracle import ref_gpu as RG
+            if not RG.available():
+                ref_gpu = {"value": None, "unavailable": "oracle/_ref/libkate_ref_gpu.so was not built"}
+            else:
+                rc = RG.RefGpuCircuit(n, gates)
+                rc.compile(fuse=0, group=RG.MAX_GROUP_QUBITS)
+                s = rc.session()
+                try:
+                    runs = [s.run() for _ in range(4)]
+                    proba = s.proba_state()
+                finally:
+                    s.close()
+                d = np.abs(np.asarray(kate_proba) - proba)
+                d[:, 1] = np.minimum(d[:, 1], 2 * np.pi - d[:, 1])
+                rms = sum(runs[1:]) / 3
+                ref_gpu = {"value": rms, "unit": unit, "runs_timed": 3, "speedup": rms / ms,
+                           "plan": "gateScheduling + gateGrouping(9) + compileDefault(0) (main.cpp's recipe, "
+                                   "grouping capped at 9 qubits)", "groups": rc.num_groups(),
+                           "timing": "wall clock of the reference's instruction loop",
+                           "proba_state_max_abs_diff_vs_kate_b200": float(d.max())}
+        except Exception as ex:  # reported, not fatal
+            ref_gpu = {"value": None, "unavailable": f"failed: {ex}"}
+
+    cpu = None
+    if not args.no_cpu_baseline and not _reference_unavailable():
+        cms, cores = cpu_run()
+        cpu = {"value": cms, "unit": unit, "cores": cores, "kind": "reference",
+               "sample": f"the whole n={n} circuit once on the reference CPUSimulator (gateScheduling + "
+                         f"gateGrouping(12)), gate phase only"}
+    cfg.update({"passes_per_step": len(passes), "ops": n_ops})
+    print(json.dumps(line(
+        ms, ms, "c128 (f64)",
+        e2e={"value": e2e_ms, "unit": unit, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+             "ms_per_step": e2e_ms},
+        roofline={"bound": "hbm", "achieved": alg / (avg_pass / 1000) / 1e9, "peak": peak, "unit": "GB/s",
+                  "frac": alg / (avg_pass / 1000) / 1e9 / peak, "traffic": committed_traffic(n),
+                  "peak_source": peak_kind, "kernel": "k_tile<double2> (register-staged group pass)",
+                  "alg_bytes_per_launch": alg, "avg_launch_ms": avg_pass,
+                  "profiled_pass_ms": {"min": min(pass_ms), "max": max(pass_ms),
+                                       "mean": sum(pass_ms) / len(pass_ms)}},
+        gpu_launches=launches * args.steps, clocks=clk.summary(), cpu_baseline=cpu, ref_gpu_baseline=ref_gpu)))
 
 
 def _hea_batch(K, C, count, seed=2024):

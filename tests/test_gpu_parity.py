@@ -27,6 +27,16 @@ def test_layered_n20_10_layers_matches_oracle(oracle):
     assert np.abs(res.as_array() - oracle.measure(n, ref)).max() <= 1e-9
 
 
+def test_qulacs_bench_n20_matches_oracle(oracle):
+    # The reference's own benchmark circuit (BenchCircuits.hpp:8-42).
+    n = 20
+    gates = circuits.qulacs_bench(n)
+    sim, res = run(n, gates)
+    ref = oracle.simulate(n, gates)
+    assert np.abs(sim.state() - ref).max() <= TOL
+    assert np.abs(res.as_array() - oracle.measure(n, ref)).max() <= 1e-9
+
+
 @pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 7, 9, 12, 13, 16])
 def test_random_circuits_all_gate_kinds(oracle, n):
     rng = np.random.default_rng(100 + n)

@@ -40,6 +40,15 @@ def test_layered_n20_plan_matches_oracle(oracle):
     assert np.abs(pv.run(zero_state(n)) - oracle.simulate(n, gates)).max() <= 1e-12
 
 
+def test_qulacs_bench_ring_plan_matches_oracle(oracle):
+    # The reference's benchmark circuit closes its CNOT ring with
+    # (n-1, 0): the tile of that gate holds the lowest and highest qubit.
+    n = 16
+    gates = circuits.qulacs_bench(n)
+    pv = PlanView(K.Circuit(n, gates), 12, 4, 0)
+    assert np.abs(pv.run(zero_state(n)) - oracle.simulate(n, gates)).max() <= 1e-12
+
+
 def test_every_pass_keeps_the_low_bits_in_the_tile():
     n = 24
     pv = PlanView(K.Circuit(n, circuits.layered(n, 4)), 12, 4, 0)
