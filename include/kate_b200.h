@@ -82,6 +82,14 @@ KATE_API const char* kate_last_error(void);
 /* Library version string. */
 KATE_API const char* kate_version(void);
 
+/* printGpuInfo()  HIPcode/DeviceInfo.hpp:10-35: the number of CUDA devices
+ * (0 when none answers), and one device's name (NUL-terminated, at most
+ * name_cap bytes), global memory, shared memory per block and SM count.
+ * Every output pointer is nullable. */
+KATE_API kate_status kate_device_count(int* out);
+KATE_API kate_status kate_device_properties(int device, char* name, int name_cap, size_t* global_mem,
+                                            size_t* shared_mem_per_block, int* sm_count);
+
 /* ---- circuit building: backendagnosticcode/QuantumCircuit.hpp:18-37 ---- */
 
 /* Circuit(int nqbits)  QuantumCircuit.hpp:18-20. 1 <= nqbits <= 40. */
@@ -166,6 +174,15 @@ KATE_API kate_status kate_sim_execute(kate_sim* s, double* theta_phi);
 /* execute(proba_state& in, displaytime)  HIPcode/simulator.hpp:354-406: the
  * initial state is the product state given by 2*n doubles (theta, phi). */
 KATE_API kate_status kate_sim_execute_from(kate_sim* s, const double* theta_phi_in, double* theta_phi_out);
+
+/* execute(displaytime = true)  HIPcode/simulator.hpp:301-353: the same run
+ * as kate_sim_execute (theta_phi_in nullable: |0..0>; else the product state
+ * of kate_sim_execute_from), with the phases the reference prints timed:
+ * ms[0] initialisation and ms[1] the group passes (CUDA events on the
+ * simulator's stream), ms[2] the measurement (host clock, copy included),
+ * ms[3] the number of group passes. ms and theta_phi_out nullable. */
+KATE_API kate_status kate_sim_execute_timed(kate_sim* s, const double* theta_phi_in, double* theta_phi_out,
+                                            double* ms);
 
 /* Asynchronous form for callers that own a CUDA stream (cudaStream_t passed
  * as void*; NULL = the simulator's own stream): initialise and run every

@@ -14,6 +14,7 @@
 #include <cmath>
 #include <iostream>
 #include <string>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -54,6 +55,29 @@ public:
     double norm() const { return std::sqrt(a * a + b * b); }
     void print() const { std::cout << a << " + " << b << "i"; }
 };
+
+// printGpuInfo (HIPcode/DeviceInfo.hpp:10-35): host threads, the CUDA
+// devices, and device 0's memory in qubits of complex128 state.
+inline void printGpuInfo() {
+    std::cout << "CPU Info: " << std::thread::hardware_concurrency() << " threads" << std::endl;
+    int count = 0;
+    kate_device_count(&count);
+    if (count == 0) {
+        std::cout << "couldnt detect devices, check permissions" << std::endl;
+        return;
+    }
+    char name[256];
+    size_t gmem = 0, smem = 0;
+    int sms = 0;
+    for (int i = 0; i < count; i++)
+        if (check(kate_device_properties(i, name, (int)sizeof(name), nullptr, nullptr, nullptr)))
+            std::cout << "GPU " << i << " : " << name << std::endl;
+    std::cout << "-----------------------" << std::endl;
+    if (!check(kate_device_properties(0, name, (int)sizeof(name), &gmem, &smem, &sms))) return;
+    std::cout << "current GPU: " << std::endl << name << " (" << sms << " SMs)" << std::endl << std::endl;
+    std::cout << "Global memory: " << gmem << " (" << (int)std::log2((double)gmem / 16.0) << " qbits)" << std::endl;
+    std::cout << "Shared memory per block : " << smem << std::endl << std::endl;
+}
 
 // Square row-major matrix (basic_host_types.hpp:86-186).
 template <typename T>
@@ -194,21 +218,18 @@ public:
     Simulator& operator=(const Simulator&) = delete;
     ~Simulator() { kate_sim_destroy(s_); }
 
-    proba_state execute(bool displaytime = false) {
-        (void)displaytime;
-        std::vector<double> tp(2 * n_);
-        check(kate_sim_execute(s_, tp.data()));
-        return to_proba(tp);
-    }
+    // displaytime prints the phases the reference prints (device time of
+    // the initialisation and of the group passes, host time of the
+    // measurement). Qubit relabelings replace the reference's swaps, so the
+    // swap share is 0.
+    proba_state execute(bool displaytime = false) { return run(nullptr, displaytime); }
     proba_state execute(proba_state& in, bool displaytime = false) {
-        (void)displaytime;
-        std::vector<double> tin(2 * n_), tp(2 * n_);
+        std::vector<double> tin(2 * n_);
         for (int i = 0; i < n_ && i < (int)in.val.size(); i++) {
             tin[2 * i] = in.val[i].first;
             tin[2 * i + 1] = in.val[i].second;
         }
-        check(kate_sim_execute_from(s_, tin.data(), tp.data()));
-        return to_proba(tp);
+        return run(tin.data(), displaytime);
     }
     // The state in the reference's amplitude order.
     std::vector<Complex> state() {
@@ -221,6 +242,21 @@ public:
     kate_sim* handle() { return s_; }
 
 private:
+    proba_state run(const double* tin, bool displaytime) {
+        std::vector<double> tp(2 * n_);
+        if (!displaytime) {
+            check(tin ? kate_sim_execute_from(s_, tin, tp.data()) : kate_sim_execute(s_, tp.data()));
+            return to_proba(tp);
+        }
+        double ms[4] = {0, 0, 0, 0};
+        if (check(kate_sim_execute_timed(s_, tin, tp.data(), ms))) {
+            std::cout << "Initialization/Measurement : " << ms[0] << " / " << ms[2] << " ms" << std::endl;
+            std::cout << "Total computing time : " << ms[1] << " ms with swap% : 0%" << std::endl;
+            std::cout << "Average swap time : 0 ms and average group time : " << (ms[3] > 0 ? ms[1] / ms[3] : 0.0)
+                      << " ms" << std::endl;
+        }
+        return to_proba(tp);
+    }
     proba_state to_proba(const std::vector<double>& tp) {
         std::vector<std::pair<double, double>> v(n_);
         for (int i = 0; i < n_; i++) v[i] = {tp[2 * i], tp[2 * i + 1]};

@@ -274,6 +274,40 @@ def release_cached_memory(device: int = -1):
     _check(_lib.lib().kate_release_cached_memory(int(device)))
 
 
+def devices():
+    """The CUDA devices: a list of (name, global memory bytes, shared memory
+    per block, SM count); empty when no device answers."""
+    L = _lib.lib()
+    n = ctypes.c_int()
+    _check(L.kate_device_count(ctypes.byref(n)))
+    out = []
+    for i in range(n.value):
+        name = ctypes.create_string_buffer(256)
+        gm, sm = ctypes.c_size_t(), ctypes.c_size_t()
+        cnt = ctypes.c_int()
+        _check(L.kate_device_properties(i, name, 256, ctypes.byref(gm), ctypes.byref(sm), ctypes.byref(cnt)))
+        out.append((name.value.decode(), gm.value, sm.value, cnt.value))
+    return out
+
+
+def printGpuInfo():
+    """printGpuInfo (HIPcode/DeviceInfo.hpp:10-35): host threads, the CUDA
+    devices, device 0's memory in qubits of complex128 state."""
+    import math
+    print(f"CPU Info: {os.cpu_count()} threads")
+    devs = devices()
+    if not devs:
+        print("couldnt detect devices, check permissions")
+        return
+    for i, d in enumerate(devs):
+        print(f"GPU {i} : {d[0]}")
+    print("-----------------------")
+    name, gm, sm, cnt = devs[0]
+    print(f"current GPU: \n{name} ({cnt} SMs)\n")
+    print(f"Global memory: {gm} ({int(math.log2(gm / 16))} qbits)")
+    print(f"Shared memory per block : {sm}\n")
+
+
 def mergeGate(gates: Sequence[Gate]) -> Gate:
     """CPUmergeGate / mergeGate (CPUcode/GateMerger.hpp:8-55): FP64 product
     of the gates on the sorted union of their qubits."""
@@ -310,10 +344,25 @@ class Simulator:
         return self._h
 
     def execute(self, arg=False, displaytime: bool = False) -> proba_state:
-        """execute(displaytime) or execute(proba_state_in, displaytime)."""
+        """execute(displaytime) or execute(proba_state_in, displaytime).
+        With displaytime the phases the reference prints are timed and
+        printed (HIPcode/simulator.hpp:346-350); ``last_times`` keeps them
+        (init_ms, passes_ms, measure_ms, passes)."""
         out = np.zeros(2 * self.nqbits, dtype=np.float64)
+        pin = None
         if isinstance(arg, proba_state):
             pin = arg.as_array().ravel().copy()
+        else:
+            displaytime = bool(arg) or displaytime
+        if displaytime:
+            ms = np.zeros(4, dtype=np.float64)
+            _check(self._lib.kate_sim_execute_timed(self._h, None if pin is None else pin.ctypes.data_as(_dp),
+                                                    out.ctypes.data_as(_dp), ms.ctypes.data_as(_dp)))
+            self.last_times = tuple(float(x) for x in ms)
+            print(f"Initialization/Measurement : {ms[0]:g} / {ms[2]:g} ms")
+            print(f"Total computing time : {ms[1]:g} ms with swap% : 0%")
+            print(f"Average swap time : 0 ms and average group time : {ms[1] / max(ms[3], 1):g} ms")
+        elif pin is not None:
             _check(self._lib.kate_sim_execute_from(self._h, pin.ctypes.data_as(_dp), out.ctypes.data_as(_dp)))
         else:
             _check(self._lib.kate_sim_execute(self._h, out.ctypes.data_as(_dp)))
@@ -390,7 +439,7 @@ class Simulator:
         return out
 
 
-__all__ = ["Gate", "Circuit", "Simulator", "mergeGate", "release_cached_memory", "proba_state", "KateError", "Hadamard", "CNOT", "CRk",
+__all__ = ["Gate", "Circuit", "Simulator", "mergeGate", "release_cached_memory", "devices", "printGpuInfo", "proba_state", "KateError", "Hadamard", "CNOT", "CRk",
            "TOFFOLI", "RX", "RZ", "DENSE", "C128", "C64"]
 
 

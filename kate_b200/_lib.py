@@ -21,6 +21,8 @@ _vpp = _c.POINTER(_c.c_void_p)
 SIGNATURES = {
     "kate_last_error": [],
     "kate_version": [],
+    "kate_device_count": [_ip],
+    "kate_device_properties": [_i, _c.c_char_p, _i, _c.POINTER(_c.c_size_t), _c.POINTER(_c.c_size_t), _ip],
     "kate_circuit_create": [_i, _vpp],
     "kate_circuit_destroy": [_vp],
     "kate_circuit_clone": [_vp, _vpp],
@@ -47,6 +49,7 @@ SIGNATURES = {
     "kate_sim_destroy": [_vp],
     "kate_sim_execute": [_vp, _dp],
     "kate_sim_execute_from": [_vp, _dp, _dp],
+    "kate_sim_execute_timed": [_vp, _dp, _dp, _dp],
     "kate_sim_run_async": [_vp, _vp],
     "kate_sim_synchronize": [_vp],
     "kate_sim_proba_state": [_vp, _dp],

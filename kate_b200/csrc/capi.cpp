@@ -2,6 +2,8 @@
 #include "devcache.hpp"
 #include "kate_b200.h"
 
+#include <cuda_runtime.h>
+
 #include <cstring>
 #include <exception>
 #include <string>
@@ -78,6 +80,34 @@ extern "C" {
 
 const char* kate_last_error(void) { return g_last_error.c_str(); }
 const char* kate_version(void) { return "kate_b200 0.1 (sm_100a)"; }
+
+kate_status kate_device_count(int* out) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();  // no driver or no device: report zero devices
+        n = 0;
+    }
+    if (out) *out = n;
+    return KATE_OK;
+}
+
+kate_status kate_device_properties(int device, char* name, int name_cap, size_t* global_mem,
+                                   size_t* shared_mem_per_block, int* sm_count) {
+    int n = 0;
+    kate_device_count(&n);
+    REQUIRE(device >= 0 && device < n, "no such CUDA device");
+    cudaDeviceProp p{};
+    const cudaError_t e = cudaGetDeviceProperties(&p, device);
+    if (e != cudaSuccess) return fail(KATE_ECUDA, std::string("cudaGetDeviceProperties: ") + cudaGetErrorString(e));
+    if (name && name_cap > 0) {
+        std::strncpy(name, p.name, (size_t)name_cap - 1);
+        name[name_cap - 1] = 0;
+    }
+    if (global_mem) *global_mem = p.totalGlobalMem;
+    if (shared_mem_per_block) *shared_mem_per_block = p.sharedMemPerBlock;
+    if (sm_count) *sm_count = p.multiProcessorCount;
+    return KATE_OK;
+}
 
 kate_status kate_circuit_create(int nqbits, kate_circuit** out) {
     return guarded([&] {
@@ -377,6 +407,13 @@ kate_status kate_sim_execute_from(kate_sim* s, const double* in, double* out) {
         if (e.empty()) e = s->sim->synchronize();
         if (e.empty() && out) e = s->sim->proba_state(out);
         return sim_status(e);
+    });
+}
+
+kate_status kate_sim_execute_timed(kate_sim* s, const double* in, double* out, double* ms) {
+    return guarded([&] {
+        REQUIRE(s, "null simulator");
+        return sim_status(s->sim->execute_timed(in, out, ms));
     });
 }
 

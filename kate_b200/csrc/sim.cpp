@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -223,6 +224,24 @@ std::string Simulator::run_async(void* stream_in, const double* tp) {
     SimImpl& S = *d_;
     KCHECK(cudaSetDevice(S.device));
     cudaStream_t st = stream_in ? (cudaStream_t)stream_in : S.stream;
+    std::string e = enqueue_init(st, tp);
+    if (!e.empty()) return e;
+    e = enqueue_passes(st);
+    if (!e.empty()) return e;
+    if (st != S.stream) {
+        // Order later library work on the simulator's stream after the caller's.
+        cudaEvent_t ev;
+        KCHECK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        KCHECK(cudaEventRecord(ev, st));
+        KCHECK(cudaStreamWaitEvent(S.stream, ev, 0));
+        cudaEventDestroy(ev);
+    }
+    return "";
+}
+
+std::string Simulator::enqueue_init(void* stream, const double* tp) {
+    SimImpl& S = *d_;
+    cudaStream_t st = (cudaStream_t)stream;
     if (tp) {
         // execute(proba_state&): product state, qubit i placed at label
         // initial_permutation[i] (CPUcode/simulator.hpp:139-162).
@@ -241,16 +260,56 @@ std::string Simulator::run_async(void* stream_in, const double* tp) {
     } else {
         KCHECK(launch_set_basis0(S.d_state, S.dim(), S.precision, st));
     }
+    return "";
+}
+
+std::string Simulator::enqueue_passes(void* stream) {
+    SimImpl& S = *d_;
+    cudaStream_t st = (cudaStream_t)stream;
     for (size_t i = 0; i < S.hpasses.size(); i++) KCHECK(S.launch_pass(i, st));
     S.phys = S.plan.final_phys;
     S.has_state = true;
-    if (st != S.stream) {
-        // Order later library work on the simulator's stream after the caller's.
-        cudaEvent_t ev;
-        KCHECK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-        KCHECK(cudaEventRecord(ev, st));
-        KCHECK(cudaStreamWaitEvent(S.stream, ev, 0));
-        cudaEventDestroy(ev);
+    return "";
+}
+
+namespace {
+struct EventSet {
+    cudaEvent_t e[3] = {nullptr, nullptr, nullptr};
+    ~EventSet() {
+        for (auto x : e)
+            if (x) cudaEventDestroy(x);
+    }
+};
+}  // namespace
+
+std::string Simulator::execute_timed(const double* tp_in, double* tp_out, double* ms) {
+    SimImpl& S = *d_;
+    KCHECK(cudaSetDevice(S.device));
+    EventSet ev;
+    for (auto& x : ev.e) KCHECK(cudaEventCreate(&x));
+    KCHECK(cudaEventRecord(ev.e[0], S.stream));
+    std::string e = enqueue_init(S.stream, tp_in);
+    if (!e.empty()) return e;
+    KCHECK(cudaEventRecord(ev.e[1], S.stream));
+    e = enqueue_passes(S.stream);
+    if (!e.empty()) return e;
+    KCHECK(cudaEventRecord(ev.e[2], S.stream));
+    e = synchronize();
+    if (!e.empty()) return e;
+    float a = 0, b = 0;
+    KCHECK(cudaEventElapsedTime(&a, ev.e[0], ev.e[1]));
+    KCHECK(cudaEventElapsedTime(&b, ev.e[1], ev.e[2]));
+    const auto t0 = std::chrono::steady_clock::now();
+    if (tp_out) {
+        e = proba_state(tp_out);
+        if (!e.empty()) return e;
+    }
+    const auto t1 = std::chrono::steady_clock::now();
+    if (ms) {
+        ms[0] = a;
+        ms[1] = b;
+        ms[2] = std::chrono::duration<double, std::milli>(t1 - t0).count();
+        ms[3] = (double)S.hpasses.size();
     }
     return "";
 }

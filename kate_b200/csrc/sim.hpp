@@ -22,6 +22,10 @@ public:
 
     std::string run_async(void* stream, const double* theta_phi_in);  // init + all passes, no sync
     std::string synchronize();
+    // init + passes with CUDA events between them, then the measurement on
+    // the host clock: ms[0] init, ms[1] group passes, ms[2] proba_state,
+    // ms[3] number of passes. tp_in / tp_out nullable.
+    std::string execute_timed(const double* tp_in, double* tp_out, double* ms);
     std::string proba_state(double* theta_phi);                       // reference measurement
     std::string get_state(double* out);                               // 2*2^n doubles, label order
     std::string set_state(const double* in);
@@ -38,6 +42,9 @@ public:
     SimImpl* impl() { return d_; }
 
 private:
+    // Queue the initial state / every group pass on stream st (cudaStream_t).
+    std::string enqueue_init(void* st, const double* tp);
+    std::string enqueue_passes(void* st);
     SimImpl* d_ = nullptr;
 };
 

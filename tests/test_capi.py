@@ -134,3 +134,13 @@ def test_plan_requires_valid_tile():
     h = ctypes.c_void_p()
     assert _lib.lib().kate_plan_create(c.handle, 0, 0, 0, ctypes.byref(h)) == K.KATE_EINVAL
     assert _lib.lib().kate_plan_create(c.handle, 15, 0, 0, ctypes.byref(h)) == K.KATE_EINVAL
+
+
+def test_device_queries_without_a_gpu_report_zero_devices():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("GPU present")
+    assert K.devices() == []
+    L = _lib.lib()
+    with pytest.raises(K.KateError, match="no such CUDA device"):
+        K._check(L.kate_device_properties(0, None, 0, None, None, None))

@@ -12,16 +12,25 @@ from kate_b200 import _lib
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-@pytest.fixture(scope="module")
-def facade_exe(tmp_path_factory):
-    out = str(tmp_path_factory.mktemp("cxx") / "facade_main")
+def _build(tmp_path_factory, name):
+    out = str(tmp_path_factory.mktemp("cxx") / name)
     libdir = os.path.dirname(_lib.LIB_PATH)
     cmd = ["g++", "-std=c++17", "-O1", "-I" + os.path.join(ROOT, "include"), os.path.join(ROOT, "tests", "cxx",
-           "facade_main.cpp"), "-L" + libdir, "-lkate_b200", "-Wl,-rpath," + libdir, "-o", out]
+           name + ".cpp"), "-L" + libdir, "-lkate_b200", "-Wl,-rpath," + libdir, "-o", out]
     # the library is named libkate_b200.so in the package directory
     r = subprocess.run(cmd, capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     return out
+
+
+@pytest.fixture(scope="module")
+def facade_exe(tmp_path_factory):
+    return _build(tmp_path_factory, "facade_main")
+
+
+@pytest.fixture(scope="module")
+def bench_exe(tmp_path_factory):
+    return _build(tmp_path_factory, "bench_main")
 
 
 def test_facade_builds_and_runs_the_passes(facade_exe):
@@ -35,3 +44,32 @@ def test_facade_simulates_on_the_gpu(facade_exe, oracle):
     r = subprocess.run([facade_exe, "sim"], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stdout + r.stderr
     assert r.stdout.count("Qbit ") == 10
+
+
+def test_reference_main_builds_with_bench_circuits(bench_exe):
+    # The reference's main.cpp pattern: printGpuInfo, QulacsBench, QFT,
+    # randomCircuit (BenchCircuits.hpp), the compile passes.
+    n = 12
+    r = subprocess.run([bench_exe, "plan", str(n)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert f"qulacs gates {41 * n}" in r.stdout
+    assert f"qft gates {n * (n + 1) // 2}" in r.stdout
+    assert "random gates 50" in r.stdout
+    assert "CPU Info:" in r.stdout and "done" in r.stdout
+
+
+@pytest.mark.gpu
+def test_reference_main_simulates_with_displaytime(bench_exe, oracle):
+    from kate_b200 import circuits
+    n = 12
+    r = subprocess.run([bench_exe, "sim", str(n)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "GPU 0 : " in r.stdout
+    assert "Initialization/Measurement : " in r.stdout and "Total computing time : " in r.stdout
+    got = []
+    for line in r.stdout.splitlines():
+        if line.startswith("Qbit "):
+            t, p = line.split(":", 1)[1].split(",")
+            got.append((float(t.split("=")[1]), float(p.split("=")[1])))
+    ref = oracle.measure(n, oracle.simulate(n, circuits.qulacs_bench(n)))
+    assert np.abs(np.array(got) - ref).max() <= 1e-5  # printed with 6 significant digits

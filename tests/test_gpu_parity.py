@@ -37,6 +37,22 @@ def test_qulacs_bench_n20_matches_oracle(oracle):
     assert np.abs(res.as_array() - oracle.measure(n, ref)).max() <= 1e-9
 
 
+def test_execute_displaytime_times_the_phases(oracle, capsys):
+    # execute(true) prints the reference's three timing lines
+    # (HIPcode/simulator.hpp:346-350) and returns the same proba_state.
+    n = 16
+    gates = circuits.qulacs_bench(n)
+    sim = K.Simulator(K.Circuit(n, gates), 1, K.C128, 0)
+    res = sim.execute(True)
+    out = capsys.readouterr().out
+    assert "Initialization/Measurement : " in out and "Total computing time : " in out
+    init_ms, passes_ms, meas_ms, npass = sim.last_times
+    assert npass == len(sim.passes()) and passes_ms > 0 and init_ms >= 0 and meas_ms > 0
+    assert np.abs(res.as_array() - oracle.measure(n, oracle.simulate(n, gates))).max() <= 1e-9
+    names = [d[0] for d in K.devices()]
+    assert names and "B200" in names[0]
+
+
 @pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 7, 9, 12, 13, 16])
 def test_random_circuits_all_gate_kinds(oracle, n):
     rng = np.random.default_rng(100 + n)
