@@ -260,23 +260,43 @@ std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n,
 
     // Greedy register stage from the ops not yet done: its register bits R
     // (at most 4 targets) and its op list in order.
+    // Each pick is the lowest-index ready op whose target is a register bit
+    // (or that has none), else the lowest-index ready op with a target while
+    // R has room. The ready ops are kept as an ascending list, updated from
+    // the pending-predecessor counts as ops are picked.
+    std::vector<std::vector<int>> succs(N);
+    for (int i = 0; i < N; i++)
+        for (int p : preds[i]) succs[p].push_back(i);
+    std::vector<int> npend(N);
     auto select = [&](const std::vector<char>& base, std::vector<int>& R, std::vector<int>& list) {
-        std::vector<char> d2(base);
+        std::vector<int> rdy;
+        for (int i = 0; i < N; i++) {
+            int c = 0;
+            for (int p : preds[i]) c += !base[p];
+            npend[i] = c;
+            if (!base[i] && c == 0) rdy.push_back(i);
+        }
+        auto in_R = [&](int t) { return std::find(R.begin(), R.end(), t) != R.end(); };
         for (;;) {
-            int pick = -1;
-            for (int i = 0; i < N && pick < 0; i++)
-                if (regable(i) && ready(i, d2) &&
-                    (L[i].tgt < 0 || std::find(R.begin(), R.end(), L[i].tgt) != R.end()))
-                    pick = i;
-            if (pick < 0 && R.size() < 4)
-                for (int i = 0; i < N && pick < 0; i++)
-                    if (regable(i) && ready(i, d2) && L[i].tgt >= 0) {
-                        pick = i;
+            size_t at = rdy.size();
+            for (size_t k = 0; k < rdy.size() && at == rdy.size(); k++) {
+                const int i = rdy[k];
+                if (regable(i) && (L[i].tgt < 0 || in_R(L[i].tgt))) at = k;
+            }
+            if (at == rdy.size() && R.size() < 4)
+                for (size_t k = 0; k < rdy.size() && at == rdy.size(); k++) {
+                    const int i = rdy[k];
+                    if (regable(i) && L[i].tgt >= 0) {
+                        at = k;
                         R.push_back(L[i].tgt);
                     }
-            if (pick < 0) break;
-            d2[pick] = 1;
+                }
+            if (at == rdy.size()) break;
+            const int pick = rdy[at];
+            rdy.erase(rdy.begin() + (long)at);
             list.push_back(pick);
+            for (int s : succs[pick])
+                if (--npend[s] == 0 && !base[s]) rdy.insert(std::lower_bound(rdy.begin(), rdy.end(), s), s);
         }
     };
     auto pad = [&](std::vector<int>& R) {
