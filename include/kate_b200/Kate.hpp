@@ -174,6 +174,85 @@ public:
         check(kate_circuit_compile_opt(h_, k, mtm, groupsize, numberofgpulog2, maxlocalqbitnumber));
     }
     void exportqcx(const std::string& filename) { check(kate_circuit_export_qcx(h_, filename.c_str())); }
+    // QuantumCircuit::print (QuantumCircuit.hpp:38-123): the gate list (by
+    // group once grouped) before compilation; after it the program: swaps,
+    // then each group with its gates, with permutationtable the
+    // label-to-qubit table before each group.
+    void print(bool permutationtable = false) const {
+        int ng = 0, ngr = 0, ni = 0;
+        kate_circuit_num_gates(h_, &ng);
+        kate_circuit_num_groups(h_, &ngr);
+        kate_circuit_num_instructions(h_, &ni);
+        std::vector<int> q(256);
+        auto gate_line = [&](int i) {
+            int id = 0, nq = 0, opt = 0;
+            kate_circuit_get_gate(h_, i, &id, q.data(), &nq, &opt, nullptr);
+            std::cout << "Identifier : " << id << ", Qbits affected : ";
+            for (int k = 0; k < nq; k++) std::cout << q[k] << " ";
+            std::cout << std::endl;
+        };
+        auto group_head = [&](const char* label, int g, int* end) {
+            int nq = 0;
+            kate_circuit_get_group(h_, g, end, q.data(), &nq);
+            std::cout << label << " " << g << " with qbits ";
+            for (int k = 0; k < nq; k++) std::cout << q[k] << " ";
+            std::cout << " : " << std::endl;
+        };
+        if (ni == 0) {
+            int group = 0, end = -1;
+            if (ngr) group_head("Group", 0, &end);
+            for (int i = 0; i < ng; i++) {
+                if (ngr) {
+                    if (group >= ngr) {
+                        std::cout << "ERROR while printing the circuit, group vector is bad" << std::endl;
+                        return;
+                    }
+                    if (end == i) group_head("Group", ++group, &end);
+                    std::cout << "   ";
+                    gate_line(i);
+                } else {
+                    std::cout << "gate " << i << " is ";
+                    gate_line(i);
+                }
+            }
+            return;
+        }
+        std::vector<int> perm(nqbits), fin(nqbits), inv(nqbits);
+        int valid = 0;
+        kate_circuit_get_permutations(h_, perm.data(), fin.data(), &valid);
+        for (int m = 0; m < nqbits; m++) inv[perm[m]] = m;
+        std::cout << "-------Quantum-Program-------" << std::endl;
+        int i = 0, group = 0;
+        for (int k = 0; k < ni; k++) {
+            int kind = 0, nq = 0;
+            kate_circuit_get_instruction(h_, k, &kind, q.data(), &nq);
+            if (kind == 0) {
+                std::cout << "SWAP ";
+                for (int m = 0; m < nq / 2; m++) {
+                    std::cout << q[2 * m] << " and " << q[2 * m + 1] << ", ";
+                    std::swap(inv[q[2 * m]], inv[q[2 * m + 1]]);
+                }
+            } else {
+                if (permutationtable) {
+                    std::cout << "Permutation table (subjective to real) : " << std::endl;
+                    for (int m = 0; m < nqbits; m++) std::cout << m << " " << (m < 10 ? " " : "");
+                    std::cout << std::endl;
+                    for (int m = 0; m < nqbits; m++) std::cout << inv[m] << " " << (inv[m] < 10 ? " " : "");
+                    std::cout << std::endl << std::endl;
+                }
+                int end = 0;
+                group_head("EXEC Group", group, &end);
+                for (int j = i; j < end; j++) {
+                    std::cout << "   ";
+                    gate_line(j);
+                }
+                i = end;
+                group++;
+            }
+            std::cout << std::endl << std::endl;
+        }
+        std::cout << "-----------------------------" << std::endl;
+    }
     int gateCount() const {
         int n = 0;
         kate_circuit_num_gates(h_, &n);

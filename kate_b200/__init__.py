@@ -257,6 +257,68 @@ class Circuit:
                                                        ctypes.byref(v)))
         return (list(a), list(b)) if v.value else (None, None)
 
+    def print(self, permutationtable: bool = False):
+        """Kate's QuantumCircuit::print (QuantumCircuit.hpp:38-123): the gate
+        list (by group once grouped) before compilation, the program
+        (swaps, then each group with its gates; with permutationtable the
+        label-to-qubit table before each group) after it."""
+        print(self.program_text(permutationtable), end="")
+
+    def program_text(self, permutationtable: bool = False) -> str:
+        """The text ``print`` writes."""
+        gates = self.gate_set_ordered
+        groups = self.groups
+        instr = self.instructions
+
+        def gate_line(g):
+            return "Identifier : " + str(g[0]) + ", Qbits affected : " + "".join(f"{q} " for q in g[1]) + "\n"
+
+        def group_head(label, k):
+            return f"{label} {k} with qbits " + "".join(f"{q} " for q in groups[k][1]) + " : \n"
+
+        out = ""
+        if not instr:
+            group = 0
+            if groups:
+                out += group_head("Group", 0)
+            for i, g in enumerate(gates):
+                if groups:
+                    if group >= len(groups):
+                        return out + "ERROR while printing the circuit, group vector is bad\n"
+                    if groups[group][0] == i:
+                        group += 1
+                        out += group_head("Group", group)
+                    out += "   " + gate_line(g)
+                else:
+                    out += f"gate {i} is " + gate_line(g)
+            return out
+        perm, _ = self.permutations()
+        n = self.nqbits
+        inv = [0] * n
+        for m in range(n):
+            inv[perm[m]] = m
+        out += "-------Quantum-Program-------\n"
+        i, group = 0, 0
+        for kind, q in instr:
+            if kind == 0:
+                out += "SWAP "
+                for m in range(len(q) // 2):
+                    a, b = q[2 * m], q[2 * m + 1]
+                    out += f"{a} and {b}, "
+                    inv[a], inv[b] = inv[b], inv[a]
+            else:
+                if permutationtable:
+                    out += "Permutation table (subjective to real) : \n"
+                    out += "".join(f"{m} " + (" " if m < 10 else "") for m in range(n)) + "\n"
+                    out += "".join(f"{inv[m]} " + (" " if inv[m] < 10 else "") for m in range(n)) + "\n\n"
+                out += group_head("EXEC Group", group)
+                for j in range(i, groups[group][0]):
+                    out += "   " + gate_line(gates[j])
+                i = groups[group][0]
+                group += 1
+            out += "\n\n"
+        return out + "-----------------------------\n"
+
     def merge(self, begin: int, end: int) -> Gate:
         """mergeGate of gates [begin, end) of this circuit."""
         q = np.zeros(64, dtype=np.int32)

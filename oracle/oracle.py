@@ -205,6 +205,11 @@ class RefCircuit:
     def export_qcx(self, path):
         self.lib.kref_export_qcx(self.h, path.encode())
 
+    def print_to(self, path, permutationtable=False):
+        """QuantumCircuit::print, appended to the file at path."""
+        if self.lib.kref_print(self.h, int(permutationtable), path.encode()) != 0:
+            raise OSError(f"cannot append to {path}")
+
 
 class RefSession:
     def __init__(self, circ: RefCircuit):
@@ -253,6 +258,8 @@ class Ref:
         lib.kref_merge.restype = _i
         lib.kref_simulate.argtypes = [_vp, _dp, _dp, _dp, ctypes.POINTER(_d)]
         lib.kref_export_qcx.argtypes = [_vp, ctypes.c_char_p]
+        lib.kref_print.argtypes = [_vp, ctypes.c_int, ctypes.c_char_p]
+        lib.kref_print.restype = ctypes.c_int
         lib.kref_session_new.argtypes = [_vp]
         lib.kref_session_new.restype = _vp
         lib.kref_session_run.argtypes = [_vp]

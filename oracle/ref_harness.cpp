@@ -14,6 +14,7 @@
 //   CPUmergeGate                       CPUcode/GateMerger.hpp:8-55
 //   CPUSimulator::execute              CPUcode/simulator.hpp:71-128
 //   exportqcx                          backendagnosticcode/Circuit.hpp:763-774
+//   print                              backendagnosticcode/QuantumCircuit.hpp:38-123
 //
 // Thread-count pin: CPUSimulator::executeCommand splits 2^(n-14) groups over
 // std::thread::hardware_concurrency() threads and silently drops the
@@ -237,5 +238,16 @@ double kref_session_run(void* s) {
 void kref_session_free(void* s) { delete static_cast<Kate::Simulator*>(s); }
 
 void kref_export_qcx(void* h, const char* path) { static_cast<Handle*>(h)->circ.exportqcx(std::string(path)); }
+
+// QuantumCircuit::print(permutationtable) with std::cout appended to `path`.
+int kref_print(void* h, int permutationtable, const char* path) {
+    std::ofstream f(path, std::ios::app);
+    if (!f) return 1;
+    std::streambuf* old = std::cout.rdbuf(f.rdbuf());
+    static_cast<Handle*>(h)->circ.print(permutationtable != 0);
+    std::cout.flush();
+    std::cout.rdbuf(old);
+    return 0;
+}
 
 }  // extern "C"

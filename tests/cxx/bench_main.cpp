@@ -13,6 +13,20 @@ using namespace Kate;
 int main(int argc, char** argv) {
     const bool sim = argc > 1 && std::strcmp(argv[1], "sim") == 0;
     const int n = argc > 2 ? std::atoi(argv[2]) : 12;
+    if (argc > 1 && std::strcmp(argv[1], "print") == 0) {
+        // Circuit::print before compilation (grouped), then of two programs:
+        // one with swap instructions (allocate(1)), one without.
+        Circuit c = QulacsBench(n);
+        c.gateScheduling();
+        c.gateGrouping(3);
+        c.print();
+        Circuit swapped = c;
+        swapped.allocate(1);
+        swapped.print(true);
+        c.compileDefault(0);
+        c.print(false);
+        return last_status() == KATE_OK ? 0 : 1;
+    }
     printGpuInfo();
     Circuit circuit = QulacsBench(n);
     std::cout << "qulacs gates " << circuit.gateCount() << std::endl;

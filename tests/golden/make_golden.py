@@ -14,6 +14,8 @@ Outputs (small, committed):
                allocate / compileDefault on seeded circuits
   merge.npz    CPUmergeGate results
   circuit.qcx  exportqcx output of a small circuit
+  print_qulacs4.txt  QuantumCircuit::print output (grouped, with swaps,
+               compiled); ``make_golden.py print`` rewrites only this file
 """
 from __future__ import annotations
 
@@ -144,8 +146,37 @@ def main():
     c = ref.circuit(5, [(2, [0], 0, None), (3, [1, 2], 0, None), (4, [3, 0], 3, None), (5, [0, 1, 4], 0, None),
                         (0, [2, 3], 0, np.eye(4, dtype=np.complex128))])
     c.export_qcx(os.path.join(HERE, "circuit.qcx"))
+    write_print_golden(ref)
     print("golden fixtures written to", HERE)
 
 
-if __name__ == "__main__":
+def write_print_golden(ref):
+    """print_qulacs4.txt: QuantumCircuit::print of the 4-qubit QulacsBench
+    circuit after gateScheduling + gateGrouping(3), then with permutation
+    tables after allocate(1) (swap instructions), then after
+    compileDefault(0)."""
+    path = os.path.join(HERE, "print_qulacs4.txt")
+    if os.path.exists(path):
+        os.remove(path)
+    gates = circuits.qulacs_bench(4)
+
+    def grouped():
+        c = ref.circuit(4, gates)
+        c.schedule()
+        c.group(3)
+        return c
+
+    grouped().print_to(path)
+    s = grouped()
+    s.allocate(1)
+    s.print_to(path, True)
+    c = grouped()
+    c.compile_default(0)
+    c.print_to(path, False)
+
+
+if __name__ == "__main__" and sys.argv[1:] == ["print"]:
+    from oracle.oracle import Ref as _Ref  # noqa: E402
+    write_print_golden(_Ref())
+elif __name__ == "__main__":
     main()

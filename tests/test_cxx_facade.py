@@ -73,3 +73,36 @@ def test_reference_main_simulates_with_displaytime(bench_exe, oracle):
             got.append((float(t.split("=")[1]), float(p.split("=")[1])))
     ref = oracle.measure(n, oracle.simulate(n, circuits.qulacs_bench(n)))
     assert np.abs(np.array(got) - ref).max() <= 1e-5  # printed with 6 significant digits
+
+
+def test_circuit_print_matches_between_cxx_and_python(bench_exe):
+    # QuantumCircuit::print (QuantumCircuit.hpp:38-123) from the C++ facade
+    # and the Python mirror: grouped gate list, a program with swaps and
+    # permutation tables, a program without swaps.
+    import kate_b200 as K
+    from kate_b200 import circuits
+    n = 6
+    r = subprocess.run([bench_exe, "print", str(n)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, r.stdout + r.stderr
+    c = K.Circuit(n, circuits.qulacs_bench(n))
+    c.gateScheduling()
+    c.gateGrouping(3)
+    want = c.program_text()
+    s = c.copy()
+    s.allocate(1)
+    swapped = s.program_text(True)
+    assert "SWAP " in swapped and "Permutation table (subjective to real) : " in swapped
+    want += swapped
+    c.compileDefault(0)
+    want += c.program_text(False)
+    assert r.stdout == want
+    assert want.count("EXEC Group") == 2 * len(c.groups)
+
+
+def test_circuit_print_matches_the_reference_golden(bench_exe):
+    # tests/golden/print_qulacs4.txt is the reference's own print output
+    # (tests/golden/make_golden.py).
+    golden = open(os.path.join(ROOT, "tests", "golden", "print_qulacs4.txt")).read()
+    r = subprocess.run([bench_exe, "print", "4"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout == golden
