@@ -52,9 +52,28 @@ public:
     Complex operator-(Complex o) const { return Complex(a - o.a, b - o.b); }
     Complex operator*(Complex o) const { return Complex(a * o.a - b * o.b, a * o.b + b * o.a); }
     Complex operator*(double d) const { return Complex(a * d, b * d); }
+    Complex operator*(int d) const { return Complex(a * d, b * d); }
+    Complex operator/(Complex o) const {
+        const double n = o.a * o.a + o.b * o.b;
+        return Complex((a * o.a + b * o.b) / n, (o.a * b - a * o.b) / n);
+    }
+    void operator+=(Complex o) { a += o.a, b += o.b; }
+    void operator-=(Complex o) { a -= o.a, b -= o.b; }
+    void operator*=(Complex o) { *this = *this * o; }
+    void operator*=(double d) { a *= d, b *= d; }
     double norm() const { return std::sqrt(a * a + b * b); }
+    // atan(b / a), as the reference computes it (not atan2).
+    double angle() const { return std::atan(b / a); }
     void print() const { std::cout << a << " + " << b << "i"; }
 };
+
+namespace detail {
+inline void print_entry(const Complex& c) { c.print(); }
+template <typename T>
+void print_entry(const T& v) {
+    std::cout << v;
+}
+}  // namespace detail
 
 // printGpuInfo (HIPcode/DeviceInfo.hpp:10-35): host threads, the CUDA
 // devices, and device 0's memory in qubits of complex128 state.
@@ -100,6 +119,50 @@ public:
     void fill(T v) {
         for (auto& x : storage) x = v;
     }
+    void copy(const Matrix& o) { storage = o.storage, data = storage.data(); }
+    void print() const {
+        for (int i = 0; i < n; i++) {
+            for (int j = 0; j < n; j++) {
+                detail::print_entry(data[(size_t)i * n + j]);
+                std::cout << " | ";
+            }
+            std::cout << std::endl;
+        }
+    }
+    Matrix operator+(const Matrix& o) const {
+        Matrix r(*this);
+        r += o;
+        return r;
+    }
+    Matrix operator-(const Matrix& o) const {
+        Matrix r(*this);
+        r -= o;
+        return r;
+    }
+    void operator+=(const Matrix& o) {
+        for (size_t i = 0; i < storage.size(); i++) storage[i] += o.storage[i];
+    }
+    void operator-=(const Matrix& o) {
+        for (size_t i = 0; i < storage.size(); i++) storage[i] -= o.storage[i];
+    }
+    // Matrix product (this * o), summed in k order like the reference.
+    Matrix operator*(const Matrix& o) const {
+        Matrix r(n);
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) {
+                T sum = T(0);
+                for (int k = 0; k < n; k++) sum += data[(size_t)i * n + k] * o(k, j);
+                r(i, j, sum);
+            }
+        return r;
+    }
+    void operator*=(double d) {
+        for (auto& x : storage) x *= d;
+    }
+    void transpose() {
+        for (int i = 0; i < n; i++)
+            for (int j = i + 1; j < n; j++) std::swap(data[(size_t)i * n + j], data[(size_t)j * n + i]);
+    }
 };
 
 // Gate (basic_host_types.hpp:190-296).
@@ -107,10 +170,16 @@ class Gate {
 public:
     int identifier = -1;
     int optarg = 0;
+    double optarg2 = 0;
+    Complex optarg3;
     std::vector<int> qbits;
     Matrix<Complex> densecontent;
-    Gate(int id, std::vector<int>& q, int opt = 0) : identifier(id), optarg(opt), qbits(q) {}
+    Gate(int id, std::vector<int>& q, int opt = 0, double opt2 = 0, Complex opt3 = 0)
+        : identifier(id), optarg(opt), optarg2(opt2), optarg3(opt3), qbits(q) {}
     Gate(Matrix<Complex>& m, std::vector<int>& q) : identifier(0), qbits(q), densecontent(m) {}
+    // A gate id carrying a matrix (basic_host_types.hpp:246-262): the id
+    // decides what is applied, as in the reference.
+    Gate(int id, Matrix<Complex>& m, std::vector<int>& q) : identifier(id), qbits(q), densecontent(m) {}
     void print() const {
         std::cout << "Identifier : " << identifier << ", Qbits affected : ";
         for (int q : qbits) std::cout << q << " ";

@@ -37,6 +37,9 @@ def test_facade_builds_and_runs_the_passes(facade_exe):
     r = subprocess.run([facade_exe], capture_output=True, text=True, timeout=60)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "gates" in r.stdout
+    # H*H = I (x2 after the scale), (1+2i)/(3+4i) = 0.44+0.08i, +1, *i, *2
+    vals = [float(x) for x in r.stdout.split("arith ")[1].split()[:5]]
+    assert vals == pytest.approx([2.0, 0.0, -0.16, 2.88, np.pi / 4], abs=1e-6)  # printed to 6 digits
 
 
 @pytest.mark.gpu
