@@ -47,14 +47,24 @@ kate_status from_msg(const std::string& msg, kate_status code = KATE_EINVAL) {
 }
 
 // Simulator messages from CUDA calls carry the call name; classify them.
+// A bounded device wait that gave up says "timed out".
 kate_status sim_status(const std::string& msg) {
     if (msg.empty()) return KATE_OK;
+    if (msg.find("timed out") != std::string::npos) return fail(KATE_ETIMEDOUT, msg);
     if (msg.find("cudaMalloc") != std::string::npos || msg.find("MemoryAllocation") != std::string::npos)
         return fail(KATE_ENOMEM, msg);
     if (msg.find("no state") != std::string::npos) return fail(KATE_ESTATE, msg);
     if (msg.find("cuda") != std::string::npos || msg.find("launch") != std::string::npos)
         return fail(KATE_ECUDA, msg);
     return fail(KATE_EINVAL, msg);
+}
+
+// Errors of device work already queued: a bounded wait that gave up, else
+// a CUDA failure.
+kate_status device_status(const std::string& msg) {
+    if (msg.empty()) return KATE_OK;
+    if (msg.find("timed out") != std::string::npos) return fail(KATE_ETIMEDOUT, msg);
+    return fail(KATE_ECUDA, msg);
 }
 
 template <typename F>
@@ -749,7 +759,7 @@ kate_status kate_batch_synchronize(kate_batch* b) {
     return guarded([&] {
         REQUIRE(b, "null batch");
         std::string e = b->b->synchronize();
-        if (!e.empty()) return fail(KATE_ECUDA, e);
+        if (!e.empty()) return device_status(e);
         return KATE_OK;
     });
 }
@@ -760,7 +770,7 @@ kate_status kate_batch_run(kate_batch* b) {
         std::string e = b->b->run_async(nullptr);
         if (!e.empty()) return sim_status(e);
         e = b->b->synchronize();
-        if (!e.empty()) return fail(KATE_ECUDA, e);
+        if (!e.empty()) return device_status(e);
         return KATE_OK;
     });
 }
@@ -769,7 +779,7 @@ kate_status kate_batch_expect_z(kate_batch* b, double* out) {
     return guarded([&] {
         REQUIRE(b && out, "null pointer");
         std::string e = b->b->expect_z(out);
-        if (!e.empty()) return fail(KATE_ECUDA, e);
+        if (!e.empty()) return device_status(e);
         return KATE_OK;
     });
 }
@@ -811,7 +821,7 @@ kate_status kate_batch_time(kate_batch* b, int runs, float* ms) {
     return guarded([&] {
         REQUIRE(b && ms && runs > 0, "null pointer or no runs");
         std::string e = b->b->time_runs(runs, ms);
-        if (!e.empty()) return fail(KATE_ECUDA, e);
+        if (!e.empty()) return device_status(e);
         return KATE_OK;
     });
 }

@@ -123,8 +123,9 @@ def test_dependency_wait_runs_out_and_reports(oracle):
     b.close()
     o.fault_task = ntasks  # 1-based: the last task, a <Z> reduction that waits on the passes
     bad = K.Batch(circs, precision=K.C64, options=o)
-    with pytest.raises(K.KateError, match="timed out"):
+    with pytest.raises(K.KateError, match="timed out") as err:
         bad.run()
+    assert err.value.status == K.KATE_ETIMEDOUT
     bad.close()
     o.fault_task = 0
     good = K.Batch(circs, precision=K.C64, options=o)
