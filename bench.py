@@ -165,6 +165,20 @@ def measured_hbm_peak():
     return 6650.0, "fallback"
 
 
+NOMINAL_HBM_GBS = 8000.0  # B200 HBM3e, nominal
+
+
+def per_pass_gbs(alg_bytes, pass_ms, peak):
+    """Each pass's HBM rate (algorithmic bytes / its event-timed duration)
+    as a distribution, against the measured and the nominal peak."""
+    g = sorted(alg_bytes / (ms / 1000.0) / 1e9 for ms in pass_ms if ms > 0)
+    if not g:
+        return None
+    med = statistics.median(g)
+    return {"min": g[0], "median": med, "max": g[-1], "median_frac": med / peak,
+            "median_frac_of_nominal": med / NOMINAL_HBM_GBS, "passes": len(g)}
+
+
 def committed_traffic(n):
     """Per-launch DRAM bytes of the group-pass kernel from the committed ncu
     summary (profiles/group_pass_traffic.json), scaled to 2^n amplitudes."""
@@ -424,7 +438,9 @@ def main():
                              "peak_source": peak_kind, "kernel": "k_tile<double2> (register-staged group pass)",
                              "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_pass_ms,
                              "profiled_pass_ms": {"min": min(pass_ms), "max": max(pass_ms),
-                                                  "mean": sum(pass_ms) / len(pass_ms)}},
+                                                  "mean": sum(pass_ms) / len(pass_ms)},
+                             "per_pass_gbs": per_pass_gbs(alg_bytes, pass_ms, peak),
+                             "frac_of_nominal": achieved / NOMINAL_HBM_GBS},
                 "passes_per_step": len(passes), "passes_per_layer": len(passes) / L,
                 "gpu_launches": launches * args.steps, "clocks": clk.summary(),
                 "cpu_baseline": cpu, "ref_gpu_baseline": ref_gpu}
@@ -736,7 +752,9 @@ def run_qulacs(args):
                   "peak_source": peak_kind, "kernel": "k_tile<double2> (register-staged group pass)",
                   "alg_bytes_per_launch": alg, "avg_launch_ms": avg_pass,
                   "profiled_pass_ms": {"min": min(pass_ms), "max": max(pass_ms),
-                                       "mean": sum(pass_ms) / len(pass_ms)}},
+                                       "mean": sum(pass_ms) / len(pass_ms)},
+                  "per_pass_gbs": per_pass_gbs(alg, pass_ms, peak),
+                  "frac_of_nominal": alg / (avg_pass / 1000) / 1e9 / NOMINAL_HBM_GBS},
         gpu_launches=launches * args.steps, clocks=clk.summary(), cpu_baseline=cpu, ref_gpu_baseline=ref_gpu)))
 
 

@@ -55,3 +55,16 @@ def test_single_process_is_unchanged():
     import bench
     assert bench.max_over_ranks(42.0) == 42.0
     assert bench.replica_rate(20, 500.0, 1) == pytest.approx(40.0)
+
+
+def test_per_pass_rates_against_the_peaks():
+    sys.path.insert(0, ROOT)
+    import bench
+    alg = 2 * 16 * 2 ** 30
+    d = bench.per_pass_gbs(alg, [10.0, 20.0, 0.0, 5.0], 6548.8)
+    assert d["passes"] == 3  # a zero duration is dropped
+    assert d["median"] == pytest.approx(alg / 0.010 / 1e9)
+    assert d["min"] < d["median"] < d["max"]
+    assert d["median_frac"] == pytest.approx(d["median"] / 6548.8)
+    assert d["median_frac_of_nominal"] == pytest.approx(d["median"] / 8000.0)
+    assert bench.per_pass_gbs(alg, [], 1.0) is None
