@@ -14,9 +14,20 @@ int main(int argc, char** argv) {
     const bool sim = argc > 1 && std::strcmp(argv[1], "sim") == 0;
     const int n = argc > 2 ? std::atoi(argv[2]) : 12;
     if (argc > 1 && std::strcmp(argv[1], "print") == 0) {
-        // Circuit::print before compilation (grouped), then of two programs:
+        // Circuit::print of plain gates, before compilation (grouped), then of two programs:
         // one with swap instructions (allocate(1)), one without.
         Circuit c = QulacsBench(n);
+        Circuit head(n);  // the first 3n gates (H pairs, one CNOT ring), ungrouped
+        for (int q = 0; q < n; q++) {
+            std::vector<int> v{q};
+            head.appendGate(Gate(Hadamard, v, 0));
+            head.appendGate(Gate(Hadamard, v, 0));
+        }
+        for (int q = 0; q < n; q++) {
+            std::vector<int> v{q, (q + 1) % n};
+            head.appendGate(Gate(CNOT, v));
+        }
+        head.print();
         c.gateScheduling();
         c.gateGrouping(3);
         c.print();

@@ -151,14 +151,16 @@ def main():
 
 
 def write_print_golden(ref):
-    """print_qulacs4.txt: QuantumCircuit::print of the 4-qubit QulacsBench
-    circuit after gateScheduling + gateGrouping(3), then with permutation
+    """print_qulacs4.txt: QuantumCircuit::print of the first 12 gates of the
+    4-qubit QulacsBench circuit as appended, of the whole circuit after
+    gateScheduling + gateGrouping(3), then with permutation
     tables after allocate(1) (swap instructions), then after
     compileDefault(0)."""
     path = os.path.join(HERE, "print_qulacs4.txt")
     if os.path.exists(path):
         os.remove(path)
     gates = circuits.qulacs_bench(4)
+    ref.circuit(4, gates[:12]).print_to(path)  # the first 3n gates, ungrouped: "gate i is ..."
 
     def grouped():
         c = ref.circuit(4, gates)

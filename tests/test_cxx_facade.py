@@ -87,10 +87,12 @@ def test_circuit_print_matches_between_cxx_and_python(bench_exe):
     n = 6
     r = subprocess.run([bench_exe, "print", str(n)], capture_output=True, text=True, timeout=60)
     assert r.returncode == 0, r.stdout + r.stderr
+    want = K.Circuit(n, circuits.qulacs_bench(n)[:3 * n]).program_text()
+    assert want.startswith("gate 0 is Identifier : 2")
     c = K.Circuit(n, circuits.qulacs_bench(n))
     c.gateScheduling()
     c.gateGrouping(3)
-    want = c.program_text()
+    want += c.program_text()
     s = c.copy()
     s.allocate(1)
     swapped = s.program_text(True)
