@@ -1,0 +1,42 @@
+// Pass-specialised group-pass kernels (complex128).
+//
+// The register-staged tile kernel (k_tile.cu) interprets a pass program: per
+// op it loads the op from shared memory, switches on its kind and register
+// bit, and runs one of several unrolled bodies. On B200 that costs about
+// three instructions of dispatch, branching and register moves per FP64
+// instruction. This generator instead turns a pass program into CUDA source
+// in which every op is straight-line code on named registers: register bits,
+// shared-memory and HBM offsets and loop bounds are compile-time constants;
+// matrices stay data (a __grid_constant__ parameter read from the constant
+// bank), so passes of the same shape share one kernel. The source is
+// compiled for sm_100a with NVRTC when a simulator is created and cached per
+// device by its text. The arithmetic of each op is the interpreter's, op for
+// op, so both paths compute the same amplitudes.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "device_types.h"
+
+namespace kate {
+
+// CUDA source of the kernel for `prog`, or "" (with *why set) when the
+// program has a form the generator does not take (shared-memory ops, or a
+// first / last stage whose lanes would not read / write 256-byte runs).
+std::string jit_pass_source(const PassProg& prog, std::string* why);
+
+// Compiles the sources not yet cached on `device` (in parallel) and returns
+// a kernel handle per source. Returns "" on success.
+std::string jit_compile(int device, const std::vector<std::string>& srcs, std::vector<void*>* fns);
+
+// Grid of a pass-specialised kernel for 2^ncb cosets on `device`.
+int jit_grid(int ncb, int device);
+
+// Launches kernel fn (from jit_compile) on the complex128 state st with the
+// matrices of prog.
+cudaError_t jit_launch(void* fn, void* st, const PassProg& prog, int grid, cudaStream_t s);
+
+}  // namespace kate

@@ -501,26 +501,54 @@ __device__ __forceinline__ void store_tile(const TileTables<C2>& T, C2* __restri
     }
 }
 
+// Barrier of the threads that run a program: the whole CTA (MODE 0), or the
+// 256 consumer threads of the warp-specialised tile kernel, named barrier 1
+// (MODE 1; its producer warp does not take part).
+template <int MODE>
+__device__ __forceinline__ void prog_bar() {
+    if constexpr (MODE == 0) __syncthreads();
+    else asm volatile("bar.sync 1, 256;\n" ::: "memory");
+}
+
+// Byte offset, in a tile stored in plain index order (element e at 16 e),
+// of the element that a complex128 swizzled byte offset s addresses. Linear
+// over GF(2) like the swizzle, so XOR combinations convert term by term.
+__device__ __forceinline__ uint32_t plain_off(uint32_t s) { return ops::swz(s >> 4) << 4; }
+
 // Runs the program in T on the tile at shared address tb (generic pointer
 // tile), for coset base cbase. Ends with the last stage's registers stored;
 // no trailing barrier. SM: whether the program may hold shared-memory ops.
 // D (complex128 only, may be null): with D->okL the first stage loads from
 // the state gst at coset base cbase, with D->okS the last stage stores there
 // (DirectIO); the caller then skips the tile copy in or out.
-template <typename C2, bool SM, int MAXK = 5>
+// MODE 0: the tile arrives swizzled and barriers span the CTA. MODE 1
+// (complex128, no shared-memory ops): the warp-specialised kernel; the tile
+// arrives in plain index order (bulk copies cannot permute within their
+// 256-byte runs), so the first stage loads through plain_off, and its
+// stores, which use the swizzled order, wait behind a barrier for every
+// thread's first-stage loads. D->okL is not used in this mode.
+template <typename C2, bool SM, int MAXK = 5, int MODE = 0>
 __device__ __forceinline__ void run_program(const TileTables<C2>& T, int nops, uint32_t tb, C2* tile, uint64_t cbase,
                                             const DevOp* __restrict__ sops, int sop0,
                                             const double2* __restrict__ pool, uint32_t t,
                                             const DirectIO* D = nullptr, C2* __restrict__ gst = nullptr) {
+    static_assert(MODE == 0 || (!SM && sizeof(C2) == 16), "the warp-specialised mode runs complex128 register programs");
     using A = Amp<C2>;
     using R = typename A::R;
     C2 a[16];
     bool open = false;
     bool started = false;  // a stage has been loaded
+    bool plain_open = false;  // MODE 1: the open stage was loaded from the plain-order tile
     uint32_t s0s = 0;    // store offset base of the open stage (flipped by SOP_XF)
     uint32_t lflip = 0;  // load offset flips for the next stage (SOP_XL)
     int si = 0;          // open stage's table
     auto store_regs = [&]() {
+        if constexpr (MODE == 1) {
+            if (plain_open) {
+                prog_bar<MODE>();
+                plain_open = false;
+            }
+        }
         const uint16_t* tab = T.stab[si];
         const uint32_t v0 = tab[36], v1 = tab[37], v2 = tab[38], v3 = tab[39];
 #pragma unroll
@@ -535,7 +563,21 @@ __device__ __forceinline__ void run_program(const TileTables<C2>& T, int nops, u
             const uint16_t* tab = T.stab[si];
             const uint32_t s0 = (uint32_t)tab[t & 15u] ^ (uint32_t)tab[16 + (t >> 4)];
             const uint32_t sl = s0 ^ lflip;
-            if constexpr (sizeof(C2) == 16) {
+            if constexpr (MODE == 1) {
+                if (!started) {
+                    const uint32_t p0 = plain_off(tab[32]), p1 = plain_off(tab[33]), p2 = plain_off(tab[34]),
+                                   p3 = plain_off(tab[35]), pl = plain_off(sl);
+#pragma unroll
+                    for (int j = 0; j < 16; j++) a[j] = A::lds(tb + reg_off(j, pl, p0, p1, p2, p3));
+                    started = true;
+                    plain_open = true;
+                    s0s = s0;
+                    lflip = 0;
+                    open = true;
+                    break;
+                }
+            }
+            if constexpr (sizeof(C2) == 16 && MODE == 0) {
                 if (D != nullptr && !started && D->okL) {
                     // Register and thread vectors may share tile bits (folded
                     // CNOTs), so offsets combine by XOR, never by addition.
@@ -553,7 +595,7 @@ __device__ __forceinline__ void run_program(const TileTables<C2>& T, int nops, u
             // src = 1: both stages give the same tile bits to the warp index,
             // so each warp reloads only the slots it stored.
             if (op.src == 1) __syncwarp();
-            else __syncthreads();
+            else prog_bar<MODE>();
             const uint32_t w0 = tab[32], w1 = tab[33], w2 = tab[34], w3 = tab[35];
 #pragma unroll
             for (int j = 0; j < 16; j++) a[j] = A::lds(tb + reg_off(j, sl, w0, w1, w2, w3));
@@ -572,7 +614,7 @@ __device__ __forceinline__ void run_program(const TileTables<C2>& T, int nops, u
             break;
         }
         case SOP_SMEM: {
-            if (!SM) break;
+            if constexpr (!SM) break;
             if (open) {
                 store_regs();
                 open = false;

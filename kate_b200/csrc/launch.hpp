@@ -36,6 +36,14 @@ int generic_pass_grid(int n, int m, int device);
 cudaError_t launch_tile(void* st, int prec, const PassProg& prog, const DevOp* sops, const void* pool, int grid,
                         int nbuf, cudaStream_t s);
 int tile_pass_grid(int n, int device, int nbuf, int prec);
+// Warp-specialised complex128 tile kernel (k_tile_ws.cu): one CTA per SM, a
+// producer warp streaming tiles with bulk copies into a ring of shared-memory
+// buffers. Applies to register-staged programs without shared-memory ops
+// whose tile holds physical bits 0..3. err: device int set to 1 if a bounded
+// wait gave up.
+bool tile_ws_applies(const PassProg& prog);
+int tile_ws_grid(int n, int device);
+cudaError_t launch_tile_ws(void* st, const PassProg& prog, int* err, int grid, cudaStream_t s);
 
 // Complex64 pass of 5-qubit dense blocks on the tensor cores. err: device
 // int set to 1 if a bounded wait gave up.

@@ -12,6 +12,7 @@
 #include <random>
 
 #include "devcache.hpp"
+#include "jit.hpp"
 #include "launch.hpp"
 
 namespace kate {
@@ -52,11 +53,17 @@ struct SimImpl {
     int grid = 0;
     int tile_grid = 0;
     int nbuf = 1;  // tile kernel buffering (1: two CTAs per SM, 2: one CTA, prefetching)
+    int ws_grid = 0;
+    std::vector<char> ws_ok;  // pass i runs on the warp-specialised complex128 tile kernel
+    std::vector<void*> jit_fn;  // pass i runs on its pass-specialised kernel (complex128)
+    int jit_grid_n = 0;
 
     // Launches pass i of the plan on stream st.
     cudaError_t launch_pass(size_t i, cudaStream_t st) {
         const PlannedPass& p = plan.passes[i];
         if (p.bprog) return launch_block_c64(d_state, *p.bprog, d_bimg, d_err, block_grid, st);
+        if (p.prog && i < jit_fn.size() && jit_fn[i]) return jit_launch(jit_fn[i], d_state, *p.prog, jit_grid_n, st);
+        if (p.prog && i < ws_ok.size() && ws_ok[i]) return launch_tile_ws(d_state, *p.prog, d_err, ws_grid, st);
         if (p.prog) return launch_tile(d_state, precision, *p.prog, d_sops, d_pool, tile_grid, nbuf, st);
         return launch_pass_generic(d_state, precision, hpasses[i], d_ops, d_pool, grid, st);
     }
@@ -191,6 +198,36 @@ std::string Simulator::create(const Program& prog_in, int precision, int device,
     }
     if (impl->n >= KATE_TILE_BITS) {
         impl->tile_grid = tile_pass_grid(impl->n, device, impl->nbuf, precision);
+        const char* jv = std::getenv("KATE_JIT");
+        if (precision == 0 && !(jv && std::atoi(jv) == 0)) {
+            // Pass-specialised kernels for every register-staged pass whose
+            // program the generator takes; the others keep the interpreter.
+            std::vector<std::string> srcs(impl->plan.passes.size());
+            std::vector<size_t> idx;
+            for (size_t i = 0; i < impl->plan.passes.size(); i++) {
+                const PlannedPass& p = impl->plan.passes[i];
+                if (!p.prog || p.bprog) continue;
+                srcs[i] = jit_pass_source(*p.prog, nullptr);
+                if (!srcs[i].empty()) idx.push_back(i);
+            }
+            std::vector<std::string> todo;
+            for (size_t i : idx) todo.push_back(srcs[i]);
+            std::vector<void*> fns;
+            const std::string je = jit_compile(device, todo, &fns);
+            if (!je.empty()) return fail("pass kernel compilation: " + je);
+            impl->jit_fn.assign(impl->plan.passes.size(), nullptr);
+            for (size_t k = 0; k < idx.size(); k++) impl->jit_fn[idx[k]] = fns[k];
+            impl->jit_grid_n = jit_grid(impl->n - KATE_TILE_BITS, device);
+        }
+        const char* ws = std::getenv("KATE_TILE_WS");
+        if (precision == 0 && ws && std::atoi(ws) == 1) {
+            impl->ws_grid = tile_ws_grid(impl->n, device);
+            impl->ws_ok.assign(impl->plan.passes.size(), 0);
+            for (size_t i = 0; i < impl->plan.passes.size(); i++) {
+                const PlannedPass& p = impl->plan.passes[i];
+                impl->ws_ok[i] = p.prog && !p.bprog && tile_ws_applies(*p.prog);
+            }
+        }
         if (precision == 1) impl->block_grid = block_c64_grid(impl->n, device);
     }
     impl->phys.resize(impl->n);
