@@ -225,6 +225,12 @@ KATE_API kate_status kate_sim_nqbits(kate_sim* s, int* out);
  * (capacity 16) and the number of gates it applies. */
 KATE_API kate_status kate_sim_num_passes(kate_sim* s, int* out);
 KATE_API kate_status kate_sim_get_pass(kate_sim* s, int i, int* tile_qbits, int* m, int* ngates);
+/* Kernel that runs pass i of the simulator: 0 generic shared-memory
+ * kernel, 1 register-staged interpreter, 2 pass-specialised kernel
+ * (complex128; see kate_plan_pass_source), 3 complex64 tensor-core blocks.
+ * Replaces the choice executeCommand makes per group instruction
+ * (HIPcode/simulator.hpp:760-810). */
+KATE_API kate_status kate_sim_pass_kernel(kate_sim* s, int i, int* kind);
 
 /* ---- group-pass plans (host only, no device needed) ----
  * The single-GPU replacement for gateGrouping + allocate + the per-group
@@ -251,6 +257,15 @@ KATE_API kate_status kate_plan_get_op(const kate_plan* p, int i, int* ints, uint
  * *has = 0 when the pass runs on the generic shared-memory kernel. */
 KATE_API kate_status kate_plan_get_program(const kate_plan* p, int i, void* out, size_t cap, size_t* size, int* has);
 KATE_API kate_status kate_plan_num_smem_ops(const kate_plan* p, int* out);
+/* CUDA source of the pass-specialised kernel of pass i: its register-staged
+ * program as straight-line code, compiled for sm_100a with NVRTC when a
+ * complex128 simulator is created. from_zero != 0: the form for the first
+ * pass of a run from |0...0>, which generates its input. *size = bytes with
+ * the terminating 0, copied when cap allows; KATE_EINVAL when the pass has
+ * no such kernel (the simulator then interprets its program). Replaces the
+ * reference's per-group kernel launch (HIPcode/simulator.hpp:143-218). */
+KATE_API kate_status kate_plan_pass_source(const kate_plan* p, int i, int from_zero, char* out, size_t cap,
+                                           size_t* size);
 /* Complex64 tensor-core block program of pass i (the BlockProg struct of
  * kate_b200/csrc/device_types.h) and the pool of block operand images. */
 KATE_API kate_status kate_plan_get_block_program(const kate_plan* p, int i, void* out, size_t cap, size_t* size,

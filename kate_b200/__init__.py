@@ -484,6 +484,17 @@ class Simulator:
         _check(self._lib.kate_sim_profile_passes(self._h, ms, ctypes.byref(init)))
         return init.value, [ms[i] for i in range(n.value)]
 
+    def pass_kernels(self) -> List[int]:
+        """Kernel per pass: 0 generic, 1 interpreter, 2 pass-specialised, 3 complex64 blocks."""
+        n = ctypes.c_int()
+        _check(self._lib.kate_sim_num_passes(self._h, ctypes.byref(n)))
+        out = []
+        for i in range(n.value):
+            k = ctypes.c_int()
+            _check(self._lib.kate_sim_pass_kernel(self._h, i, ctypes.byref(k)))
+            out.append(k.value)
+        return out
+
     def launches_per_run(self) -> int:
         v = ctypes.c_int()
         _check(self._lib.kate_sim_launches_per_run(self._h, ctypes.byref(v)))

@@ -62,6 +62,7 @@ SIGNATURES = {
     "kate_sim_nqbits": [_vp, _ip],
     "kate_sim_profile_passes": [_vp, _c.POINTER(_c.c_float), _c.POINTER(_c.c_float)],
     "kate_sim_launches_per_run": [_vp, _ip],
+    "kate_sim_pass_kernel": [_vp, _i, _ip],
     "kate_sim_num_passes": [_vp, _ip],
     "kate_sim_get_pass": [_vp, _i, _ip, _ip, _ip],
     "kate_plan_create": [_vp, _i, _i, _c.c_uint, _vpp],
@@ -72,6 +73,7 @@ SIGNATURES = {
     "kate_plan_get_op": [_vp, _i, _ip, _u64p, _dp],
     "kate_plan_final_layout": [_vp, _ip, _ip],
     "kate_plan_get_program": [_vp, _i, _vp, _c.c_size_t, _c.POINTER(_c.c_size_t), _ip],
+    "kate_plan_pass_source": [_vp, _i, _i, _c.c_char_p, _c.c_size_t, _c.POINTER(_c.c_size_t)],
     "kate_plan_num_smem_ops": [_vp, _ip],
     "kate_plan_get_block_program": [_vp, _i, _vp, _c.c_size_t, _c.POINTER(_c.c_size_t), _ip],
     "kate_plan_block_images": [_vp, _vp, _c.c_size_t, _c.POINTER(_c.c_size_t)],

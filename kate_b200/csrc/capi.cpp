@@ -12,6 +12,7 @@
 #include "circuit.hpp"
 #include "plan.hpp"
 #include "serve.hpp"
+#include "jit.hpp"
 #include "sim.hpp"
 
 struct kate_circuit {
@@ -499,6 +500,14 @@ kate_status kate_sim_launches_per_run(kate_sim* s, int* out) {
     return KATE_OK;
 }
 
+kate_status kate_sim_pass_kernel(kate_sim* s, int i, int* kind) {
+    REQUIRE(s && kind, "null pointer");
+    const int k = s->sim->pass_kernel(i);
+    REQUIRE(k >= 0, "pass index out of range");
+    *kind = k;
+    return KATE_OK;
+}
+
 kate_status kate_sim_nqbits(kate_sim* s, int* out) {
     REQUIRE(s && out, "null pointer");
     *out = s->sim->nqbits();
@@ -622,6 +631,19 @@ kate_status kate_plan_get_program(const kate_plan* p, int i, void* out, size_t c
     const auto& pp = p->plan.passes[i];
     *has = pp.prog ? 1 : 0;
     if (pp.prog && out && cap >= sizeof(PassProg)) std::memcpy(out, pp.prog.get(), sizeof(PassProg));
+    return KATE_OK;
+}
+
+kate_status kate_plan_pass_source(const kate_plan* p, int i, int from_zero, char* out, size_t cap, size_t* size) {
+    REQUIRE(p && size, "null pointer");
+    REQUIRE(i >= 0 && i < (int)p->plan.passes.size(), "pass index out of range");
+    const auto& pp = p->plan.passes[i];
+    REQUIRE(pp.prog != nullptr, "pass has no register-staged program");
+    std::string why;
+    const std::string src = kate::jit_pass_source(*pp.prog, &why, from_zero != 0);
+    REQUIRE(!src.empty(), "pass has no specialised kernel: " + why);
+    *size = src.size() + 1;
+    if (out && cap >= src.size() + 1) std::memcpy(out, src.c_str(), src.size() + 1);
     return KATE_OK;
 }
 

@@ -19,7 +19,6 @@ namespace kate {
 namespace {
 
 constexpr int TB = KATE_TILE_BITS;
-constexpr int OCC = 2;  // CTAs per SM (64 KiB exchange tile each, <= 128 registers)
 
 uint32_t swz(uint32_t i) { return i ^ (((i >> 3) ^ (i >> 6) ^ (i >> 9)) & 7u); }
 
@@ -150,7 +149,7 @@ bool lanes_ok(const PassProg& P, int st, const uint8_t* pos) {
 
 }  // namespace
 
-std::string jit_pass_source(const PassProg& P, std::string* why) {
+std::string jit_pass_source(const PassProg& P, std::string* why, bool from_zero, int occ) {
     auto no = [&](const char* w) {
         if (why) *why = w;
         return std::string();
@@ -182,7 +181,7 @@ std::string jit_pass_source(const PassProg& P, std::string* why) {
     const int nm = std::max(1, (int)P.nmats);
     o << kPreamble;
     o << "struct __align__(16) Mats { double2 m[" << nm << "]; };\n";
-    o << "extern \"C\" __global__ void __launch_bounds__(256, " << OCC
+    o << "extern \"C\" __global__ void __launch_bounds__(256, " << occ
       << ") kate_pass(double2* __restrict__ st, const __grid_constant__ Mats M) {\n";
     o << "  extern __shared__ __align__(16) unsigned char smem[];\n";
     o << "  const u32 tb = (u32)__cvta_generic_to_shared(smem);\n";
@@ -223,6 +222,25 @@ std::string jit_pass_source(const PassProg& P, std::string* why) {
           << ";\n";
         i = j + 1;
     }
+    if (from_zero) {
+        // The input is |0...0>: every coset but 0 is zero in and out, so its
+        // output is written without being read or computed.
+        o << "    if (c != 0) {\n      const double2 z = mk(0.0, 0.0);\n";
+        if (okS) {
+            o << "      const u64 b = cb ^ pout;\n";
+            for (int j = 0; j < 16; j++)
+                o << "      st[b ^ " << hex(slot_phys(rvec(P, last, 36, j) >> 4, g.out)) << "] = z;\n";
+        } else {
+            o << "      const u64 gb = cb ^ cdT;\n";
+            for (int j = 0; j < 16; j++) {
+                uint64_t go = 0;
+                for (int i = 0; i < 4; i++)
+                    if ((j >> i) & 1) go |= 1ull << P.tphys[8 + i];
+                o << "      st[gb ^ " << hex(go) << "] = z;\n";
+            }
+        }
+        o << "      return;\n    }\n";
+    }
     o << "    double2 a0, a1, a2, a3, a4, a5, a6, a7, a8, a9, a10, a11, a12, a13, a14, a15;\n";
     o << "    u32 lfl = 0, sfl = 0; u64 lflp = 0, sflp = 0;\n";
     bool open = false, started = false;
@@ -236,7 +254,21 @@ std::string jit_pass_source(const PassProg& P, std::string* why) {
                     o << "    sts(tb + ((s0_" << si << " ^ sfl) ^ " << hex32(rvec(P, si, 36, j)) << "), a" << j << ");\n";
             }
             si = op.idx;
-            if (!started && !okL) {
+            if (!started && from_zero) {
+                // Coset 0 of |0...0>: the amplitude at global index 0 is 1.
+                if (okL) {
+                    o << "    { const u64 b = pin ^ lflp;\n";
+                    for (int j = 0; j < 16; j++)
+                        o << "      a" << j << " = mk((b ^ " << hex(slot_phys(rvec(P, si, 32, j) >> 4, g.in))
+                          << ") == 0 ? 1.0 : 0.0, 0.0);\n";
+                } else {
+                    o << "    { const u32 sl = s0_" << si << " ^ lfl;\n";
+                    for (int j = 0; j < 16; j++)
+                        o << "      a" << j << " = mk((sl ^ " << hex32(rvec(P, si, 32, j)) << ") == 0 ? 1.0 : 0.0, 0.0);\n";
+                }
+                o << "    }\n";
+                started = true;
+            } else if (!started && !okL) {
                 o << "    { const u64 gb = cb ^ cdT;\n";
                 for (int j = 0; j < 16; j++) {
                     uint64_t go = 0;
@@ -415,6 +447,7 @@ struct Api {
     CUresult (*get_fn)(CUfunction*, CUmodule, const char*);
     CUresult (*set_attr)(CUfunction, CUfunction_attribute, int);
     CUresult (*occupancy)(int*, CUfunction, int, size_t);
+    CUresult (*get_attr)(int*, CUfunction_attribute, CUfunction);
     CUresult (*launch)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, CUstream,
                        void**, void**);
     std::string nvrtc_err, drv_err;
@@ -452,6 +485,7 @@ Api& api() {
         a.drv_ok = drv("cuModuleLoadData", (void**)&a.mod_load) && drv("cuModuleGetFunction", (void**)&a.get_fn) &&
                    drv("cuFuncSetAttribute", (void**)&a.set_attr) &&
                    drv("cuOccupancyMaxActiveBlocksPerMultiprocessor", (void**)&a.occupancy) &&
+                   drv("cuFuncGetAttribute", (void**)&a.get_attr) &&
                    drv("cuLaunchKernel", (void**)&a.launch);
         if (!a.drv_ok) a.drv_err = "CUDA driver entry points unavailable";
     });
@@ -553,6 +587,12 @@ std::string jit_compile(int device, const std::vector<std::string>& srcs, std::v
         (*fns)[i] = (void*)it->second;
     }
     return "";
+}
+
+int jit_local_bytes(void* fn) {
+    int v = 0;
+    if (!api().drv_ok || api().get_attr(&v, CU_FUNC_ATTRIBUTE_LOCAL_SIZE_BYTES, (CUfunction)fn) != CUDA_SUCCESS) return -1;
+    return v;
 }
 
 int jit_grid(int ncb, int device) {

@@ -24,13 +24,22 @@
 namespace kate {
 
 // CUDA source of the kernel for `prog`, or "" (with *why set) when the
-// program has a form the generator does not take (shared-memory ops, or a
-// first / last stage whose lanes would not read / write 256-byte runs).
-std::string jit_pass_source(const PassProg& prog, std::string* why);
+// program has a form the generator does not take (shared-memory ops, a
+// register op before the first stage). from_zero: the pass is the first of
+// a run from |0...0>; it generates its input instead of loading it (only
+// coset 0 is nonzero; every other coset's output is zero, written without
+// being read), so the run needs no separate initialisation pass.
+// occ: CTAs per SM the kernel is compiled for (launch bounds; each CTA
+// holds a 64 KiB exchange tile, so at most 3).
+std::string jit_pass_source(const PassProg& prog, std::string* why, bool from_zero = false, int occ = 2);
 
 // Compiles the sources not yet cached on `device` (in parallel) and returns
 // a kernel handle per source. Returns "" on success.
 std::string jit_compile(int device, const std::vector<std::string>& srcs, std::vector<void*>* fns);
+
+// Local memory (register spill) bytes per thread of a compiled kernel; -1
+// when unknown.
+int jit_local_bytes(void* fn);
 
 // Grid of a pass-specialised kernel for 2^ncb cosets on `device`.
 int jit_grid(int ncb, int device);

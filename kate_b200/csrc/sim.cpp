@@ -56,12 +56,15 @@ struct SimImpl {
     int ws_grid = 0;
     std::vector<char> ws_ok;  // pass i runs on the warp-specialised complex128 tile kernel
     std::vector<void*> jit_fn;  // pass i runs on its pass-specialised kernel (complex128)
+    void* jit_fn0 = nullptr;    // pass 0 generating its input |0...0> (no initialisation pass)
+    bool zero_start = false;    // the run being enqueued starts with jit_fn0
     int jit_grid_n = 0;
 
     // Launches pass i of the plan on stream st.
     cudaError_t launch_pass(size_t i, cudaStream_t st) {
         const PlannedPass& p = plan.passes[i];
         if (p.bprog) return launch_block_c64(d_state, *p.bprog, d_bimg, d_err, block_grid, st);
+        if (i == 0 && zero_start && jit_fn0) return jit_launch(jit_fn0, d_state, *p.prog, jit_grid_n, st);
         if (p.prog && i < jit_fn.size() && jit_fn[i]) return jit_launch(jit_fn[i], d_state, *p.prog, jit_grid_n, st);
         if (p.prog && i < ws_ok.size() && ws_ok[i]) return launch_tile_ws(d_state, *p.prog, d_err, ws_grid, st);
         if (p.prog) return launch_tile(d_state, precision, *p.prog, d_sops, d_pool, tile_grid, nbuf, st);
@@ -151,6 +154,11 @@ std::string Simulator::create(const Program& prog_in, int precision, int device,
         const int v = std::atoi(e);
         if (v >= 1 && v <= 8) impl->opt.coalesce = v;
     }
+    // Gates a pass may take at most (the planner packs greedily up to it).
+    if (const char* e = std::getenv("KATE_MAX_GATES")) {
+        const int v = std::atoi(e);
+        if (v >= 1 && v <= 96) impl->opt.max_gates_per_pass = v;
+    }
     std::string e = build_plan(impl->prog, impl->opt, &impl->plan);
     if (!e.empty()) return fail(e);
 
@@ -202,21 +210,54 @@ std::string Simulator::create(const Program& prog_in, int precision, int device,
         if (precision == 0 && !(jv && std::atoi(jv) == 0)) {
             // Pass-specialised kernels for every register-staged pass whose
             // program the generator takes; the others keep the interpreter.
-            std::vector<std::string> srcs(impl->plan.passes.size());
+            // Two CTAs per SM (at most 128 registers). KATE_JIT_OCC=3 asks
+            // for three (at most 80 registers; a kernel that would spill
+            // stays at two): measured slower on the layered workload (54.6
+            // against 56.8 layers/s), kept as a tuning option.
+            const char* oe = std::getenv("KATE_JIT_OCC");
+            const int occ_force = oe ? std::atoi(oe) : 0;
+            const int occ_first = occ_force == 3 ? 3 : 2;
             std::vector<size_t> idx;
+            std::vector<std::string> todo;
+            std::vector<char> zero_form;
             for (size_t i = 0; i < impl->plan.passes.size(); i++) {
                 const PlannedPass& p = impl->plan.passes[i];
                 if (!p.prog || p.bprog) continue;
-                srcs[i] = jit_pass_source(*p.prog, nullptr);
-                if (!srcs[i].empty()) idx.push_back(i);
+                std::string src = jit_pass_source(*p.prog, nullptr, false, occ_first);
+                if (src.empty()) continue;
+                idx.push_back(i);
+                todo.push_back(std::move(src));
+                zero_form.push_back(0);
             }
-            std::vector<std::string> todo;
-            for (size_t i : idx) todo.push_back(srcs[i]);
+            // Pass 0 also in the form that generates |0...0> itself.
+            const bool zero0 = !idx.empty() && idx[0] == 0;
+            if (zero0) {
+                idx.push_back(0);
+                todo.push_back(jit_pass_source(*impl->plan.passes[0].prog, nullptr, true, occ_first));
+                zero_form.push_back(1);
+            }
             std::vector<void*> fns;
-            const std::string je = jit_compile(device, todo, &fns);
+            std::string je = jit_compile(device, todo, &fns);
             if (!je.empty()) return fail("pass kernel compilation: " + je);
+            if (occ_first == 3) {
+                std::vector<size_t> redo;
+                std::vector<std::string> src2;
+                for (size_t k = 0; k < fns.size(); k++)
+                    if (jit_local_bytes(fns[k]) != 0) {
+                        redo.push_back(k);
+                        src2.push_back(jit_pass_source(*impl->plan.passes[idx[k]].prog, nullptr, zero_form[k] != 0, 2));
+                    }
+                if (!redo.empty()) {
+                    std::vector<void*> f2;
+                    je = jit_compile(device, src2, &f2);
+                    if (!je.empty()) return fail("pass kernel compilation: " + je);
+                    for (size_t r = 0; r < redo.size(); r++) fns[redo[r]] = f2[r];
+                }
+            }
+            if (zero0) idx.pop_back();
             impl->jit_fn.assign(impl->plan.passes.size(), nullptr);
             for (size_t k = 0; k < idx.size(); k++) impl->jit_fn[idx[k]] = fns[k];
+            if (zero0) impl->jit_fn0 = fns.back();
             impl->jit_grid_n = jit_grid(impl->n - KATE_TILE_BITS, device);
         }
         const char* ws = std::getenv("KATE_TILE_WS");
@@ -294,16 +335,29 @@ std::string Simulator::enqueue_init(void* stream, const double* tp) {
             P.v[1][lab][1] = ei * s0;
         }
         KCHECK(launch_init_product(S.d_state, S.n, P, S.precision, st));
+    } else if (S.jit_fn0) {
+        // The first pass writes the whole state from |0...0> itself.
+        S.zero_start = true;
+        return "";
     } else {
         KCHECK(launch_set_basis0(S.d_state, S.dim(), S.precision, st));
     }
+    S.zero_start = false;
     return "";
 }
 
 std::string Simulator::enqueue_passes(void* stream) {
     SimImpl& S = *d_;
     cudaStream_t st = (cudaStream_t)stream;
-    for (size_t i = 0; i < S.hpasses.size(); i++) KCHECK(S.launch_pass(i, st));
+    const bool zs = S.zero_start;
+    S.zero_start = false;
+    if (zs && S.hpasses.empty()) KCHECK(launch_set_basis0(S.d_state, S.dim(), S.precision, st));
+    for (size_t i = 0; i < S.hpasses.size(); i++) {
+        S.zero_start = zs && i == 0;
+        const cudaError_t ce = S.launch_pass(i, st);
+        S.zero_start = false;
+        KCHECK(ce);
+    }
     S.phys = S.plan.final_phys;
     S.has_state = true;
     return "";
@@ -516,7 +570,19 @@ std::string Simulator::profile_passes(float* ms, float* init_ms) {
     return "";
 }
 
-int Simulator::launches_per_run() const { return 1 + (int)d_->hpasses.size(); }
+int Simulator::launches_per_run() const {
+    return (d_->jit_fn0 ? 0 : 1) + (int)d_->hpasses.size();
+}
+
+int Simulator::pass_kernel(int i) const {
+    const SimImpl& S = *d_;
+    if (i < 0 || i >= (int)S.plan.passes.size()) return -1;
+    const PlannedPass& p = S.plan.passes[i];
+    if (p.bprog) return 3;
+    if (p.prog && (size_t)i < S.jit_fn.size() && S.jit_fn[i]) return 2;
+    if (p.prog) return 1;
+    return 0;
+}
 
 std::string Simulator::state_device(void** dptr, int* phys) {
     *dptr = d_->d_state;

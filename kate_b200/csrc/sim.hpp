@@ -35,6 +35,10 @@ public:
     std::string state_device(void** dptr, int* phys);
     std::string profile_passes(float* ms, float* init_ms);
     int launches_per_run() const;
+    // Kernel that runs pass i: 0 generic shared-memory kernel, 1 register-
+    // staged interpreter, 2 pass-specialised kernel, 3 complex64 tensor-core
+    // blocks; -1 for an index out of range.
+    int pass_kernel(int i) const;
 
     int nqbits() const;
     int precision() const;

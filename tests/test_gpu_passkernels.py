@@ -1,0 +1,66 @@
+"""Pass-specialised kernels on the GPU: they run every pass of complex128
+plans, give the interpreter's amplitudes (<= 1e-12; both are checked
+against the oracle elsewhere), and a run from |0...0> needs no separate
+initialisation pass."""
+import os
+
+import numpy as np
+import pytest
+
+import kate_b200 as K
+from kate_b200 import circuits
+from common import random_circuit
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+
+
+def sim_with(n, gates, jit):
+    old = os.environ.get("KATE_JIT")
+    os.environ["KATE_JIT"] = "1" if jit else "0"
+    try:
+        return K.Simulator(K.Circuit(n, gates), 1, K.C128, 0)
+    finally:
+        if old is None:
+            del os.environ["KATE_JIT"]
+        else:
+            os.environ["KATE_JIT"] = old
+
+
+@pytest.mark.parametrize("n,seed", [(16, 1), (20, 2), (22, 3)])
+def test_layered_passes_run_specialised_and_match_interpreter(n, seed, oracle):
+    gates = circuits.layered(n, 6, seed=seed)
+    a = sim_with(n, gates, True)
+    assert all(k == 2 for k in a.pass_kernels())
+    # The first pass generates |0...0>: no initialisation launch.
+    assert a.launches_per_run() == len(a.pass_kernels())
+    a.execute()
+    b = sim_with(n, gates, False)
+    assert all(k == 1 for k in b.pass_kernels())
+    b.execute()
+    sa, sb = a.state(), b.state()
+    assert np.abs(sa - sb).max() <= TOL
+    if n <= 20:
+        assert np.abs(sa - oracle.simulate(n, gates)).max() <= TOL
+
+
+def test_random_circuits_specialised_vs_oracle(oracle):
+    rng = np.random.default_rng(77)
+    for n in (12, 13, 15, 18):
+        gates = random_circuit(n, 120, rng, kinds=("h", "cnot", "crk", "toff", "d1", "diag1", "diag2"))
+        s = sim_with(n, gates, True)
+        s.execute()
+        assert np.abs(s.state() - oracle.simulate(n, gates)).max() <= TOL
+
+
+def test_from_zero_first_pass_equals_product_state_start():
+    # execute() starts from |0...0> inside the first pass; execute(proba_state)
+    # with every theta = 0 initialises the same state in a separate kernel.
+    n = 20
+    gates = circuits.layered(n, 4, seed=9)
+    s = sim_with(n, gates, True)
+    s.execute()
+    a = s.state().copy()
+    s.execute(K.proba_state(np.zeros((n, 2))))
+    b = s.state()
+    assert np.abs(a - b).max() <= TOL
