@@ -231,6 +231,15 @@ KATE_API kate_status kate_sim_get_pass(kate_sim* s, int i, int* tile_qbits, int*
  * Replaces the choice executeCommand makes per group instruction
  * (HIPcode/simulator.hpp:760-810). */
 KATE_API kate_status kate_sim_pass_kernel(kate_sim* s, int i, int* kind);
+/* Complex64 simulators renormalise the state at the end of every run:
+ * ||psi||^2 is reduced in FP64 on the device and every amplitude multiplied
+ * by 1 / ||psi|| (the tensor-core blocks' split-BF16 products do not keep
+ * the norm exactly). This returns the last run's ||psi||^2 before the
+ * rescale (how far the run drifted). KATE_ESTATE before the first run,
+ * KATE_EINVAL for complex128 simulators, which are not rescaled. No
+ * counterpart in the reference (it has no complex64 path; its measurement,
+ * HIPcode/simulator.hpp:483-543, is the FP64 reduction modelled here). */
+KATE_API kate_status kate_sim_norm2_before_renorm(kate_sim* s, double* norm2);
 
 /* ---- group-pass plans (host only, no device needed) ----
  * The single-GPU replacement for gateGrouping + allocate + the per-group
@@ -286,27 +295,37 @@ KATE_API kate_status kate_plan_final_layout(const kate_plan* p, int* phys, int* 
  * bound to a fixed budget or a memory pool it does not own, a host-language
  * binding that cannot manage device buffer lifetimes. Computes the
  * reference's per-qubit (theta, phi) of a state vector the caller already
- * holds on the current device: d_state is 2^nqbits complex128 amplitudes;
- * phys_of_label[x] (nullable: identity) is the bit of the amplitude index
- * holding program label x (kate_sim_state_device reports it);
- * final_inverse_permutation (nullable: identity) maps labels to output
- * qubits as in kate_sim_proba_state; theta_phi receives 2*nqbits doubles.
+ * holds on the current device: d_state is 2^nqbits complex128 amplitudes in
+ * a device buffer of state_bytes bytes (at least 16 * 2^nqbits; a complex64
+ * or shorter buffer returns KATE_EINVAL, as do a host pointer, another
+ * device's pointer, a pointer not 16-byte aligned, and a state that does not
+ * fit the allocation the pointer lies in); phys_of_label[x] (nullable:
+ * identity) is the bit of the amplitude index holding program label x
+ * (kate_sim_state_device reports it); final_inverse_permutation (nullable:
+ * identity) maps labels to output qubits as in kate_sim_proba_state; both
+ * must be permutations of 0..nqbits-1. theta_phi receives 2*nqbits doubles.
  * Queued on `stream` (cudaStream_t as void*, NULL = default stream) and
  * waited for before returning.
  *
  * It calls no cudaMalloc/cudaFree and no allocating library routine: its
  * scratch is one fixed __device__ array of KATE_NOALLOC_SCRATCH_BYTES bytes
- * that every GPU loading the library holds until the process exits, so
- * nqbits is limited to KATE_NOALLOC_MAX_QUBITS (larger sizes return
- * KATE_EINVAL). The first call on a device looks up the array's device
- * address (cudaGetSymbolAddress) for that device; make that first call
- * before any stream capture. The array is shared by all calls and keeps the
- * last call's contents (each call writes every slot it reads); calls that
- * overlap on the GPU race on it, so the caller must serialise them. */
+ * that every GPU where the library's device code is loaded holds until the
+ * process exits, so nqbits is limited to KATE_NOALLOC_MAX_QUBITS (larger
+ * sizes return KATE_EINVAL). With CUDA's lazy module loading (the default)
+ * the device code, and this array, is loaded on a device by the first
+ * kernel launch or symbol lookup there, which can itself need device
+ * memory: a caller that reserves all of a device's memory makes its first
+ * call there (or runs any simulator there) before reserving it. Every call
+ * looks up the array's device address (cudaGetSymbolAddress; no allocation
+ * once loaded); make the first call on a device before any stream capture.
+ * The array is shared by all calls and keeps the last call's contents (each
+ * call writes every slot it reads); calls that overlap on the GPU race on
+ * it, so the caller must serialise them. */
 #define KATE_NOALLOC_MAX_QUBITS 30
 #define KATE_NOALLOC_SCRATCH_BYTES 672704
-KATE_API kate_status kate_proba_state_noalloc(const void* d_state, int nqbits, const int* phys_of_label,
-                                              const int* final_inverse_permutation, double* theta_phi, void* stream);
+KATE_API kate_status kate_proba_state_noalloc(const void* d_state, size_t state_bytes, int nqbits,
+                                              const int* phys_of_label, const int* final_inverse_permutation,
+                                              double* theta_phi, void* stream);
 
 /* ---- device memory held for reuse ----
  * No counterpart in the reference, which allocates the state in every

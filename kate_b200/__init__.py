@@ -484,6 +484,12 @@ class Simulator:
         _check(self._lib.kate_sim_profile_passes(self._h, ms, ctypes.byref(init)))
         return init.value, [ms[i] for i in range(n.value)]
 
+    def norm2_before_renorm(self) -> float:
+        """Complex64: ||psi||^2 of the last run before it was rescaled to 1."""
+        v = ctypes.c_double()
+        _check(self._lib.kate_sim_norm2_before_renorm(self._h, ctypes.byref(v)))
+        return v.value
+
     def pass_kernels(self) -> List[int]:
         """Kernel per pass: 0 generic, 1 interpreter, 2 pass-specialised, 3 complex64 blocks."""
         n = ctypes.c_int()

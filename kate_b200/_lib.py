@@ -63,6 +63,7 @@ SIGNATURES = {
     "kate_sim_profile_passes": [_vp, _c.POINTER(_c.c_float), _c.POINTER(_c.c_float)],
     "kate_sim_launches_per_run": [_vp, _ip],
     "kate_sim_pass_kernel": [_vp, _i, _ip],
+    "kate_sim_norm2_before_renorm": [_vp, _dp],
     "kate_sim_num_passes": [_vp, _ip],
     "kate_sim_get_pass": [_vp, _i, _ip, _ip, _ip],
     "kate_plan_create": [_vp, _i, _i, _c.c_uint, _vpp],
@@ -78,7 +79,7 @@ SIGNATURES = {
     "kate_plan_get_block_program": [_vp, _i, _vp, _c.c_size_t, _c.POINTER(_c.c_size_t), _ip],
     "kate_plan_block_images": [_vp, _vp, _c.c_size_t, _c.POINTER(_c.c_size_t)],
     "kate_plan_get_smem_op": [_vp, _i, _ip, _u64p, _dp],
-    "kate_proba_state_noalloc": [_vp, _i, _ip, _ip, _dp, _vp],
+    "kate_proba_state_noalloc": [_vp, _c.c_size_t, _i, _ip, _ip, _dp, _vp],
     "kate_batch_options_default": [_vp],
     "kate_batch_autotune": [_vpp, _i, _i, _i, _vp],
     "kate_batch_create": [_vpp, _i, _i, _i, _vp, _vpp],

@@ -500,6 +500,14 @@ kate_status kate_sim_launches_per_run(kate_sim* s, int* out) {
     return KATE_OK;
 }
 
+kate_status kate_sim_norm2_before_renorm(kate_sim* s, double* norm2) {
+    REQUIRE(s && norm2, "null pointer");
+    const std::string e = s->sim->norm2_before_renorm(norm2);
+    if (e.rfind("no run", 0) == 0) return fail(KATE_ESTATE, e);
+    if (!e.empty()) return fail(e.find("complex64") != std::string::npos ? KATE_EINVAL : KATE_ECUDA, e);
+    return KATE_OK;
+}
+
 kate_status kate_sim_pass_kernel(kate_sim* s, int i, int* kind) {
     REQUIRE(s && kind, "null pointer");
     const int k = s->sim->pass_kernel(i);

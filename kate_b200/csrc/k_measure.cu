@@ -150,7 +150,93 @@ __global__ void k_probs(const S* __restrict__ st, uint64_t dim, double* __restri
     }
 }
 
+// ---- renormalisation of complex64 states ----
+// ||psi||^2 in FP64: each CTA sums |a|^2 over a grid-stride range (16-byte
+// loads, two amplitudes each, in a fixed per-thread order), reduces it in a
+// fixed tree, writes its partial; the last CTA to finish adds the partials
+// in CTA order (deterministic) and writes out[0] = ||psi||^2 and out[1] =
+// 1 / ||psi||, then resets the counter for the next run.
+constexpr int RN_GRID = 148 * 4;
+
+__global__ void __launch_bounds__(256) k_norm2_c64(const float4* __restrict__ st, uint64_t npairs,
+                                                   double* __restrict__ part, unsigned* __restrict__ count,
+                                                   double* __restrict__ out) {
+    __shared__ double red[256];
+    __shared__ bool last;
+    const uint32_t t = threadIdx.x;
+    const uint64_t stride = (uint64_t)gridDim.x * 256;
+    double acc = 0.0;
+    uint64_t i = (uint64_t)blockIdx.x * 256 + t;
+    for (; i + 3 * stride < npairs; i += 4 * stride) {
+        float4 v[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) v[k] = __ldcs(st + i + k * stride);
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            acc += ((double)v[k].x * v[k].x + (double)v[k].y * v[k].y) + ((double)v[k].z * v[k].z + (double)v[k].w * v[k].w);
+    }
+    for (; i < npairs; i += stride) {
+        const float4 v = __ldcs(st + i);
+        acc += ((double)v.x * v.x + (double)v.y * v.y) + ((double)v.z * v.z + (double)v.w * v.w);
+    }
+    red[t] = acc;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (t < (uint32_t)w) red[t] += red[t + w];
+        __syncthreads();
+    }
+    if (t == 0) {
+        part[blockIdx.x] = red[0];
+        __threadfence();
+        last = atomicAdd(count, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && t == 0) {
+        __threadfence();
+        double tot = 0.0;
+        for (uint32_t c = 0; c < gridDim.x; c++) tot += ((volatile double*)part)[c];
+        out[0] = tot;
+        out[1] = tot > 0.0 ? 1.0 / sqrt(tot) : 1.0;
+        *count = 0;
+    }
+}
+
+// Multiplies every amplitude by the scale the norm kernel wrote (read on
+// the device: no host round trip between the two launches). The product is
+// formed in FP64 and rounded once, so each amplitude carries only its own
+// rounding error; a scale rounded to FP32 first would shift the whole norm
+// by up to 2^-23.
+__global__ void __launch_bounds__(256) k_scale_c64(float4* __restrict__ st, uint64_t npairs,
+                                                   const double* __restrict__ out) {
+    const double f = out[1];
+    const uint64_t stride = (uint64_t)gridDim.x * 256;
+    for (uint64_t i = (uint64_t)blockIdx.x * 256 + threadIdx.x; i < npairs; i += stride) {
+        float4 v = __ldcs(st + i);
+        v.x = (float)((double)v.x * f);
+        v.y = (float)((double)v.y * f);
+        v.z = (float)((double)v.z * f);
+        v.w = (float)((double)v.w * f);
+        __stcs(st + i, v);
+    }
+}
+
 }  // namespace
+
+size_t renorm_scratch_bytes() { return (RN_GRID + 4) * sizeof(double); }
+
+cudaError_t launch_renorm_c64(void* st, int n, void* scratch, cudaStream_t s) {
+    if (n < 1) return cudaErrorInvalidValue;
+    const uint64_t npairs = (1ull << n) / 2;
+    double* part = (double*)scratch;
+    double* out = part + RN_GRID;
+    unsigned* count = (unsigned*)(out + 2);
+    const unsigned grid = (unsigned)(npairs < (uint64_t)RN_GRID * 256 ? (npairs + 255) / 256 : RN_GRID);
+    k_norm2_c64<<<grid, 256, 0, s>>>((const float4*)st, npairs, part, count, out);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_scale_c64<<<grid, 256, 0, s>>>((float4*)st, npairs, out);
+    return cudaGetLastError();
+}
 
 BitSumShape bitsum_shape(int n) {
     BitSumShape s{};

@@ -22,6 +22,14 @@ cudaError_t launch_pass_generic(void* st, int prec, const DevPass& p, const DevO
                                 cudaStream_t s);
 cudaError_t launch_bitsums(const void* st, int prec, int n, int kind, void* partials, cudaStream_t s);
 cudaError_t launch_probs(const void* st, int prec, uint64_t dim, double* out, cudaStream_t s);
+// Renormalisation of a complex64 state (n >= 1 qubits): ||psi||^2 reduced in
+// FP64 on the device, then every amplitude multiplied by 1 / ||psi||. The
+// scratch (renorm_scratch_bytes(), zeroed once) holds the per-CTA partials,
+// then ||psi||^2 and 1 / ||psi|| as doubles 0 and 1 after the partials
+// (offset renorm_result_offset()), then a counter.
+size_t renorm_scratch_bytes();
+constexpr size_t renorm_result_offset() { return 148 * 4 * sizeof(double); }
+cudaError_t launch_renorm_c64(void* st, int n, void* scratch, cudaStream_t s);
 
 // c128 state (double2 amplitudes)
 cudaError_t launch_set_basis0_c128(void* st, uint64_t dim, cudaStream_t s);

@@ -11,17 +11,29 @@
 //
 // The per-CTA partial sums of the reduction live in a file-scope
 // __device__ array of a fixed size (KATE_NOALLOC_SCRATCH_BYTES, about 660 KB
-// on every GPU that loads the library, held until the process exits), so
-// the call is limited to states of at most KATE_NOALLOC_MAX_QUBITS qubits.
-// The array is shared by every call and keeps the last call's contents;
-// every slot a call reads is written by the same call first, so nothing
-// needs clearing. Calls that overlap on the GPU (on different streams, or
-// from different threads) race on the array and must be serialised by the
-// caller.
+// on every GPU where the library's device code is loaded, held until the
+// process exits), so the call is limited to states of at most
+// KATE_NOALLOC_MAX_QUBITS qubits. Under CUDA's lazy module loading the
+// device code (and this array) is loaded on a device by the first kernel
+// launch or symbol lookup there, which can itself need device memory: a
+// caller that reserves all of a device's memory makes one call (or runs any
+// simulator) on it first. The array is shared by every call and keeps the
+// last call's contents; every slot a call reads is written by the same call
+// first, so nothing needs clearing. Calls that overlap on the GPU (on
+// different streams, or from different threads) race on the array and must
+// be serialised by the caller.
+//
+// The caller's pointer is checked before anything is launched: it must be
+// device memory of the current device (cudaPointerGetAttributes), 16-byte
+// aligned, and the complex128 state of 16 * 2^nqbits bytes must fit both
+// the caller's stated buffer size and the allocation the pointer lies in
+// (cuMemGetAddressRange); a complex64 or short buffer is refused instead of
+// being read past its end.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
-#include <mutex>
+#include <cstdint>
 #include <string>
 
 #include "kate_b200.h"
@@ -65,26 +77,49 @@ __global__ void k_finish(const double2* __restrict__ part, int n, int g, int nou
     out[o] = s;
 }
 
-std::mutex g_mu;
-void* g_addr[64] = {nullptr};
-
 kate_status fail(kate_status st, const std::string& m) {
     set_last_error(m);
     return st;
 }
 
+// Checks that [p, p + bytes) lies inside one device allocation (driver
+// cuMemGetAddressRange, resolved at run time). True when the range fits or
+// the driver call is unavailable.
+bool fits_allocation(const void* p, size_t bytes) {
+    using Fn = CUresult (*)(CUdeviceptr*, size_t*, CUdeviceptr);
+    static Fn fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return (Fn) nullptr;
+        return (Fn)f;
+    }();
+    if (!fn) return true;
+    CUdeviceptr base = 0;
+    size_t size = 0;
+    if (fn(&base, &size, (CUdeviceptr)(uintptr_t)p) != CUDA_SUCCESS) return false;
+    return (uint64_t)(uintptr_t)p + bytes <= (uint64_t)base + size;
+}
+
 }  // namespace
 }  // namespace kate
 
-extern "C" kate_status kate_proba_state_noalloc(const void* d_state, int nqbits, const int* phys_of_label,
-                                                const int* final_inverse_permutation, double* theta_phi,
-                                                void* stream) {
+extern "C" kate_status kate_proba_state_noalloc(const void* d_state, size_t state_bytes, int nqbits,
+                                                const int* phys_of_label, const int* final_inverse_permutation,
+                                                double* theta_phi, void* stream) {
     using namespace kate;
     if (!d_state || !theta_phi) return fail(KATE_EINVAL, "null state or output pointer");
     if (nqbits < 1 || nqbits > KATE_NOALLOC_MAX_QUBITS)
         return fail(KATE_EINVAL, "kate_proba_state_noalloc handles 1 to " +
                                      std::to_string(KATE_NOALLOC_MAX_QUBITS) + " qubits (fixed scratch size)");
     const int n = nqbits;
+    const size_t need = (size_t)16 << n;
+    if (state_bytes < need)
+        return fail(KATE_EINVAL, "state_bytes " + std::to_string(state_bytes) + " is below the " +
+                                     std::to_string(need) + " bytes of a complex128 state of " + std::to_string(n) +
+                                     " qubits (complex64 states are not accepted)");
+    if (((uintptr_t)d_state & 15u) != 0) return fail(KATE_EINVAL, "d_state is not 16-byte aligned");
     int phys[KATE_NOALLOC_MAX_QUBITS];
     bool seen[KATE_NOALLOC_MAX_QUBITS] = {false};
     for (int x = 0; x < n; x++) {
@@ -92,23 +127,33 @@ extern "C" kate_status kate_proba_state_noalloc(const void* d_state, int nqbits,
         if (phys[x] < 0 || phys[x] >= n || seen[phys[x]]) return fail(KATE_EINVAL, "phys_of_label is not a permutation");
         seen[phys[x]] = true;
     }
+    if (final_inverse_permutation) {
+        bool out_seen[KATE_NOALLOC_MAX_QUBITS] = {false};
+        for (int x = 0; x < n; x++) {
+            const int o = final_inverse_permutation[x];
+            if (o < 0 || o >= n || out_seen[o]) return fail(KATE_EINVAL, "final_inverse_permutation is not a permutation");
+            out_seen[o] = true;
+        }
+    }
     int dev = 0;
     cudaError_t ce = cudaGetDevice(&dev);
     if (ce != cudaSuccess) return fail(KATE_ECUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(ce));
-    if (dev < 0 || dev >= 64) return fail(KATE_EINVAL, "device index above 63");
-    void* scratch = nullptr;
-    {
-        // Set-up, once per device: the device address of the scratch array.
-        std::lock_guard<std::mutex> lk(g_mu);
-        if (!g_addr[dev]) {
-            ce = cudaGetSymbolAddress(&g_addr[dev], g_scratch);
-            if (ce != cudaSuccess) {
-                g_addr[dev] = nullptr;
-                return fail(KATE_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(ce));
-            }
-        }
-        scratch = g_addr[dev];
+    cudaPointerAttributes attr;
+    ce = cudaPointerGetAttributes(&attr, d_state);
+    if (ce != cudaSuccess) {
+        cudaGetLastError();
+        return fail(KATE_EINVAL, std::string("d_state is not a CUDA pointer: ") + cudaGetErrorString(ce));
     }
+    if ((attr.type != cudaMemoryTypeDevice && attr.type != cudaMemoryTypeManaged) || attr.device != dev)
+        return fail(KATE_EINVAL, "d_state is not device memory of the current device");
+    if (!fits_allocation(d_state, need))
+        return fail(KATE_EINVAL, "the " + std::to_string(need) + "-byte state does not fit the allocation d_state lies in");
+    // The scratch array's device address on this device (looked up on every
+    // call: no allocation once the module is loaded, and it stays valid
+    // across a cudaDeviceReset).
+    void* scratch = nullptr;
+    ce = cudaGetSymbolAddress(&scratch, g_scratch);
+    if (ce != cudaSuccess) return fail(KATE_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(ce));
     double2* part = (double2*)scratch;
     double2* fin = part + kPartials;
     const int g = n <= 12 ? 0 : (n - 12 < kGridBits ? n - 12 : kGridBits);

@@ -45,6 +45,8 @@ struct SimImpl {
     void* d_part = nullptr;
     void* d_bimg = nullptr;   // complex64 block operand images
     int* d_err = nullptr;     // set by kernels whose bounded waits gave up
+    void* d_norm = nullptr;   // complex64: renormalisation scratch and result
+    bool renormed = false;    // a complex64 run has been renormalised
     size_t part_bytes = 0;
     std::vector<DevPass> hpasses;
     cudaStream_t stream = nullptr;
@@ -190,6 +192,11 @@ std::string Simulator::create(const Program& prog_in, int precision, int device,
     if (ce != cudaSuccess) return fail(cuda_err("cudaMalloc(block images)", ce));
     if (!impl->plan.bimg.empty())
         cudaMemcpy(impl->d_bimg, impl->plan.bimg.data(), impl->plan.bimg.size(), cudaMemcpyHostToDevice);
+    if (precision == 1) {
+        ce = cudaMalloc(&impl->d_norm, renorm_scratch_bytes());
+        if (ce != cudaSuccess) return fail(cuda_err("cudaMalloc(renormalisation)", ce));
+        cudaMemset(impl->d_norm, 0, renorm_scratch_bytes());
+    }
     ce = cudaMalloc(&impl->d_err, sizeof(int));
     if (ce != cudaSuccess) return fail(cuda_err("cudaMalloc(error flag)", ce));
     cudaMemset(impl->d_err, 0, sizeof(int));
@@ -290,6 +297,7 @@ Simulator::~Simulator() {
     cudaFree(d_->d_part);
     cudaFree(d_->d_bimg);
     cudaFree(d_->d_err);
+    cudaFree(d_->d_norm);
     if (d_->stream) cudaStreamDestroy(d_->stream);
     delete d_;
 }
@@ -357,6 +365,11 @@ std::string Simulator::enqueue_passes(void* stream) {
         const cudaError_t ce = S.launch_pass(i, st);
         S.zero_start = false;
         KCHECK(ce);
+    }
+    if (S.precision == 1) {
+        // Complex64: ||psi|| in FP64, then the state rescaled to norm 1.
+        KCHECK(launch_renorm_c64(S.d_state, S.n, S.d_norm, st));
+        S.renormed = true;
     }
     S.phys = S.plan.final_phys;
     S.has_state = true;
@@ -571,7 +584,17 @@ std::string Simulator::profile_passes(float* ms, float* init_ms) {
 }
 
 int Simulator::launches_per_run() const {
-    return (d_->jit_fn0 ? 0 : 1) + (int)d_->hpasses.size();
+    return (d_->jit_fn0 ? 0 : 1) + (int)d_->hpasses.size() + (d_->precision == 1 ? 2 : 0);
+}
+
+std::string Simulator::norm2_before_renorm(double* out) {
+    SimImpl& S = *d_;
+    if (S.precision != 1) return "only complex64 simulators are renormalised";
+    if (!S.renormed) return "no run has been renormalised yet";
+    KCHECK(cudaSetDevice(S.device));
+    KCHECK(cudaStreamSynchronize(S.stream));
+    KCHECK(cudaMemcpy(out, (const char*)S.d_norm + renorm_result_offset(), sizeof(double), cudaMemcpyDeviceToHost));
+    return "";
 }
 
 int Simulator::pass_kernel(int i) const {

@@ -39,6 +39,9 @@ public:
     // staged interpreter, 2 pass-specialised kernel, 3 complex64 tensor-core
     // blocks; -1 for an index out of range.
     int pass_kernel(int i) const;
+    // Complex64: ||psi||^2 of the last run's state before it was rescaled to
+    // norm 1 (FP64 reduction on the device).
+    std::string norm2_before_renorm(double* out);
 
     int nqbits() const;
     int precision() const;
