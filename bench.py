@@ -96,11 +96,29 @@ def parse():
     return a
 
 
+L2_BYTES = 126 << 20
+
+
+def l2_flush_buffer(n, dev, amp_bytes=16):
+    """A buffer twice the L2 size to write between timed steps when the
+    state (amp_bytes * 2^n) is smaller than 128 MiB; None otherwise."""
+    import torch
+    if (amp_bytes << n) >= (128 << 20):
+        return None
+    return torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
+
+
+def l2_note(n, amp_bytes=16):
+    if (amp_bytes << n) >= (128 << 20):
+        return "state larger than L2 (126 MB); no flush needed"
+    return "state smaller than L2: each timed step follows a 252 MB buffer write (L2 flushed), timed on its own"
+
+
 def workload_config(args):
     return {"workload": f"layered RX/RZ/CNOT-ladder circuit, n={args.nqubits}, {args.layers} layers, complex128",
             "nqubits": args.nqubits, "layers": args.layers, "seed": args.seed,
             "gates": args.layers * (3 * args.nqubits - 1), "state_bytes": 16 << args.nqubits,
-            "l2": "state larger than L2 (126 MB); no flush needed", "parallelism": "replicas"}
+            "l2": l2_note(args.nqubits), "parallelism": "replicas"}
 
 
 class Clocks:
@@ -230,14 +248,24 @@ def replica_rate(units_per_rank, ms_max, world):
     return world * units_per_rank / (ms_max / 1000.0)
 
 
-def cpu_reference_sample(n, seed):
-    """Times one layer of the n-qubit circuit on the reference's CPU simulator."""
+def ref_sample_layers(n, L):
+    """Layers of the circuit one CPU-reference step runs: the whole circuit
+    when it is small (seconds at n <= 22, e.g. the 20-qubit 10-layer
+    configuration), else one layer of it (a 30-qubit layer takes about 20 s
+    on 16 cores; the whole circuit would take minutes)."""
+    return L if n <= 22 else 1
+
+
+def cpu_reference_sample(n, seed, L=1):
+    """Times the reference's CPU simulator on ref_sample_layers(n, L) layers
+    of the n-qubit circuit."""
     from kate_b200 import circuits
     from oracle.oracle import Ref, available_ref
 
     if available_ref():
         ref = Ref()
-        c = ref.circuit(n, circuits.layered(n, 1, seed))
+        ls = ref_sample_layers(n, L)
+        c = ref.circuit(n, circuits.layered(n, ls, seed))
         c.schedule()
         c.fuse(5, 1e-6)
         c.group(12)
@@ -245,10 +273,10 @@ def cpu_reference_sample(n, seed):
         sess = c.session()
         ms = sess.run()
         sess.close()
-        return {"value": 1000.0 / ms, "unit": UNIT, "cores": ref.hw_threads(), "kind": "reference",
-                "sample": f"1 layer of the n={n} circuit ({3 * n - 1} gates) on the reference CPUSimulator "
-                          f"(gateScheduling+gateFusion(5)+gateGrouping(12)), gate phase only",
-                "ms_per_layer": ms}
+        return {"value": ls * 1000.0 / ms, "unit": UNIT, "cores": ref.hw_threads(), "kind": "reference",
+                "sample": f"{ls} layer(s) of the n={n} circuit ({ls * (3 * n - 1)} gates) on the reference "
+                          f"CPUSimulator (gateScheduling+gateFusion(5)+gateGrouping(12)), gate phase only",
+                "ms_per_layer": ms / ls}
     from oracle.oracle import Oracle
     o = Oracle()
     nn = min(n, 26)
@@ -311,7 +339,8 @@ def run_reference(args):
                           "(the reference headers were absent at build time)"}))
         return
     ref = Ref()
-    c = ref.circuit(n, circuits.layered(n, 1, args.seed))
+    ls = ref_sample_layers(n, args.layers)
+    c = ref.circuit(n, circuits.layered(n, ls, args.seed))
     c.schedule()
     c.fuse(5, 1e-6)
     c.group(12)
@@ -322,16 +351,19 @@ def run_reference(args):
     times = [sess.run() for _ in range(args.steps)]
     sess.close()
     total_ms = sum(times)
-    value = args.steps * 1000.0 / total_ms
+    value = args.steps * ls * 1000.0 / total_ms
     cores = ref.hw_threads()
+    sample = (f"each step = {ls} layer(s) of the n={n} circuit (the same seeded angles; "
+              f"{'the whole circuit' if ls == args.layers else 'one layer, planned on its own'}) on the "
+              f"reference CPUSimulator (gateScheduling+gateFusion(5)+gateGrouping(12)), gate phase only, "
+              f"{cores} threads")
+    cfg = dict(workload_config(args), reference_sample=sample)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c128 (f64)", "data": "synthetic",
-            "impl": "reference", "config": workload_config(args),
+            "impl": "reference", "config": cfg,
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
-                             "sample": f"each step = 1 layer of the n={n} circuit on the reference "
-                                       f"CPUSimulator (gateScheduling+gateFusion(5)+gateGrouping(12)), "
-                                       f"gate phase only, {cores} threads"},
+                             "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -379,14 +411,29 @@ def main():
     torch.cuda.synchronize()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
+    flush = l2_flush_buffer(n, dev)
     with Clocks(local) as clk:
-        ev0.record(stream)
-        for _ in range(args.steps):
-            sim.run_async(stream.cuda_stream)
-        ev1.record(stream)
-        ev1.synchronize()
+        if flush is None:
+            ev0.record(stream)
+            for _ in range(args.steps):
+                sim.run_async(stream.cuda_stream)
+            ev1.record(stream)
+            ev1.synchronize()
+            ms = ev0.elapsed_time(ev1)
+        else:
+            # A state smaller than L2: each step timed on its own, after a
+            # write of a buffer twice the L2 size (outside the events).
+            ms = 0.0
+            for _ in range(args.steps):
+                with torch.cuda.stream(stream):
+                    flush.fill_(1)
+                ev0.record(stream)
+                sim.run_async(stream.cuda_stream)
+                ev1.record(stream)
+                ev1.synchronize()
+                ms += ev0.elapsed_time(ev1)
     torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1)
+    del flush
     if dist:
         ms = max_over_ranks(ms, dev)
     ms_per_step = ms / args.steps
@@ -439,7 +486,7 @@ def main():
         del sim
         torch.cuda.empty_cache()
         try:
-            cpu = cpu_reference_sample(n, args.seed)
+            cpu = cpu_reference_sample(n, args.seed, L)
         except Exception as e:  # reported, not fatal
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {e}"}
 

@@ -249,6 +249,7 @@ KATE_API kate_status kate_sim_norm2_before_renorm(kate_sim* s, double* norm2);
 #define KATE_PLAN_NO_REMAP 1u   /* keep the low physical bits fixed */
 #define KATE_PLAN_NO_FUSE1Q 2u  /* do not multiply single-qubit chains */
 #define KATE_PLAN_C64 4u        /* complex64 plan: dense 5-qubit tensor-core blocks */
+#define KATE_PLAN_NO_DENSE2 8u  /* dense two-qubit gates as shared-memory ops, not register ops */
 KATE_API kate_status kate_plan_create(const kate_circuit* c, int max_tile, int coalesce, unsigned flags,
                                       kate_plan** out);
 KATE_API kate_status kate_plan_destroy(kate_plan* p);

@@ -82,11 +82,13 @@ def build(verbose: bool = False) -> str:
 
 def build_oracle(with_ref: bool = True, verbose: bool = False) -> None:
     """Compiles oracle/libkate_oracle.so and, when the reference headers are
-    present, oracle/_ref/libkate_ref.so and oracle/_ref/libkate_ref_gpu.so
-    (test and measurement infrastructure)."""
+    present (the tree in KATE_REF_DIR, default the reference checkout this
+    build was written against), oracle/_ref/libkate_ref.so and
+    oracle/_ref/libkate_ref_gpu.so (test and measurement infrastructure)."""
     targets = ["oracle"]
-    if with_ref and os.path.exists("/root/reference/Kate.hpp"):
-        targets += ["ref", "refgpu"]
+    ref_dir = os.environ.get("KATE_REF_DIR", "/root/reference")
+    if with_ref and os.path.exists(os.path.join(ref_dir, "Kate.hpp")):
+        targets += ["ref", "refgpu", f"REF={ref_dir}"]
     r = subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), *targets], capture_output=True, text=True)
     if verbose:
         print(r.stdout, r.stderr)

@@ -555,6 +555,7 @@ kate_status kate_plan_create(const kate_circuit* c, int max_tile, int coalesce, 
         opt.remap = !(flags & KATE_PLAN_NO_REMAP);
         opt.fuse_1q = !(flags & KATE_PLAN_NO_FUSE1Q);
         opt.c64 = (flags & KATE_PLAN_C64) != 0;
+        opt.dense2_reg = !opt.c64 && !(flags & KATE_PLAN_NO_DENSE2);
         auto* p = new kate_plan();
         std::string e = kate::build_plan(prog, opt, &p->plan);
         if (!e.empty()) {

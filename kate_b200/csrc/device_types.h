@@ -53,6 +53,10 @@ typedef struct {
 #define SOP_URB 14   // x0' = t0 x0 + x1,     x1' = t1 x1 - x0      (real [[a, b], [-b, d]] / b)
 #define SOP_UXA 15   // x0' = x0 + i t0 x1,   x1' = x1 + i t1 x0    ([[a, ib], [ic, a]] / a)
 #define SOP_UXB 16   // x0' = x1 - i t0 x0,   x1' = x0 - i t1 x1    ([[a, ib], [ib, d]] / (ib))
+// Dense two-qubit gate on register bits a (local index bit 0) and src (bit
+// 1), a < src; matrix mats[idx .. idx+15] (4x4 complex, row-major). Only in
+// complex128 plans (PlanOptions::dense2_reg).
+#define SOP_U2 17
 
 #define SRC_REG 0
 #define SRC_THR 1

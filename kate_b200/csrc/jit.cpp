@@ -87,6 +87,27 @@ static __device__ __forceinline__ double2 row2(double2 u0, double2 u1, double2 x
     r.y = fma(u1.y, y.x, r.y);
     return r;
 }
+static __device__ __forceinline__ double2 row4(double2 u0, double2 u1, double2 u2, double2 u3, double2 x0, double2 x1,
+                                                double2 x2, double2 x3) {
+    double2 r;
+    r.x = u0.x * x0.x;
+    r.x = fma(-u0.y, x0.y, r.x);
+    r.x = fma(u1.x, x1.x, r.x);
+    r.x = fma(-u1.y, x1.y, r.x);
+    r.x = fma(u2.x, x2.x, r.x);
+    r.x = fma(-u2.y, x2.y, r.x);
+    r.x = fma(u3.x, x3.x, r.x);
+    r.x = fma(-u3.y, x3.y, r.x);
+    r.y = u0.x * x0.y;
+    r.y = fma(u0.y, x0.x, r.y);
+    r.y = fma(u1.x, x1.y, r.y);
+    r.y = fma(u1.y, x1.x, r.y);
+    r.y = fma(u2.x, x2.y, r.y);
+    r.y = fma(u2.y, x2.x, r.y);
+    r.y = fma(u3.x, x3.y, r.y);
+    r.y = fma(u3.y, x3.x, r.y);
+    return r;
+}
 static __device__ __forceinline__ double2 lds(u32 a) {
     double2 v;
     asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"(a));
@@ -360,6 +381,20 @@ std::string jit_pass_source(const PassProg& P, std::string* why, bool from_zero,
                     o << aj << " = mk(fma(" << t0 << ", x.y, y.x), fma(-" << t0 << ", x.x, y.y)); " << ak << " = mk(fma("
                       << t1 << ", y.y, x.x), fma(-" << t1 << ", y.x, x.y)); ";
             });
+            break;
+        }
+        case SOP_U2: {
+            const int i = op.idx, A = 1 << op.a, B = 1 << op.src;
+            for (int j = 0; j < 16; j++) {
+                if ((j & A) || (j & B)) continue;
+                const int r[4] = {j, j | A, j | B, j | A | B};
+                o << "    { const double2 x0 = a" << r[0] << ", x1 = a" << r[1] << ", x2 = a" << r[2] << ", x3 = a"
+                  << r[3] << ";\n";
+                for (int row = 0; row < 4; row++)
+                    o << "      a" << r[row] << " = row4(" << g.m(i + 4 * row) << ", " << g.m(i + 4 * row + 1) << ", "
+                      << g.m(i + 4 * row + 2) << ", " << g.m(i + 4 * row + 3) << ", x0, x1, x2, x3);\n";
+                o << "    }\n";
+            }
             break;
         }
         case SOP_H:

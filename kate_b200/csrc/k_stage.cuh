@@ -96,6 +96,30 @@ __device__ __forceinline__ void reg_u(C2 (&a)[16], C2 u00, C2 u01, C2 u10, C2 u1
     }
 }
 
+// Dense two-qubit gate on register bits A (matrix index bit 0) and B (bit
+// 1), matrix M (4x4 row-major, complex128 only).
+template <int A, int B>
+__device__ __forceinline__ void reg_u2(double2 (&a)[16], const double2* M) {
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+        if (((j >> A) & 1) || ((j >> B) & 1)) continue;
+        const int r1 = j | (1 << A), r2 = j | (1 << B), r3 = j | (1 << A) | (1 << B);
+        const double2 x0 = a[j], x1 = a[r1], x2 = a[r2], x3 = a[r3];
+        double2 y[4];
+#pragma unroll
+        for (int row = 0; row < 4; row++) {
+            y[row] = cmul(M[4 * row], x0);
+            cfma(y[row], M[4 * row + 1], x1);
+            cfma(y[row], M[4 * row + 2], x2);
+            cfma(y[row], M[4 * row + 3], x3);
+        }
+        a[j] = y[0];
+        a[r1] = y[1];
+        a[r2] = y[2];
+        a[r3] = y[3];
+    }
+}
+
 template <int B, typename C2>
 __device__ __forceinline__ void reg_h(C2 (&a)[16]) {
     using R = typename Amp<C2>::R;
@@ -670,6 +694,20 @@ __device__ __forceinline__ void run_program(const TileTables<C2>& T, int nops, u
             else if (op.kind == SOP_URB) reg_rot_bit<1>(a, op.a, t0, t1);
             else if (op.kind == SOP_UXA) reg_rot_bit<2>(a, op.a, t0, t1);
             else reg_rot_bit<3>(a, op.a, t0, t1);
+            break;
+        }
+        case SOP_U2: {
+            if constexpr (sizeof(C2) == 16) {
+                const double2* M = reinterpret_cast<const double2*>(&T.mats[op.idx]);
+                switch (op.a * 4 + op.src) {
+                case 1: reg_u2<0, 1>(a, M); break;
+                case 2: reg_u2<0, 2>(a, M); break;
+                case 3: reg_u2<0, 3>(a, M); break;
+                case 6: reg_u2<1, 2>(a, M); break;
+                case 7: reg_u2<1, 3>(a, M); break;
+                default: reg_u2<2, 3>(a, M); break;
+                }
+            }
             break;
         }
         case SOP_H: {

@@ -353,6 +353,7 @@ std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out) {
     const int n = prog.nqbits;
     plan = Plan();
     plan.n = n;
+    plan.dense2_reg = opt.dense2_reg && !opt.c64;
     plan.initial_permutation = prog.initial_permutation;
     plan.final_inverse_permutation = prog.final_inverse_permutation;
     std::vector<int> lab2log(n);
@@ -506,7 +507,17 @@ std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out) {
             }
         } else if (opt.staged) {
             auto prog = std::make_shared<PassProg>();
-            pp.prog_note = build_pass_program(plan, pp, n, plan.smem_ops, plan.pool, prog.get());
+            // Dense two-qubit gates as register ops when asked for; a pass
+            // whose program would then not fit the kernel parameter keeps
+            // them as shared-memory ops.
+            const size_t so = plan.smem_ops.size(), po = plan.pool.size();
+            pp.prog_note = opt.dense2_reg ? build_pass_program(plan, pp, n, plan.smem_ops, plan.pool, prog.get(), true)
+                                          : std::string("off");
+            if (!pp.prog_note.empty()) {
+                plan.smem_ops.resize(so);
+                plan.pool.resize(po);
+                pp.prog_note = build_pass_program(plan, pp, n, plan.smem_ops, plan.pool, prog.get(), false);
+            }
             if (pp.prog_note.empty()) pp.prog = prog;
         }
         plan.passes.push_back(std::move(pp));

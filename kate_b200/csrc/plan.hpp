@@ -40,6 +40,7 @@ struct PlanOptions {
     bool staged = true;  // build register-staged programs for the tile kernel
     bool c64 = false;    // complex64 state: passes become dense 5-qubit tensor-core blocks
     int max_gates_per_pass = 96;  // keeps a pass program within the kernel parameter
+    bool dense2_reg = false;  // dense two-qubit gates as register ops (SOP_U2) rather than shared-memory ops
 };
 
 struct PlannedPass {
@@ -66,6 +67,7 @@ struct PGate {
 
 struct Plan {
     int n = 0;
+    bool dense2_reg = false;         // PlanOptions::dense2_reg of the plan
     std::vector<PGate> pgates;
     std::vector<PlannedPass> passes;
     std::vector<int> final_phys;     // logical qubit -> physical bit after the last pass
@@ -87,7 +89,7 @@ std::vector<PlannedPass> plan_relayout(int n, const std::vector<int>& phys, cons
 // Register-staged program of a pass (12-qubit tiles). Non-register ops are
 // appended to smem_ops (their tables to pool). Returns "" on success.
 std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n, std::vector<DevOp>& smem_ops,
-                               std::vector<Cx>& pool, PassProg* out);
+                               std::vector<Cx>& pool, PassProg* out, bool dense2 = false);
 
 // Complex64 block program of a pass (12-qubit tiles); operand images are
 // appended to `pool`. Returns "" on success.

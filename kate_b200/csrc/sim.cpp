@@ -151,6 +151,12 @@ std::string Simulator::create(const Program& prog_in, int precision, int device,
         if (!e.empty()) return fail(e);
     }
     impl->opt.c64 = precision == 1;
+    {
+        // Dense two-qubit gates as register ops for complex128, where the
+        // pass-specialised kernels run them straight-line.
+        const char* jv = std::getenv("KATE_JIT");
+        impl->opt.dense2_reg = precision == 0 && !(jv && std::atoi(jv) == 0);
+    }
     // Contiguous low physical bits every tile holds (runs of 2^c amplitudes per access).
     if (const char* e = std::getenv("KATE_COALESCE")) {
         const int v = std::atoi(e);

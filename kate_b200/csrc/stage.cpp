@@ -22,6 +22,8 @@ namespace {
 struct LOp {
     int kind = 0;        // SOP_*
     int tgt = -1;        // target tile bit
+    int tgt2 = -1;       // U2: second target tile bit (matrix index bit 1)
+    Cx m2[16];           // U2: 4x4 matrix, row-major
     uint32_t tctl = 0;   // control tile bits
     uint64_t pctl = 0;   // control coset (physical) bits
     int dtile = -1;      // D1: tile bit, or -1
@@ -125,7 +127,7 @@ int classify_2x2(const Cx* m) {
 }
 
 std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n, std::vector<DevOp>& smem_ops,
-                               std::vector<Cx>& pool, PassProg* out) {
+                               std::vector<Cx>& pool, PassProg* out, bool dense2) {
     const int m = (int)pass.phys_in.size();
     if (m != KATE_TILE_BITS) return "register-staged kernel needs 12-qubit tiles";
     const std::vector<int>& phys = pass.phys_before;
@@ -153,6 +155,12 @@ std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n,
             o.kind = classify_2x2(g.table.data());
             o.tgt = tile_bit(g.tq[0]);
             for (int i = 0; i < 4; i++) o.m[i] = g.table[i];
+        } else if (g.kind == OPK_DENSE && g.tq.size() == 2 && dense2) {
+            o.kind = SOP_U2;
+            o.tgt = tile_bit(g.tq[0]);
+            o.tgt2 = tile_bit(g.tq[1]);
+            for (int i = 0; i < 16; i++) o.m2[i] = g.table[i];
+            if (o.tgt2 < 0) return "internal: target outside the tile";
         } else if (g.kind == OPK_H) {
             o.kind = SOP_H;
             o.tgt = tile_bit(g.tq[0]);
@@ -222,7 +230,8 @@ std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n,
             o.smem = (int)smem_ops.size();
             smem_ops.push_back(one.ops[0]);
         }
-        if ((o.kind == SOP_U || o.kind == SOP_UR || o.kind == SOP_UX || o.kind == SOP_H || o.kind == SOP_X) &&
+        if ((o.kind == SOP_U || o.kind == SOP_UR || o.kind == SOP_UX || o.kind == SOP_H || o.kind == SOP_X ||
+             o.kind == SOP_U2) &&
             o.tgt < 0)
             return "internal: target outside the tile";
         L.push_back(std::move(o));
@@ -277,18 +286,26 @@ std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n,
             if (!base[i] && c == 0) rdy.push_back(i);
         }
         auto in_R = [&](int t) { return std::find(R.begin(), R.end(), t) != R.end(); };
+        // Targets of op i not yet register bits (-1 entries ignored).
+        auto missing = [&](int i) {
+            int c = 0;
+            if (L[i].tgt >= 0 && !in_R(L[i].tgt)) c++;
+            if (L[i].tgt2 >= 0 && !in_R(L[i].tgt2)) c++;
+            return c;
+        };
         for (;;) {
             size_t at = rdy.size();
             for (size_t k = 0; k < rdy.size() && at == rdy.size(); k++) {
                 const int i = rdy[k];
-                if (regable(i) && (L[i].tgt < 0 || in_R(L[i].tgt))) at = k;
+                if (regable(i) && missing(i) == 0) at = k;
             }
             if (at == rdy.size() && R.size() < 4)
                 for (size_t k = 0; k < rdy.size() && at == rdy.size(); k++) {
                     const int i = rdy[k];
-                    if (regable(i) && L[i].tgt >= 0) {
+                    if (regable(i) && L[i].tgt >= 0 && R.size() + missing(i) <= 4) {
                         at = k;
-                        R.push_back(L[i].tgt);
+                        if (!in_R(L[i].tgt)) R.push_back(L[i].tgt);
+                        if (L[i].tgt2 >= 0 && !in_R(L[i].tgt2)) R.push_back(L[i].tgt2);
                     }
                 }
             if (at == rdy.size()) break;
@@ -414,14 +431,19 @@ std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n,
         // stage before it, and the store suffix when it commutes with every
         // kept op after it. Ops commute when neither's target is a qubit the
         // other touches (controls and diagonals only read the Z basis).
-        auto touched = [&](const LOp& o) {
-            uint32_t m2 = o.tctl;
+        auto targets = [&](const LOp& o) {
+            uint32_t m2 = 0;
             if (o.tgt >= 0) m2 |= 1u << o.tgt;
+            if (o.tgt2 >= 0) m2 |= 1u << o.tgt2;
+            return m2;
+        };
+        auto touched = [&](const LOp& o) {
+            uint32_t m2 = o.tctl | targets(o);
             if (o.dtile >= 0) m2 |= 1u << o.dtile;
             return m2;
         };
         auto commute = [&](const LOp& a, const LOp& b) {
-            return (a.tgt < 0 || !((touched(b) >> a.tgt) & 1u)) && (b.tgt < 0 || !((touched(a) >> b.tgt) & 1u));
+            return !(targets(a) & touched(b)) && !(targets(b) & touched(a));
         };
         auto reg_ctl = [&](const LOp& o) {
             return o.pctl == 0 && __builtin_popcount(o.tctl) == 1 && in_R(__builtin_ctz(o.tctl));
@@ -561,7 +583,21 @@ std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n,
             SOp s{};
             s.kind = (uint8_t)o.kind;
             if (o.tgt >= 0 && dr_support && ((dr_support >> regpos(o.tgt)) & 1u)) dr_flush();
+            if (o.tgt2 >= 0 && dr_support && ((dr_support >> regpos(o.tgt2)) & 1u)) dr_flush();
             switch (o.kind) {
+            case SOP_U2: {
+                // Register bits a < src; with the targets the other way round
+                // the matrix's index bits 0 and 1 trade places.
+                int r0 = regpos(o.tgt), r1 = regpos(o.tgt2);
+                const bool swap = r0 > r1;
+                s.a = (uint8_t)(swap ? r1 : r0);
+                s.src = (uint8_t)(swap ? r0 : r1);
+                s.idx = (uint16_t)mats.size();
+                auto sw = [&](int v) { return swap ? (((v & 1) << 1) | ((v >> 1) & 1)) : v; };
+                for (int r = 0; r < 4; r++)
+                    for (int c = 0; c < 4; c++) mats.push_back(o.m2[4 * sw(r) + sw(c)]);
+                break;
+            }
             case SOP_U:
             case SOP_UR:
             case SOP_UX:

@@ -279,6 +279,17 @@ class PlanView:
                         if kind == 10:  # DR: diagonal over the register bits
                             a *= mats[int(op["idx"]):int(op["idx"]) + 16][None, None, :]
                             continue
+                        if kind == 17:  # U2: 4x4 on register bits a (index bit 0) and src (bit 1)
+                            A, Bb = 1 << int(op["a"]), 1 << int(op["src"])
+                            assert int(op["a"]) < int(op["src"])
+                            u = mats[int(op["idx"]):int(op["idx"]) + 16].reshape(4, 4)
+                            base = jj[((jj & A) == 0) & ((jj & Bb) == 0)]
+                            cols = [base, base | A, base | Bb, base | A | Bb]
+                            x = np.stack([a[:, :, c] for c in cols], axis=-1)  # (C, 256, 4 groups, 4)
+                            y = x @ u.T
+                            for r in range(4):
+                                a[:, :, cols[r]] = y[..., r]
+                            continue
                         if kind in (8, 9):  # real / RX-form 2x2: same arithmetic as U here
                             kind = 3
                         if kind in (13, 14, 15, 16):  # rotations with their factor taken out

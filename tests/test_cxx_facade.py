@@ -42,11 +42,28 @@ def test_facade_builds_and_runs_the_passes(facade_exe):
     assert vals == pytest.approx([2.0, 0.0, -0.16, 2.88, np.pi / 4], abs=1e-6)  # printed to 6 digits
 
 
+def facade_circuit(n=10):
+    """The circuit tests/cxx/facade_main.cpp builds, as gate tuples."""
+    x = np.array([[0, 1], [1, 0]], dtype=np.complex128)
+    g = []
+    for i in range(n):
+        g += [(2, [i], 0, None), (2, [i], 0, None)]
+    g += [(3, [i, (i + 1) % n], 0, None) for i in range(n)]
+    g += [(4, [1, 3], 3, None), (0, [4], 0, x), (2, [5], 0, None)]
+    return g
+
+
 @pytest.mark.gpu
 def test_facade_simulates_on_the_gpu(facade_exe, oracle):
     r = subprocess.run([facade_exe, "sim"], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stdout + r.stderr
-    assert r.stdout.count("Qbit ") == 10
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("Qbit ")]
+    assert len(lines) == 10
+    # "Qbit i : teta=T , phi=P", printed with 6 significant digits.
+    got = np.array([[float(ln.split("teta=")[1].split(",")[0]), float(ln.split("phi=")[1])] for ln in lines])
+    n = 10
+    want = oracle.measure(n, oracle.simulate(n, facade_circuit(n)))
+    assert np.abs(got - want).max() <= 1e-5 * max(1.0, np.abs(want).max())
 
 
 def test_reference_main_builds_with_bench_circuits(bench_exe):
