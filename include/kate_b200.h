@@ -206,7 +206,13 @@ KATE_API kate_status kate_sim_expect_z(kate_sim* s, double* out);
 /* Probability of each computational basis state: 2^n doubles (n <= 30). */
 KATE_API kate_status kate_sim_probabilities(kate_sim* s, double* out);
 /* `shots` samples of the computational basis from |a|^2, seeded; out
- * receives shots uint64 basis indices in the reference's qubit labels. */
+ * receives shots uint64 basis indices in the reference's qubit labels.
+ * Sampled on the device (any qubit count): shot k draws u_k = (the k-th
+ * splitmix64 output of `seed` >> 11) * 2^-53 and takes the first index whose
+ * FP64 cumulative probability exceeds u_k times the total (indices of
+ * probability 0 are never drawn); only the uniforms and the samples cross
+ * PCIe. The reference has no sampling; its measurement is
+ * HIPcode/simulator.hpp:483-543. */
 KATE_API kate_status kate_sim_sample(kate_sim* s, int shots, uint64_t seed, uint64_t* out);
 
 /* Runs init + every pass once on the simulator's stream with a CUDA event

@@ -28,6 +28,13 @@ cudaError_t launch_probs(const void* st, int prec, uint64_t dim, double* out, cu
 // then ||psi||^2 and 1 / ||psi|| as doubles 0 and 1 after the partials
 // (offset renorm_result_offset()), then a counter.
 size_t renorm_scratch_bytes();
+// Inverse-CDF sampling on the device (k_sample.cu): unif holds `shots`
+// uniforms in [0, 1), ascending; out[s] receives the physical index of the
+// first amplitude whose FP64 cumulative probability exceeds unif[s] * total.
+// scratch: sample_scratch_doubles(n) doubles.
+size_t sample_scratch_doubles(int n);
+cudaError_t launch_sample(const void* st, int prec, int n, const double* unif, int shots, double* scratch,
+                          uint64_t* out, cudaStream_t s);
 constexpr size_t renorm_result_offset() { return 148 * 4 * sizeof(double); }
 cudaError_t launch_renorm_c64(void* st, int n, void* scratch, cudaStream_t s);
 

@@ -549,21 +549,47 @@ std::string Simulator::probabilities(double* out) {
 std::string Simulator::sample(int shots, uint64_t seed, uint64_t* out) {
     SimImpl& S = *d_;
     if (shots < 0) return "shots must be >= 0";
-    if (S.n > 30) return "sampling is limited to 30 qubits";
-    std::vector<double> p(S.dim());
-    std::string e = probabilities(p.data());
-    if (!e.empty()) return e;
-    // Inverse-CDF sampling on sorted uniforms (splitmix64-seeded mt19937_64).
-    std::vector<double> cdf(p.size());
-    double acc = 0.0;
-    for (size_t i = 0; i < p.size(); i++) cdf[i] = (acc += p[i]);
-    std::mt19937_64 rng(seed);
-    std::uniform_real_distribution<double> U(0.0, 1.0);
+    if (!S.has_state) return "no state: execute the simulator first";
+    if (shots == 0) return "";
+    KCHECK(cudaSetDevice(S.device));
+    // Uniforms u = (splitmix64 >> 11) * 2^-53 in draw order (the generator
+    // the server's samples use), sorted for the device with their shot index.
+    std::vector<std::pair<double, int>> us((size_t)shots);
+    uint64_t sm = seed;
     for (int k = 0; k < shots; k++) {
-        double u = U(rng) * acc;
-        size_t idx = (size_t)(std::lower_bound(cdf.begin(), cdf.end(), u) - cdf.begin());
-        if (idx >= p.size()) idx = p.size() - 1;
-        out[k] = idx;
+        sm += 0x9E3779B97F4A7C15ull;
+        uint64_t z = sm;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        us[(size_t)k] = {(double)(z >> 11) * (1.0 / 9007199254740992.0), k};
+    }
+    std::sort(us.begin(), us.end());
+    std::vector<double> u((size_t)shots);
+    for (int k = 0; k < shots; k++) u[(size_t)k] = us[(size_t)k].first;
+    const size_t nscr = sample_scratch_doubles(S.n);
+    char* buf = nullptr;
+    const size_t bytes = (nscr + (size_t)shots) * sizeof(double) + (size_t)shots * sizeof(uint64_t);
+    KCHECK(cudaMallocAsync((void**)&buf, bytes, S.stream));
+    double* d_scr = (double*)buf;
+    double* d_u = d_scr + nscr;
+    uint64_t* d_out = (uint64_t*)(d_u + shots);
+    std::vector<uint64_t> phys((size_t)shots);
+    cudaError_t ce = cudaMemcpyAsync(d_u, u.data(), (size_t)shots * sizeof(double), cudaMemcpyHostToDevice, S.stream);
+    if (ce == cudaSuccess) ce = launch_sample(S.d_state, S.precision, S.n, d_u, shots, d_scr, d_out, S.stream);
+    if (ce == cudaSuccess)
+        ce = cudaMemcpyAsync(phys.data(), d_out, (size_t)shots * sizeof(uint64_t), cudaMemcpyDeviceToHost, S.stream);
+    cudaFreeAsync(buf, S.stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(S.stream);
+    if (ce != cudaSuccess) return cuda_err("sample", ce);
+    // Physical index -> index in the reference's qubit labels.
+    std::vector<int> pb(S.n);
+    for (int x = 0; x < S.n; x++) pb[x] = S.phys_of_label(x);
+    for (int k = 0; k < shots; k++) {
+        const uint64_t v = phys[(size_t)k];
+        uint64_t lab = 0;
+        for (int x = 0; x < S.n; x++) lab |= ((v >> pb[x]) & 1ull) << x;
+        out[us[(size_t)k].second] = lab;
     }
     return "";
 }

@@ -113,18 +113,6 @@ def test_expect_z_and_probabilities(oracle):
     assert np.abs(sim.probabilities() - p).max() <= 1e-12
 
 
-def test_sampling_follows_probabilities(oracle):
-    n = 6
-    rng = np.random.default_rng(2)
-    gates = random_circuit(n, 30, rng)
-    sim, _ = run(n, gates)
-    p = np.abs(oracle.simulate(n, gates)) ** 2
-    s = sim.sample(200000, seed=42)
-    hist = np.bincount(s.astype(np.int64), minlength=1 << n) / len(s)
-    assert np.abs(hist - p).max() < 0.01
-    assert np.array_equal(s[:100], sim.sample(100, seed=42)[:100])
-
-
 def test_factored_rotations_at_edge_angles_complex128_and_complex64(oracle):
     """RX / RY at angles where a rotation's factor vanishes or dominates run as
     factored register ops on the GPU: the complex128 simulator within 1e-12
