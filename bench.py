@@ -835,6 +835,7 @@ def _hea_batch(K, C, count, seed=2024):
 
 def run_batch(args):
     """4096 HEA circuits in one persistent CUDA-graph launch."""
+    import numpy as np
     import torch
     import kate_b200 as K
     from kate_b200 import circuits as C
@@ -891,6 +892,22 @@ def run_batch(args):
     alg = float(sum(int(p) * 16.0 * 2 ** int(r) for p, r in zip(nprog, nres) if r > 0))
     peak, peak_kind = measured_hbm_peak()
     z = b.expect_z_flat()
+    # Precision: infidelity against complex128 on a seeded subsample of the
+    # circuits with resident states (those of <= 12 qubits run in one CTA's
+    # shared memory and keep no state), and the largest <Z> error of a
+    # subsample of the small ones.
+    rs = np.random.default_rng(args.seed + 7)
+    res_idx = [i for i in range(N) if int(nres[i]) > 0]
+    pick = sorted(rs.choice(res_idx, size=min(8, len(res_idx)), replace=False).tolist()) if res_idx else []
+    infid = batch_infidelity(K, circs, pick, batch=b) if pick else None
+    small = [i for i in range(N) if int(nres[i]) == 0][:16]
+    zoff = np.concatenate([[0], np.cumsum(ns)])
+    zerr = 0.0
+    for i in small:
+        s_ = K.Simulator(circs[i], 1, K.C128, 0)
+        s_.execute()
+        zerr = max(zerr, float(np.abs(s_.expect_z() - z[zoff[i]:zoff[i + 1]]).max()))
+        s_.close()
     b.close()
     # End to end: create (plan + upload) + run + readback, through the C ABI.
     t0 = time.perf_counter()
@@ -932,7 +949,9 @@ def run_batch(args):
                 "arena_bytes": info["arena_bytes"], "ctas": info["ctas"], "create_s": create_s,
                 "e2e_create_ms": create_ms, "host_cpus": os.cpu_count(),
                 "baseline_one_launch_per_circuit_cps": plain,
-                "speedup_vs_one_launch_per_circuit": value / plain if plain else None})
+                "speedup_vs_one_launch_per_circuit": value / plain if plain else None,
+                "infidelity_vs_c128": infid,
+                "small_circuits_max_abs_z_error_vs_c128": {"value": zerr, "circuits": len(small)}})
     print(json.dumps(_common(
         "circuits/s", "circuits/s", value, args, ms, "c64 (f32)", cfg,
         e2e={"value": N / e2e_s, "unit": "circuits/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 8 * len(z),
@@ -942,6 +961,33 @@ def run_batch(args):
                   "kernel": "k_batch<float2> (persistent task queue)", "alg_bytes_per_launch": alg,
                   "avg_launch_ms": ms},
         gpu_launches=args.steps, clocks=clk.summary(), cpu_baseline=cpu)))
+
+
+def batch_infidelity(K, circs, idx, batch=None):
+    """Infidelity 1 - |<psi64|psi128>|^2 of circuits `idx` (each with a
+    resident state, > 12 qubits) as the complex64 batch kernel computes them
+    (states read back from a batch: `batch`, or a new one of just these
+    circuits) against the complex128 simulator. Returns a summary dict."""
+    import numpy as np
+    own = batch is None
+    if own:
+        batch = K.Batch([circs[i] for i in idx], precision=K.C64)
+        batch.run()
+    res = []
+    for k, i in enumerate(idx):
+        psi64 = batch.state(k if own else i)
+        s = K.Simulator(circs[i], 1, K.C128, 0)
+        s.execute()
+        psi128 = s.state()
+        s.close()
+        ov = np.vdot(psi128, psi64)
+        f = float(1.0 - abs(ov) ** 2 / (np.vdot(psi64, psi64).real * np.vdot(psi128, psi128).real))
+        res.append({"circuit": int(i), "nqubits": int(circs[i].nqbits), "infidelity": f})
+    if own:
+        batch.close()
+    inf = [r["infidelity"] for r in res]
+    return {"max": max(inf), "mean": sum(inf) / len(inf), "circuits": res,
+            "against": "complex128 simulator on the same circuits (FP64)"}
 
 
 def _geometric_n(rng, lo=12, hi=28, p=0.3):
@@ -1033,6 +1079,13 @@ def run_serve(args):
                           "offered_s": float(gaps.sum())})
     st = srv.stats()
     srv.close()
+    # Precision: the engine's kernel and plans on a seeded subsample of the
+    # served circuits (more than 12 qubits), run as a batch with their
+    # states read back, against complex128.
+    rs = np.random.default_rng(args.seed + 7)
+    cand = [i for i in range(R) if ns[i] > 12 and ns[i] <= 24]
+    pick = sorted(rs.choice(cand, size=min(8, len(cand)), replace=False).tolist()) if cand else []
+    infid = batch_infidelity(K, circs, pick) if pick else None
     # Baseline: one-at-a-time plain launches (a Simulator per request, run,
     # <Z>, 1024 samples), served FIFO; latencies at each rate from the
     # measured service times under the same arrival process.
@@ -1060,7 +1113,7 @@ def run_serve(args):
     plain_cps = R / sum(svc)
     cfg.update({"sweep": sweep, "baseline_one_at_a_time": base, "baseline_service_cps": plain_cps,
                 "speedup_vs_one_at_a_time": best["circuits_per_s"] / plain_cps, "engine_steps": st["steps"],
-                "peak_resident_bytes": st["peak_resident_bytes"],
+                "peak_resident_bytes": st["peak_resident_bytes"], "infidelity_vs_c128": infid,
                 "engine_thread_s": {k[3:]: st[k] / 1e6 for k in ("us_admit", "us_build", "us_kernel", "us_collect")}})
     cpu = None
     if not args.no_cpu_baseline and not _reference_unavailable():

@@ -401,6 +401,13 @@ KATE_API kate_status kate_batch_info(const kate_batch* b, long long* info);
 KATE_API kate_status kate_batch_circuit_info(const kate_batch* b, int* programs, int* resident_qubits);
 /* Average device time of `runs` back-to-back runs (CUDA events). */
 KATE_API kate_status kate_batch_time(kate_batch* b, int runs, float* ms);
+/* Final state of circuit `circuit` after the last run, 2^n complex128
+ * amplitudes (re, im pairs) in the circuit's qubit labels; KATE_EINVAL for a
+ * circuit that ran whole in one CTA's shared memory (resident qubits 0 in
+ * kate_batch_circuit_info: it keeps no state). For checking a batch's
+ * complex64 arithmetic against complex128 (its infidelity); the reference
+ * exposes its state as a public member (CPUcode/simulator.hpp:18). */
+KATE_API kate_status kate_batch_get_state(kate_batch* b, int circuit, double* out);
 /* Host wall time of kate_batch_create in ms, ms[0..3]: planning (host
  * threads), assembly of the task queue, device buffers and uploads, graph
  * capture and instantiation. */

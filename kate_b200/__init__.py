@@ -602,6 +602,13 @@ class Batch:
         _check(self._lib.kate_batch_upload_bytes(self._h, ctypes.byref(v)))
         return v.value
 
+    def state(self, i: int) -> np.ndarray:
+        """Final state of circuit i (resident circuits only) in its qubit labels, complex128."""
+        n = self.nqbits[i]
+        out = np.empty(1 << n, dtype=np.complex128)
+        _check(self._lib.kate_batch_get_state(self._h, int(i), out.view(np.float64).ctypes.data_as(_dp)))
+        return out
+
     def circuit_info(self):
         """(pass programs, resident qubits) per circuit; resident qubits is 0
         for circuits run in shared memory."""

@@ -573,6 +573,39 @@ void Batch::circuit_info(int i, int* programs, int* resident_qubits) const {
     *resident_qubits = d_->cres[i];
 }
 
+std::string Batch::get_state(int i, double* out) {
+    BatchImpl& B = *d_;
+    if (i < 0 || i >= B.ncirc) return "circuit index out of range";
+    if (B.cres[i] == 0)
+        return "circuit " + std::to_string(i) + " ran in one CTA's shared memory and has no resident state";
+    const BatchCirc& C = B.circs[i];
+    const int n = C.n;                   // the circuit's qubits (outputs)
+    const uint64_t dim = 1ull << n;
+    const uint64_t dim_sim = 1ull << B.cres[i];  // amplitudes kept (padding qubits stay 0)
+    std::vector<uint8_t> h(dim_sim * B.amp_bytes());
+    cudaError_t ce = cudaSetDevice(B.device);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(B.stream);
+    if (ce == cudaSuccess)
+        ce = cudaMemcpy(h.data(), (const uint8_t*)B.d_arena + C.off * B.amp_bytes(), h.size(), cudaMemcpyDeviceToHost);
+    if (ce != cudaSuccess) return std::string("batch state: ") + cudaGetErrorString(ce);
+    // Label index x has qubit q at physical bit zbit[q].
+    for (uint64_t x = 0; x < dim; x++) {
+        uint64_t p = 0;
+        for (int q = 0; q < n; q++) p |= ((x >> q) & 1ull) << C.zbit[q];
+        if (p >= dim_sim) return "internal: output bit outside the resident state";
+        if (B.precision == 1) {
+            const float* f = reinterpret_cast<const float*>(h.data()) + 2 * p;
+            out[2 * x] = f[0];
+            out[2 * x + 1] = f[1];
+        } else {
+            const double* d = reinterpret_cast<const double*>(h.data()) + 2 * p;
+            out[2 * x] = d[0];
+            out[2 * x + 1] = d[1];
+        }
+    }
+    return "";
+}
+
 std::string batch_autotune(const std::vector<const Program*>& circuits, int precision, int device,
                            BatchOptions* opt) {
     if (opt->tune.size() < KATE_BATCH_MAX_QUBITS + 1) opt->tune.resize(KATE_BATCH_MAX_QUBITS + 1, BatchTune{0, 0});

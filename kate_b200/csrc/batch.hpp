@@ -78,6 +78,9 @@ public:
     uint64_t upload_bytes() const;  // host-to-device bytes copied by create()
     // Per circuit: pass programs and qubits simulated (0 for circuits run in shared memory).
     void circuit_info(int i, int* programs, int* resident_qubits) const;
+    // Final state of circuit i (one with a resident state) after the last
+    // run, as 2^n complex128 amplitudes in its qubit labels (synchronizes).
+    std::string get_state(int i, double* out);
 
 private:
     BatchImpl* d_ = nullptr;

@@ -848,6 +848,17 @@ kate_status kate_batch_circuit_info(const kate_batch* b, int* programs, int* res
     return KATE_OK;
 }
 
+kate_status kate_batch_get_state(kate_batch* b, int circuit, double* out) {
+    return guarded([&] {
+        REQUIRE(b && out, "null pointer");
+        std::string e = b->b->get_state(circuit, out);
+        if (e.find("no resident state") != std::string::npos || e.find("out of range") != std::string::npos)
+            return fail(KATE_EINVAL, e);
+        if (!e.empty()) return device_status(e);
+        return KATE_OK;
+    });
+}
+
 kate_status kate_batch_time(kate_batch* b, int runs, float* ms) {
     return guarded([&] {
         REQUIRE(b && ms && runs > 0, "null pointer or no runs");

@@ -133,3 +133,24 @@ def test_dependency_wait_runs_out_and_reports(oracle):
     for (n, g), z in zip(specs, good.expect_z()):
         assert np.abs(z - zexp(n, oracle.simulate(n, g))).max() <= 2e-5
     good.close()
+
+
+def test_batch_state_readback_matches_complex128():
+    """kate_batch_get_state returns a resident circuit's final state in its
+    labels: the complex64 batch arithmetic within 1e-6 infidelity of the
+    complex128 simulator; circuits run in shared memory have no state."""
+    circs = [K.Circuit(n, circuits.hea(n, n, seed=n)) for n in (10, 14, 17)]
+    b = K.Batch(circs, precision=K.C64)
+    b.run()
+    progs, res = b.circuit_info()
+    assert res[0] == 0 and res[1] == 14 and res[2] == 17
+    with pytest.raises(K.KateError):
+        b.state(0)
+    for i in (1, 2):
+        psi64 = b.state(i)
+        s = K.Simulator(circs[i], 1, K.C128, 0)
+        s.execute()
+        psi128 = s.state()
+        s.close()
+        assert 1.0 - abs(np.vdot(psi128, psi64)) ** 2 <= 1e-6
+    b.close()
