@@ -2,26 +2,28 @@
 // (tcgen05, kind::f16 with BF16 operands, split-BF16 products, FP32
 // accumulation in TMEM).
 //
-// Each CTA (256 threads; two CTAs per SM, ~97 KiB of shared memory each, so
-// one CTA's loads and CUDA-core phases overlap the other's tensor-core work)
-// processes 4096-amplitude coset tiles in a grid-stride loop. Per tile:
-//   0. the tile is copied global -> staging buffer S with 16-byte cp.async
-//      (an amplitude pair per copy: tile bit 0 is physical bit 0);
-//   for each block of the pass:
-//   1. S is rearranged into the MMA A operand: 128 rows (the values of the
-//      7 non-block tile bits) x 64 reals (the 32 complex amplitudes of the
-//      block's index, re/im interleaved), K-major with the 128-byte swizzle,
-//      as a BF16 hi part and the BF16 remainder (lo);
+// Each CTA (256 threads; two CTAs per SM, ~97 KiB of shared memory each)
+// processes 4096-amplitude coset tiles in a grid-stride loop, with two
+// staging buffers: while a tile is processed, the next one is already being
+// copied in (16-byte cp.async of amplitude pairs; tile bit 0 is physical
+// bit 0), so the HBM load latency is hidden behind the blocks. Per tile, for
+// each block of the pass:
+//   1. every thread builds its part of the MMA A operand from the staging
+//      tile: row r = t & 127 (the values of the 7 non-block tile bits), K
+//      half h = t >> 7 (the 16 block indices 16h..16h+15, re/im interleaved),
+//      as a BF16 hi part and the BF16 remainder (lo), and writes it to TMEM
+//      (tcgen05.st; the A operand of tcgen05.mma may live in TMEM: lane r,
+//      one 32-bit column per re/im pair), not shared memory;
 //   2. one elected thread issues 4 K-steps x 3 products (A_hi.B_hi,
-//      A_hi.B_lo, A_lo.B_hi; M = 128, N = 64, K = 16) into one TMEM
-//      accumulator and commits to an mbarrier;
+//      A_hi.B_lo, A_lo.B_hi; M = 128, N = 64, K = 16; A from TMEM, B from
+//      shared memory) into one TMEM accumulator and commits to an mbarrier;
 //   3. every thread reads its row's 32 results back from TMEM and writes
-//      them to S at the amplitudes' tile positions;
-//   4. the tile is written back to global with the pass's remap permutation
-//      (16-byte stores of amplitude pairs).
-// The block matrices (B operands, hi and lo) are staged in shared memory
-// once per CTA. All waits are bounded: on timeout the kernel records an
-// error flag for the host and returns after freeing its TMEM.
+//      them to the staging tile at the amplitudes' tile positions;
+// then the tile is written back to global with the pass's remap permutation
+// (16-byte stores of amplitude pairs). The block matrices (B operands, hi
+// and lo) are staged in shared memory once per CTA. All waits are bounded:
+// on timeout the kernel records an error flag for the host and returns
+// after its copies in flight completed, freeing its TMEM.
 //
 // Accuracy: hi + lo keeps ~16 bits of each FP32 operand and the dropped
 // lo.lo product is ~2^-16 relative, so one block's relative error is about
@@ -39,16 +41,16 @@ namespace {
 constexpr int NT = 256;
 constexpr int TB = KATE_TILE_BITS;  // 12 tile bits
 constexpr int TS = 1 << TB;
-constexpr uint32_t A_BYTES = 128 * 64 * 2;   // 16 KiB per operand part (hi or lo), BF16
 constexpr uint32_t S_BYTES = TS * 8;         // 32 KiB staging tile (float2)
-constexpr uint32_t OFF_A = 0;
-constexpr uint32_t OFF_AL = OFF_A + A_BYTES;
-constexpr uint32_t OFF_B = OFF_AL + A_BYTES;                                   // blocks' B images
-constexpr uint32_t OFF_S = OFF_B + KATE_C64_MAX_BLOCKS * KATE_BLOCK_IMG_BYTES;  // staging tile
-constexpr uint32_t OFF_MISC = OFF_S + S_BYTES;           // mbarrier, TMEM slot, abort flag
+constexpr uint32_t OFF_B = 0;                                                   // blocks' B images
+constexpr uint32_t OFF_S = OFF_B + KATE_C64_MAX_BLOCKS * KATE_BLOCK_IMG_BYTES;  // two staging tiles
+constexpr uint32_t OFF_MISC = OFF_S + 2 * S_BYTES;       // mbarrier, TMEM slot, abort flag
 constexpr uint32_t OFF_TAB = OFF_MISC + 64;              // per block: swizzled tile offset of block index b
 constexpr uint32_t SMEM_BYTES = OFF_TAB + KATE_C64_MAX_BLOCKS * 32 * 2 + 1024;  // + alignment slack
-constexpr uint32_t TMEM_COLS = 64;
+// TMEM columns: the FP32 accumulator (N = 64), then the A operand's hi and
+// lo parts (128 lanes x 64 BF16 = 32 columns each).
+constexpr uint32_t TMEM_COLS = 128;
+constexpr uint32_t TM_AHI = 64, TM_ALO = 96;
 constexpr long WAIT_LIMIT = 1L << 24;
 
 // Pair-preserving swizzle of the staging tile (float2 elements): XORs bits
@@ -81,12 +83,23 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
 // Instruction descriptor: D F32, A/B BF16, both K-major, N = 64, M = 128.
 constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
 
-__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+// D (TMEM) += A (TMEM) x B (shared memory descriptor).
+__device__ __forceinline__ void mma_bf16_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t bdesc, uint32_t accumulate) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(IDESC), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+        "r"(tmem_a), "l"(bdesc), "r"(IDESC), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+// 16 consecutive TMEM columns of this warp's 32 lanes from 16 registers per thread.
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&v)[16]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16};" ::"r"(taddr),
+        "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]), "r"(v[9]),
+        "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15])
+        : "memory");
 }
 
 __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
@@ -104,11 +117,6 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
     return false;
 }
 
-// Byte offset of (row, k) in a K-major SWIZZLE_128B image of 64 BF16 columns.
-__device__ __forceinline__ uint32_t a_off(uint32_t row, uint32_t chunk) {
-    return (row >> 3) * 1024u + (row & 7u) * 128u + ((chunk ^ (row & 7u)) << 4);
-}
-
 __global__ void __launch_bounds__(NT, 2)
     k_block_c64(float2* __restrict__ st, const __grid_constant__ BlockProg P, const uint8_t* __restrict__ bimg,
                 int* __restrict__ err) {
@@ -120,8 +128,6 @@ __global__ void __launch_bounds__(NT, 2)
     const uint32_t mbar = base + OFF_MISC;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(gbase + OFF_MISC + 8);
     int* abort_flag = reinterpret_cast<int*>(gbase + OFF_MISC + 16);
-    float2* S = reinterpret_cast<float2*>(gbase + OFF_S);
-    const uint32_t sb = base + OFF_S;
 
     if (t == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
@@ -209,46 +215,58 @@ __global__ void __launch_bounds__(NT, 2)
 
     const uint64_t ncos = 1ull << P.ncb;
     uint32_t phase = 0;
-    for (uint64_t c = blockIdx.x; c < ncos; c += gridDim.x) {
-        const uint64_t cb = coset_base(c);
-        {
-            const float2* src = st + cb + dT;
+    // Issues the copy of coset c into staging buffer `buf` (one cp.async
+    // group; an empty group when c is past the last coset, so every
+    // iteration waits for exactly its own tile).
+    auto load_tile = [&](uint64_t c, int buf) {
+        if (c < ncos) {
+            const float2* src = st + coset_base(c) + dT;
+            const uint32_t sb = base + OFF_S + (uint32_t)buf * S_BYTES;
 #pragma unroll
             for (int j = 0; j < 8; j++) {
                 const uint32_t d = sb + sswz(2u * t + ((uint32_t)j << 9)) * 8u;
                 asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src + dH[j]) : "memory");
             }
-            asm volatile("cp.async.commit_group;\n" ::: "memory");
-            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
         }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
+    load_tile(blockIdx.x, 0);
+    int it = 0;
+    for (uint64_t c = blockIdx.x; c < ncos; c += gridDim.x, it++) {
+        const int cur = it & 1;
+        float2* S = reinterpret_cast<float2*>(gbase + OFF_S + (uint32_t)cur * S_BYTES);
+        const uint64_t cb = coset_base(c);
+        // The other buffer was last read by the previous tile's write-back,
+        // which the barrier at the end of that iteration closed.
+        load_tile(c + gridDim.x, cur ^ 1);
+        asm volatile("cp.async.wait_group 1;\n" ::: "memory");
         __syncthreads();
 
         for (int blk = 0; blk < P.nblocks; blk++) {
             const uint16_t* tb = tab + blk * 32;
             const uint32_t ra_sw = blk == 0 ? rsa[0] : rsa[KATE_C64_MAX_BLOCKS - 1];
             const uint32_t rr_sw = blk == 0 ? rsr[0] : rsr[KATE_C64_MAX_BLOCKS - 1];
-            // 1. A operand (hi, lo) from the staging tile. Thread t: row
-            //    r = t & 127, K half h = t >> 7 (block indices 16h..16h+15,
-            //    16-byte chunks 4h..4h+3 of 4 amplitudes each).
+            // 1. A operand (hi, lo) from the staging tile into TMEM. Thread
+            //    t: row r = t & 127 (TMEM lane 32 (warp & 3) + lane), K half
+            //    h = t >> 7 (block indices 16h..16h+15: TMEM columns 16h..
+            //    16h+15 of the A parts, one re/im pair per column).
             {
-                const uint32_t r = t & 127u, h = t >> 7;
+                const uint32_t h = t >> 7;
+                uint32_t hw[16], lw[16];
 #pragma unroll
-                for (int q = 0; q < 4; q++) {
-                    uint32_t hw[4], lw[4];
-#pragma unroll
-                    for (int e = 0; e < 4; e++) {
-                        const float2 a = S[ra_sw ^ tb[h * 16u + (uint32_t)(4 * q + e)]];
-                        const uint32_t hp = bf16x2_rn(a.x, a.y);
-                        const float hre = __uint_as_float(hp << 16), him = __uint_as_float(hp & 0xffff0000u);
-                        hw[e] = hp;
-                        lw[e] = bf16x2_rn(a.x - hre, a.y - him);
-                    }
-                    const uint32_t off = a_off(r, h * 4u + (uint32_t)q);
-                    *reinterpret_cast<uint4*>(gbase + OFF_A + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
-                    *reinterpret_cast<uint4*>(gbase + OFF_AL + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+                for (int e = 0; e < 16; e++) {
+                    const float2 a = S[ra_sw ^ tb[h * 16u + (uint32_t)e]];
+                    const uint32_t hp = bf16x2_rn(a.x, a.y);
+                    const float hre = __uint_as_float(hp << 16), him = __uint_as_float(hp & 0xffff0000u);
+                    hw[e] = hp;
+                    lw[e] = bf16x2_rn(a.x - hre, a.y - him);
                 }
+                const uint32_t lane_base = tmem + (((warp & 3u) * 32u) << 16) + h * 16u;
+                tmem_st16(lane_base + TM_AHI, hw);
+                tmem_st16(lane_base + TM_ALO, lw);
+                asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
             }
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncthreads();
             // 2. Tensor-core products into TMEM.
             if (t == 0) {
@@ -256,12 +274,12 @@ __global__ void __launch_bounds__(NT, 2)
                 const uint32_t bb = base + OFF_B + blk * KATE_BLOCK_IMG_BYTES;
 #pragma unroll 1
                 for (int s = 0; s < 4; s++) {
-                    const uint32_t k = (uint32_t)s * 32u;  // K = 16 BF16 = 32 bytes per step
-                    const uint64_t a_hi = sw128_desc(base + OFF_A + k), a_lo = sw128_desc(base + OFF_AL + k);
+                    const uint32_t k = (uint32_t)s * 32u;  // K = 16 BF16 = 32 bytes per step (B)
+                    const uint32_t kc = (uint32_t)s * 8u;  // K = 16 BF16 = 8 TMEM columns per step (A)
                     const uint64_t b_hi = sw128_desc(bb + k), b_lo = sw128_desc(bb + KATE_BLOCK_IMG_BYTES / 2 + k);
-                    mma_bf16(tmem, a_hi, b_hi, s > 0 ? 1u : 0u);
-                    mma_bf16(tmem, a_hi, b_lo, 1u);
-                    mma_bf16(tmem, a_lo, b_hi, 1u);
+                    mma_bf16_ts(tmem, tmem + TM_AHI + kc, b_hi, s > 0 ? 1u : 0u);
+                    mma_bf16_ts(tmem, tmem + TM_AHI + kc, b_lo, 1u);
+                    mma_bf16_ts(tmem, tmem + TM_ALO + kc, b_hi, 1u);
                 }
                 asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
                              : "memory");
