@@ -878,7 +878,9 @@ def run_batch(args):
     t0 = time.perf_counter()
     b = K.Batch(circs, precision=K.C64, autotune=not args.no_autotune)
     create_s = time.perf_counter() - t0
-    tune = {n: [b.options.tune[n].fusion, b.options.tune[n].max_gates] for n in sorted(set(ns))}
+    tune = {n: {"fusion_k": b.options.tune[n].fusion, "max_gates": b.options.tune[n].max_gates,
+                "group_m": b.options.tune[n].group_qubits, "coalesce_c": b.options.tune[n].coalesce}
+            for n in sorted(set(ns))}
     info = b.info()
     b.time(max(1, args.warmup))
     with Clocks(0) as clk:

@@ -363,6 +363,8 @@ KATE_API kate_status kate_release_cached_memory(int device);
 typedef struct {
     int fusion;    /* gateFusion width applied to circuits without groups or instructions (1: none; 0: default) */
     int max_gates; /* gates per pass program (0: default) */
+    int group_qubits; /* m: qubits one pass's gates may span, 6..12, as gateGrouping(m) (0: 12) */
+    int coalesce;  /* c: low physical bits every pass keeps in its tile, 1..6 (0: 4) */
 } kate_batch_tuning;
 typedef struct {
     int chunk;                 /* cosets (4096-amplitude tiles) per pass task; 0: default */

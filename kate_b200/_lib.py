@@ -109,7 +109,7 @@ KATE_BATCH_MAX_QUBITS = 28
 
 
 class BatchTuning(_c.Structure):
-    _fields_ = [("fusion", _c.c_int), ("max_gates", _c.c_int)]
+    _fields_ = [("fusion", _c.c_int), ("max_gates", _c.c_int), ("group_qubits", _c.c_int), ("coalesce", _c.c_int)]
 
 
 class BatchOptions(_c.Structure):

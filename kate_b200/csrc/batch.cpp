@@ -68,7 +68,8 @@ std::string pack_circuit(const Program& in, const BatchTune& tune, bool resident
     out.n_sim = p.nqbits;
     PlanOptions o;
     o.max_tile = KATE_TILE_BITS;
-    o.coalesce = 4;
+    o.group_qubits = tune.group >= 6 && tune.group <= KATE_TILE_BITS ? tune.group : KATE_TILE_BITS;
+    o.coalesce = tune.coalesce >= 1 && tune.coalesce <= 6 ? tune.coalesce : 4;
     o.remap = !out.small;  // a resident tile is never written back, so it keeps its layout
     o.fuse_1q = true;
     o.staged = true;
@@ -168,6 +169,23 @@ const BatchTune& BatchOptions::for_n(int n) const {
     if (n >= 0 && (size_t)n < tune.size() && tune[n].fusion >= 1 && tune[n].max_gates >= 1) return tune[n];
     return kDefaultTune;
 }
+
+namespace {
+// Times one candidate tuning for qubit count n on `sample`; ms < 0 when the
+// candidate does not plan.
+std::string time_candidate(const std::vector<const Program*>& sample, int precision, int device,
+                           const BatchOptions& base, int n, const BatchTune& t, float* ms) {
+    BatchOptions o = base;
+    o.tune[n] = t;
+    Batch* b = nullptr;
+    *ms = -1.f;
+    if (!Batch::create(sample, precision, device, o, &b).empty()) return "";
+    std::string e = b->time_runs(1, ms);
+    if (e.empty()) e = b->time_runs(3, ms);
+    delete b;
+    return e;
+}
+}  // namespace
 
 struct BatchImpl {
     int device = 0;
@@ -608,12 +626,14 @@ std::string Batch::get_state(int i, double* out) {
 
 std::string batch_autotune(const std::vector<const Program*>& circuits, int precision, int device,
                            BatchOptions* opt) {
-    if (opt->tune.size() < KATE_BATCH_MAX_QUBITS + 1) opt->tune.resize(KATE_BATCH_MAX_QUBITS + 1, BatchTune{0, 0});
+    if (opt->tune.size() < KATE_BATCH_MAX_QUBITS + 1) opt->tune.resize(KATE_BATCH_MAX_QUBITS + 1, BatchTune{0, 0, 0, 0});
     std::map<int, std::vector<const Program*>> byn;
     for (const Program* p : circuits)
         if (p) byn[p->nqbits].push_back(p);
     static const int kFusion[] = {1, 2, 3};
     static const int kGates[] = {64, 96, 128};
+    static const int kGroup[] = {11, 10};
+    static const int kCoalesce[] = {3, 5};
     for (auto& kv : byn) {
         const int n = kv.first;
         const int nsim = std::max(n, KATE_TILE_BITS);
@@ -624,24 +644,39 @@ std::string batch_autotune(const std::vector<const Program*>& circuits, int prec
         float best = 0.f;
         BatchTune bt = kDefaultTune;
         bool found = false;
+        auto consider = [&](const BatchTune& t) -> std::string {
+            float ms = 0.f;
+            std::string e = time_candidate(sample, precision, device, *opt, n, t, &ms);
+            if (!e.empty()) return e;
+            if (ms >= 0.f && (!found || ms < best)) {
+                best = ms;
+                bt = t;
+                found = true;
+            }
+            return "";
+        };
+        // Coordinate search: fusion width x gates per pass at the default
+        // grouping and coalescing, then the grouping size m, then the
+        // coalesce width c (which only matters for states kept in HBM).
         for (int f : kFusion)
             for (int g : kGates) {
-                BatchOptions o = *opt;
-                o.tune[n] = BatchTune{f, g};
-                Batch* b = nullptr;
-                if (!Batch::create(sample, precision, device, o, &b).empty()) continue;
-                float ms = 0.f;
-                std::string e = b->time_runs(1, &ms);
-                if (e.empty()) e = b->time_runs(3, &ms);
-                delete b;
+                std::string e = consider(BatchTune{f, g, KATE_TILE_BITS, 4});
                 if (!e.empty()) return e;
-                if (!found || ms < best) {
-                    best = ms;
-                    bt = BatchTune{f, g};
-                    found = true;
-                }
             }
         if (!found) return "autotune: no candidate plan for " + std::to_string(n) + "-qubit circuits";
+        for (int m : kGroup) {
+            BatchTune t = bt;
+            t.group = m;
+            std::string e = consider(t);
+            if (!e.empty()) return e;
+        }
+        if (n > KATE_BATCH_SMALL_MAX)
+            for (int c : kCoalesce) {
+                BatchTune t = bt;
+                t.coalesce = c;
+                std::string e = consider(t);
+                if (!e.empty()) return e;
+            }
         opt->tune[n] = bt;
     }
     return "";

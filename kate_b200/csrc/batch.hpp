@@ -23,6 +23,8 @@ namespace kate {
 struct BatchTune {
     int fusion = 1;      // gateFusion width for circuits without compiled instructions (1: no gateFusion)
     int max_gates = 96;  // gates per pass program
+    int group = 12;      // m: qubits one pass's gates may span (gateGrouping(m)); the 12-qubit tile is filled up
+    int coalesce = 4;    // c: low physical bits every pass keeps in its tile (runs of 2^c amplitudes per access)
 };
 
 struct BatchOptions {

@@ -709,6 +709,8 @@ kate::BatchOptions to_options(const kate_batch_options* o) {
     for (int n = 0; n <= KATE_BATCH_MAX_QUBITS; n++) {
         r.tune[n].fusion = o->tune[n].fusion;
         r.tune[n].max_gates = o->tune[n].max_gates;
+        r.tune[n].group = o->tune[n].group_qubits > 0 ? o->tune[n].group_qubits : KATE_TILE_BITS;
+        r.tune[n].coalesce = o->tune[n].coalesce > 0 ? o->tune[n].coalesce : 4;
     }
     return r;
 }
@@ -749,6 +751,8 @@ kate_status kate_batch_autotune(const kate_circuit* const* circuits, int count, 
         for (int n = 0; n <= KATE_BATCH_MAX_QUBITS; n++) {
             opt->tune[n].fusion = o.tune[n].fusion;
             opt->tune[n].max_gates = o.tune[n].max_gates;
+            opt->tune[n].group_qubits = o.tune[n].group;
+            opt->tune[n].coalesce = o.tune[n].coalesce;
         }
         return KATE_OK;
     });

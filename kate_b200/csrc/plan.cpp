@@ -382,12 +382,15 @@ std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out) {
     if (opt.fuse_1q) plan.pgates = fuse_single_qubit(std::move(plan.pgates), n);
 
     const int m = std::min(opt.max_tile, n);
+    // Gates of one pass span at most mg qubits (the c low bits included);
+    // the tile is then filled up to m with other qubits.
+    const int mg = opt.group_qubits > 0 ? std::min(opt.group_qubits, m) : m;
     int maxT = 0;
     for (auto& g : plan.pgates) maxT = std::max(maxT, (int)(g.tq.size() + (opt.c64 ? g.fq.size() : 0)));
-    if (maxT > m) return "a gate has more target qubits than the tile";
+    if (maxT > mg) return "a gate has more target qubits than the tile";
     // The c low physical bits are always tile bits; leave room for the
     // widest gate's targets beside them so every pass can make progress.
-    const int c = std::max(0, std::min(opt.coalesce, m - maxT));
+    const int c = std::max(0, std::min(opt.coalesce, mg - maxT));
     Layout L(n);
     std::vector<int> rem(plan.pgates.size());
     std::iota(rem.begin(), rem.end(), 0);
@@ -399,7 +402,7 @@ std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out) {
             inT[L.inv[p]] = 1;
             tsize++;
         }
-        std::vector<int> exec = greedy_pass(plan.pgates, rem, n, m, inT, tsize, nullptr, scan_limit, opt.c64);
+        std::vector<int> exec = greedy_pass(plan.pgates, rem, n, mg, inT, tsize, nullptr, scan_limit, opt.c64);
         size_t keep = exec.size();
         if ((int)keep > opt.max_gates_per_pass) keep = opt.max_gates_per_pass;
         if (opt.c64 && m == KATE_TILE_BITS) {
@@ -459,7 +462,7 @@ std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out) {
             std::vector<char> inT2(n, 0);
             int ts2 = 0;
             std::vector<int> order;
-            greedy_pass(plan.pgates, rem, n, m, inT2, ts2, &order, scan_limit, opt.c64);
+            greedy_pass(plan.pgates, rem, n, mg, inT2, ts2, &order, scan_limit, opt.c64);
             for (int q : order)
                 if (inT[q] && (int)newlow.size() < c) newlow.push_back(q);
         }

@@ -33,7 +33,9 @@
 namespace kate {
 
 struct PlanOptions {
-    int max_tile = 12;   // m: tile qubits per pass
+    int max_tile = 12;   // tile qubits per pass (the kernels' tile)
+    int group_qubits = 0;  // m: qubits the gates of one pass may span, at most max_tile (0: max_tile); the
+                           // rest of the tile is filled with other qubits (the reference's gateGrouping(m))
     int coalesce = 4;    // c: low physical bits every tile must contain
     bool remap = true;   // move next-needed qubits into the low bits on write
     bool fuse_1q = true; // multiply chains of single-qubit ops on one qubit (FP64, host)

@@ -86,11 +86,33 @@ def test_compiled_circuits_match_simulator():
         assert np.abs(sim.expect_z() - z).max() <= 1e-12
 
 
+@pytest.mark.parametrize("m,c", [(10, 3), (11, 5), (12, 4), (10, 5), (12, 3)])
+def test_every_grouping_and_coalesce_choice_matches_oracle(oracle, m, c):
+    """The autotuner's search space beyond fusion width and gates per pass:
+    the grouping size m (qubits one pass's gates span; the 12-qubit tile is
+    filled up) and the coalesce width c (low physical bits every tile keeps).
+    Each choice gives the oracle's <Z> (complex128, 1e-12)."""
+    specs = mixed(3)
+    o = _lib.BatchOptions()
+    K._lib.lib().kate_batch_options_default(ctypes_ref(o))
+    for n in range(K._lib.KATE_BATCH_MAX_QUBITS + 1):
+        o.tune[n].fusion = 2
+        o.tune[n].max_gates = 96
+        o.tune[n].group_qubits = m
+        o.tune[n].coalesce = c
+    b = K.Batch([K.Circuit(n, g) for n, g in specs], precision=K.C128, options=o)
+    b.run()
+    for (n, g), z in zip(specs, b.expect_z()):
+        assert np.abs(z - zexp(n, oracle.simulate(n, g))).max() <= 1e-12, (n, m, c)
+
+
 def test_autotune_then_run(oracle):
     specs = [(n, circuits.hea(n, 2 * n, seed=100 + i)) for i, n in enumerate([10, 11, 13, 13, 15])]
     b = K.Batch([K.Circuit(n, g) for n, g in specs], precision=K.C64, autotune=True)
     for n in (10, 11, 13, 15):
-        assert b.options.tune[n].fusion >= 1 and b.options.tune[n].max_gates >= 1
+        t = b.options.tune[n]
+        assert t.fusion >= 1 and t.max_gates >= 1
+        assert 10 <= t.group_qubits <= 12 and 3 <= t.coalesce <= 5
     b.run()
     for (n, g), z in zip(specs, b.expect_z()):
         assert np.abs(z - zexp(n, oracle.simulate(n, g))).max() <= 2e-5
