@@ -127,6 +127,12 @@ typedef struct {
 #define KATE_C64_MAX_BLOCKS 2
 #define KATE_BLOCK_IMG_BYTES 16384
 
+// The staging tile's layout: element e (tile index) sits at position
+// e ^ sum_k parity(e & smask[k]) << k (k = 0..3, masks over tile bits 4..11:
+// linear over GF(2) and invertible), chosen per pass so that a warp's rows
+// (a block's 4 lowest non-block tile bits) and its write-back lanes fall on
+// distinct 8-byte bank pairs. smask[0] = 0 keeps amplitude pairs (e, e + 1)
+// side by side in one 16-byte slot.
 typedef struct {
     int32_t m, ncb, nblocks, pad;
     uint8_t tphys[16];
@@ -134,6 +140,7 @@ typedef struct {
     uint8_t cphys[48];
     uint8_t btb[KATE_C64_MAX_BLOCKS][8];
     uint64_t bimg[KATE_C64_MAX_BLOCKS];
+    uint16_t smask[4];
 } BlockProg;
 
 // ---- batched execution (k_batch.cu) ----

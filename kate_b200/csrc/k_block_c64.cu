@@ -46,17 +46,25 @@ constexpr uint32_t OFF_B = 0;                                                   
 constexpr uint32_t OFF_S = OFF_B + KATE_C64_MAX_BLOCKS * KATE_BLOCK_IMG_BYTES;  // two staging tiles
 constexpr uint32_t OFF_MISC = OFF_S + 2 * S_BYTES;       // mbarrier, TMEM slot, abort flag
 constexpr uint32_t OFF_TAB = OFF_MISC + 64;              // per block: swizzled tile offset of block index b
-constexpr uint32_t SMEM_BYTES = OFF_TAB + KATE_C64_MAX_BLOCKS * 32 * 2 + 1024;  // + alignment slack
+// Then 8 swizzled copy offsets P(j << 9), 8 write-back offsets P(oH[j]) and P(o1).
+constexpr uint32_t OFF_IO = OFF_TAB + KATE_C64_MAX_BLOCKS * 32 * 2;
+constexpr uint32_t SMEM_BYTES = OFF_IO + 32 * 2 + 1024;  // + alignment slack
 // TMEM columns: the FP32 accumulator (N = 64), then the A operand's hi and
 // lo parts (128 lanes x 64 BF16 = 32 columns each).
 constexpr uint32_t TMEM_COLS = 128;
 constexpr uint32_t TM_AHI = 64, TM_ALO = 96;
 constexpr long WAIT_LIMIT = 1L << 24;
 
-// Pair-preserving swizzle of the staging tile (float2 elements): XORs bits
-// 1..3 of the index with bits 4..6 and 8..10, spreading strided 8-byte
-// accesses over the banks while keeping element pairs 16-byte contiguous.
-__device__ __forceinline__ uint32_t sswz(uint32_t i) { return i ^ ((((i >> 4) ^ (i >> 8)) & 7u) << 1); }
+// The pass's staging-tile swizzle (BlockProg::smask, chosen on the host):
+// element e sits at e ^ sum_k parity(e & f[k]) << k. Linear over GF(2), so
+// offsets of XOR-combined indices XOR.
+struct Swz {
+    uint32_t f0, f1, f2, f3;
+    __device__ __forceinline__ uint32_t operator()(uint32_t e) const {
+        return e ^ ((uint32_t)__popc(e & f0) & 1u) ^ (((uint32_t)__popc(e & f1) & 1u) << 1) ^
+               (((uint32_t)__popc(e & f2) & 1u) << 2) ^ (((uint32_t)__popc(e & f3) & 1u) << 3);
+    }
+};
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -158,6 +166,9 @@ __global__ void __launch_bounds__(NT, 2)
     // of its TMEM row (r = 32 (warp & 3) + lane) deposited into the other
     // bits. sswz is linear over GF(2), so a tile offset is rsw ^ tab[b].
     uint16_t* tab = reinterpret_cast<uint16_t*>(gbase + OFF_TAB);
+    uint16_t* iot = reinterpret_cast<uint16_t*>(gbase + OFF_IO);
+    const Swz sswz{P.smask[0], P.smask[1], P.smask[2], P.smask[3]};
+    const bool pairs = P.smask[0] == 0;  // amplitude pairs stay in one 16-byte slot
     uint32_t rsa[KATE_C64_MAX_BLOCKS], rsr[KATE_C64_MAX_BLOCKS];
 #pragma unroll
     for (int blk = 0; blk < KATE_C64_MAX_BLOCKS; blk++) {
@@ -207,6 +218,15 @@ __global__ void __launch_bounds__(NT, 2)
         oH[j] = o;
     }
     const uint32_t o1 = 1u << P.outsrc[0];
+    if (t < 8) {
+        iot[t] = (uint16_t)sswz((uint32_t)t << 9);
+        iot[8 + t] = (uint16_t)sswz(oH[t]);
+    } else if (t == 8) {
+        iot[16] = (uint16_t)sswz(o1);
+    }
+    const uint32_t cp_base = sswz(2u * t);  // copy-in: element 2t + 512 j at cp_base ^ iot[j]
+    const uint32_t wb_base = sswz(pT);      // write-back: output pair j reads wb_base ^ iot[8 + j]
+    __syncthreads();
     auto coset_base = [&](uint64_t c) {
         uint64_t b = 0;
         for (int i = 0; i < P.ncb; i++) b |= ((c >> i) & 1ull) << P.cphys[i];
@@ -222,10 +242,23 @@ __global__ void __launch_bounds__(NT, 2)
         if (c < ncos) {
             const float2* src = st + coset_base(c) + dT;
             const uint32_t sb = base + OFF_S + (uint32_t)buf * S_BYTES;
+            if (pairs) {
 #pragma unroll
-            for (int j = 0; j < 8; j++) {
-                const uint32_t d = sb + sswz(2u * t + ((uint32_t)j << 9)) * 8u;
-                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src + dH[j]) : "memory");
+                for (int j = 0; j < 8; j++) {
+                    const uint32_t d = sb + (cp_base ^ iot[j]) * 8u;
+                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src + dH[j]) : "memory");
+                }
+            } else {
+                // The pair's two amplitudes land in different 8-byte slots.
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    const uint32_t e0 = cp_base ^ iot[j];
+                    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sb + e0 * 8u), "l"(src + dH[j])
+                                 : "memory");
+                    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sb + (e0 ^ 1u) * 8u),
+                                 "l"(src + dH[j] + 1)
+                                 : "memory");
+                }
             }
         }
         asm volatile("cp.async.commit_group;\n" ::: "memory");
@@ -253,13 +286,25 @@ __global__ void __launch_bounds__(NT, 2)
             {
                 const uint32_t h = t >> 7;
                 uint32_t hw[16], lw[16];
-#pragma unroll
-                for (int e = 0; e < 16; e++) {
-                    const float2 a = S[ra_sw ^ tb[h * 16u + (uint32_t)e]];
+                auto split = [&](int e, float2 a) {
                     const uint32_t hp = bf16x2_rn(a.x, a.y);
                     const float hre = __uint_as_float(hp << 16), him = __uint_as_float(hp & 0xffff0000u);
                     hw[e] = hp;
                     lw[e] = bf16x2_rn(a.x - hre, a.y - him);
+                };
+                if (P.btb[blk][0] == 0 && pairs) {
+                    // Tile bit 0 is the block's index bit 0 (and the swizzle
+                    // keeps pairs): block indices 2i, 2i + 1 of a row are one
+                    // aligned 16-byte pair.
+#pragma unroll
+                    for (int e = 0; e < 16; e += 2) {
+                        const float4 v = *reinterpret_cast<const float4*>(&S[ra_sw ^ tb[h * 16u + (uint32_t)e]]);
+                        split(e, make_float2(v.x, v.y));
+                        split(e + 1, make_float2(v.z, v.w));
+                    }
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 16; e++) split(e, S[ra_sw ^ tb[h * 16u + (uint32_t)e]]);
                 }
                 const uint32_t lane_base = tmem + (((warp & 3u) * 32u) << 16) + h * 16u;
                 tmem_st16(lane_base + TM_AHI, hw);
@@ -284,11 +329,12 @@ __global__ void __launch_bounds__(NT, 2)
                 asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
                              : "memory");
             }
-            const bool ok = mbar_wait(mbar, phase);
+            // One thread waits for the products (the others would only take
+            // issue slots from the SM's other CTA); the barrier releases them.
+            if (t == 0 && !mbar_wait(mbar, phase)) *abort_flag = 1;
             phase ^= 1u;
-            if (!ok) *abort_flag = 1;
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             __syncthreads();
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             if (*abort_flag) break;
             // 3. Results: warp w reads TMEM lanes 32(w&3)..+31 (rows) and
             //    columns 32(w>>2)..+31 (block indices 16(w>>2)..+15).
@@ -307,10 +353,18 @@ __global__ void __launch_bounds__(NT, 2)
                       "=r"(d[29]), "=r"(d[30]), "=r"(d[31])
                     : "r"(taddr));
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                if (P.btb[blk][0] == 0 && pairs) {
 #pragma unroll
-                for (int e = 0; e < 16; e++)
-                    S[rr_sw ^ tb[ch * 16u + (uint32_t)e]] =
-                        make_float2(__uint_as_float(d[2 * e]), __uint_as_float(d[2 * e + 1]));
+                    for (int e = 0; e < 16; e += 2)
+                        *reinterpret_cast<float4*>(&S[rr_sw ^ tb[ch * 16u + (uint32_t)e]]) =
+                            make_float4(__uint_as_float(d[2 * e]), __uint_as_float(d[2 * e + 1]),
+                                        __uint_as_float(d[2 * e + 2]), __uint_as_float(d[2 * e + 3]));
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 16; e++)
+                        S[rr_sw ^ tb[ch * 16u + (uint32_t)e]] =
+                            make_float2(__uint_as_float(d[2 * e]), __uint_as_float(d[2 * e + 1]));
+                }
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncthreads();
@@ -319,11 +373,20 @@ __global__ void __launch_bounds__(NT, 2)
         // 4. Write back with the remap permutation, an amplitude pair per store.
         {
             float2* dst = st + cb + dT;
+            const uint32_t po1 = iot[16];
+            if (P.outsrc[0] == 0 && pairs) {
+                // Output bit 0 keeps input bit 0: the pair is one 16-byte slot.
 #pragma unroll
-            for (int j = 0; j < 8; j++) {
-                const uint32_t src = pT | oH[j];
-                const float2 v0 = S[sswz(src)], v1 = S[sswz(src | o1)];
-                *reinterpret_cast<float4*>(dst + dH[j]) = make_float4(v0.x, v0.y, v1.x, v1.y);
+                for (int j = 0; j < 8; j++)
+                    *reinterpret_cast<float4*>(dst + dH[j]) =
+                        *reinterpret_cast<const float4*>(&S[wb_base ^ iot[8 + j]]);
+            } else {
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    const uint32_t e0 = wb_base ^ iot[8 + j];
+                    const float2 v0 = S[e0], v1 = S[e0 ^ po1];
+                    *reinterpret_cast<float4*>(dst + dH[j]) = make_float4(v0.x, v0.y, v1.x, v1.y);
+                }
             }
         }
         __syncthreads();

@@ -36,7 +36,8 @@ PROG_DTYPE = np.dtype([("m", "<i4"), ("ncb", "<i4"), ("nops", "<i4"), ("nmats", 
 
 
 BLOCK_DTYPE = np.dtype([("m", "<i4"), ("ncb", "<i4"), ("nblocks", "<i4"), ("pad", "<i4"), ("tphys", "u1", 16),
-                        ("outsrc", "u1", 16), ("cphys", "u1", 48), ("btb", "u1", (2, 8)), ("bimg", "<u8", 2)])
+                        ("outsrc", "u1", 16), ("cphys", "u1", 48), ("btb", "u1", (2, 8)), ("bimg", "<u8", 2),
+                        ("smask", "<u2", 4)], align=True)
 
 
 def _sw128_offsets_bf16(rows):
