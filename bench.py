@@ -36,8 +36,8 @@ independent replicas, one per GPU (the path does not shard on one GPU).
 
 Other workloads (``--workload``), one JSON line each:
   precision  32-qubit complex64 brickwork of Haar SU(4) gates, 20 layers,
-             fused 5-qubit blocks on the tensor cores (split-BF16 products,
-             FP32 accumulation): layers/s,
+             5-qubit blocks formed by the planner on the tensor cores
+             (split-BF16 products, FP32 accumulation): layers/s,
              speed-up over the complex128 path on the same circuit, and the
              infidelity against complex128 at n=28.
   batch      4096 hardware-efficient-ansatz circuits (n uniform in 10..22,
@@ -557,9 +557,10 @@ def run_precision(args):
 
     n, L = args.nqubits, args.layers
     gates = circuits.brickwork_su4(n, L, args.seed)
-    cfg = {"workload": f"brickwork of Haar SU(4) gates, n={n}, {L} layers, complex64, gateScheduling + "
-                       f"gateFusion(5) into 5-qubit blocks on tensor cores (split-BF16 x3); complex128 comparison on the "
-                       f"unfused circuit (its faster plan)", "nqubits": n, "layers": L, "gates": len(gates),
+    cfg = {"workload": f"brickwork of Haar SU(4) gates, n={n}, {L} layers, complex64, fused by the planner's block "
+                       f"selector into 5-qubit blocks on tensor cores (split-BF16 x3), two per pass; complex128 "
+                       f"comparison on the same circuit (register-stage plan)", "nqubits": n, "layers": L,
+           "gates": len(gates),
            "seed": args.seed,
            "state_bytes": 8 << n, "l2": "state larger than L2; no flush needed", "parallelism": "replicas"}
     if args.impl == "reference":
@@ -577,10 +578,11 @@ def run_precision(args):
                                       "d2h_bytes_per_step": 0})))
         return
     torch.cuda.set_device(0)
-    circ = K.Circuit(n, gates)  # complex128 plan: register stages, dense SU(4) as shared-memory ops
-    fused = K.Circuit(n, gates)  # complex64 plan: gateFusion(5) blocks on the tensor cores
-    fused.gateScheduling()
-    fused.gateFusion(5, 1e-6)
+    circ = K.Circuit(n, gates)  # complex128 plan: register stages, each SU(4) a dense two-qubit register op
+    # complex64 plan: the planner packs the gates into 5-qubit blocks itself
+    # (a prior gateFusion(5) pass leaves 3-5-qubit dense gates that fit its
+    # blocks less well: 29 passes against 27).
+    fused = K.Circuit(n, gates)
     sim = K.Simulator(fused, 1, K.C64, 0)
     passes = sim.passes()
     stream = torch.cuda.Stream()
@@ -617,8 +619,6 @@ def run_precision(args):
     nf = min(n, 28)
     cf = K.Circuit(nf, circuits.brickwork_su4(nf, L, args.seed))
     cf64 = K.Circuit(nf, circuits.brickwork_su4(nf, L, args.seed))
-    cf64.gateScheduling()
-    cf64.gateFusion(5, 1e-6)
     a = K.Simulator(cf64, 1, K.C64, 0)
     a.execute()
     psi64 = a.state()

@@ -216,6 +216,134 @@ std::vector<int> greedy_pass(const std::vector<PGate>& pg, const std::vector<int
     return exec;
 }
 
+// ---- complex64 passes: tensor-core blocks ----
+// A complex64 pass applies at most KATE_C64_MAX_BLOCKS dense blocks of at
+// most five qubits, all inside one m-qubit tile, each block the product of a
+// set of gates. The selector builds the pass block by block: for every gate
+// that is ready (all earlier gates on its qubits taken), it grows a qubit set
+// from the gate's qubits, up to five, one ready gate's qubits at a time,
+// keeping the growth that lets the set absorb the most gates; the set that
+// absorbs the most gates overall becomes the next block. A set absorbs every
+// remaining gate inside it whose earlier gates (on any of its qubits) are
+// taken, so on a brickwork a block holds a light cone of about 5.5 gates
+// instead of the 3.7 of a program-order prefix (32-qubit SU(4) brickwork,
+// 20 layers: 27 passes of 53 blocks against 42 passes of 83).
+
+// Gates of `live` (program order) that lie inside Q and follow only gates
+// already taken: one scan, which stops once every qubit of Q is blocked.
+int absorb_set(const std::vector<uint64_t>& gm, const std::vector<int>& live, uint64_t Q, std::vector<int>* out,
+               size_t scan_limit) {
+    uint64_t blocked = 0;
+    int cnt = 0;
+    size_t scanned = 0;
+    for (int gi : live) {
+        if (++scanned > scan_limit) break;
+        const uint64_t q = gm[gi];
+        if (!(q & ~Q) && !(q & blocked)) {
+            cnt++;
+            if (out) out->push_back(gi);
+        } else {
+            blocked |= q;
+            if ((blocked & Q) == Q) break;
+        }
+    }
+    return cnt;
+}
+
+// Ready gates of `live` once the gates marked in `skip` are taken.
+void ready_gates(const std::vector<uint64_t>& gm, const std::vector<int>& live, const std::vector<char>& skip,
+                 uint64_t all, size_t scan_limit, std::vector<int>& out) {
+    out.clear();
+    uint64_t blocked = 0;
+    size_t scanned = 0;
+    for (int gi : live) {
+        if (skip[gi]) continue;
+        if (++scanned > scan_limit || blocked == all) break;
+        const uint64_t q = gm[gi];
+        if (!(q & blocked)) out.push_back(gi);
+        blocked |= q;
+    }
+}
+
+// One complex64 pass: the gates of up to `maxb` blocks, block by block (a
+// valid execution order), drawn from `rem` (program order). `inT`/`tsize`
+// hold the tile qubits required already (the low physical bits) and receive
+// the blocks' qubits; `order` (optional) records qubits as they join.
+std::vector<int> c64_pass(const std::vector<PGate>& pg, const std::vector<int>& rem, int n, int m, int maxb,
+                          std::vector<char>& inT, int& tsize, std::vector<int>* order, size_t scan_limit) {
+    std::vector<uint64_t> gm(pg.size(), 0);
+    for (int gi : rem) {
+        uint64_t q = 0;
+        for (int x : pg[gi].tq) q |= 1ull << x;
+        for (int x : pg[gi].fq) q |= 1ull << x;
+        gm[gi] = q;
+    }
+    const uint64_t all = n >= 64 ? ~0ull : ((1ull << n) - 1);
+    uint64_t T = 0;
+    for (int q = 0; q < n; q++)
+        if (inT[q]) T |= 1ull << q;
+    std::vector<int> live(rem), exec, ready, seeds, tmp;
+    std::vector<char> mark(pg.size(), 0);
+    for (int b = 0; b < maxb && !live.empty(); b++) {
+        std::fill(mark.begin(), mark.end(), 0);
+        ready_gates(gm, live, mark, all, scan_limit, seeds);
+        int best_cnt = 0, best_tile = 0;
+        uint64_t best_Q = 0;
+        for (int s : seeds) {
+            uint64_t Q = gm[s];
+            if (__builtin_popcountll(Q) > 5 || __builtin_popcountll(T | Q) > m) continue;
+            tmp.clear();
+            int cnt = absorb_set(gm, live, Q, &tmp, scan_limit);
+            while (__builtin_popcountll(Q) < 5) {
+                for (int gi : tmp) mark[gi] = 1;
+                ready_gates(gm, live, mark, all, scan_limit, ready);
+                for (int gi : tmp) mark[gi] = 0;
+                int gc = cnt, gsize = 0;
+                uint64_t gQ = 0;
+                for (int gi : ready) {
+                    const uint64_t nQ = Q | gm[gi];
+                    const int sz = __builtin_popcountll(nQ);
+                    if (nQ == Q || sz > 5 || __builtin_popcountll(T | nQ) > m) continue;
+                    const int c2 = absorb_set(gm, live, nQ, nullptr, scan_limit);
+                    if (c2 > gc || (c2 == gc && gQ && sz < gsize)) {
+                        gc = c2;
+                        gQ = nQ;
+                        gsize = sz;
+                    }
+                }
+                if (!gQ) break;
+                Q = gQ;
+                tmp.clear();
+                cnt = absorb_set(gm, live, Q, &tmp, scan_limit);
+            }
+            const int tile = __builtin_popcountll(T | Q);
+            if (cnt > best_cnt || (cnt == best_cnt && tile < best_tile)) {
+                best_cnt = cnt;
+                best_Q = Q;
+                best_tile = tile;
+            }
+        }
+        if (best_cnt == 0) break;
+        tmp.clear();
+        absorb_set(gm, live, best_Q, &tmp, scan_limit);
+        for (int gi : tmp) mark[gi] = 1;
+        exec.insert(exec.end(), tmp.begin(), tmp.end());
+        for (int q = 0; q < n; q++)
+            if (((best_Q >> q) & 1ull) && !inT[q]) {
+                inT[q] = 1;
+                tsize++;
+                if (order) order->push_back(q);
+            }
+        T |= best_Q;
+        std::vector<int> nl;
+        nl.reserve(live.size());
+        for (int gi : live)
+            if (!mark[gi]) nl.push_back(gi);
+        live.swap(nl);
+    }
+    return exec;
+}
+
 }  // namespace
 
 DevPass to_devpass(int n, const PlannedPass& p, int op0) {
@@ -395,6 +523,7 @@ std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out) {
     std::vector<int> rem(plan.pgates.size());
     std::iota(rem.begin(), rem.end(), 0);
     const size_t scan_limit = 1u << 20;
+    const size_t c64_scan_limit = 1u << 13;  // the block selector scans this window of the remaining gates
     while (!rem.empty()) {
         std::vector<char> inT(n, 0);
         int tsize = 0;
@@ -402,15 +531,12 @@ std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out) {
             inT[L.inv[p]] = 1;
             tsize++;
         }
-        std::vector<int> exec = greedy_pass(plan.pgates, rem, n, mg, inT, tsize, nullptr, scan_limit, opt.c64);
+        const bool blocks = opt.c64 && m == KATE_TILE_BITS;
+        std::vector<int> exec = blocks ? c64_pass(plan.pgates, rem, n, mg, KATE_C64_MAX_BLOCKS, inT, tsize, nullptr,
+                                                  c64_scan_limit)
+                                       : greedy_pass(plan.pgates, rem, n, mg, inT, tsize, nullptr, scan_limit, opt.c64);
         size_t keep = exec.size();
-        if ((int)keep > opt.max_gates_per_pass) keep = opt.max_gates_per_pass;
-        if (opt.c64 && m == KATE_TILE_BITS) {
-            std::vector<int> which = block_partition(plan.pgates, exec);
-            size_t k = 0;
-            while (k < which.size() && which[k] < KATE_C64_MAX_BLOCKS) k++;
-            keep = std::min(keep, k);
-        }
+        if (!blocks && (int)keep > opt.max_gates_per_pass) keep = opt.max_gates_per_pass;
         if (keep < exec.size()) {
             // Keep a prefix of the executable gates (a prefix of a
             // dependency-closed set in program order is dependency-closed).
@@ -442,13 +568,13 @@ std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out) {
                 tsize++;
             }
         {
+            // exec is in block order for complex64 passes, so remove by mark.
+            std::vector<char> taken(plan.pgates.size(), 0);
+            for (int g : exec) taken[g] = 1;
             std::vector<int> nr;
             nr.reserve(rem.size());
-            size_t e = 0;
-            for (int g : rem) {
-                if (e < exec.size() && exec[e] == g) e++;
-                else nr.push_back(g);
-            }
+            for (int g : rem)
+                if (!taken[g]) nr.push_back(g);
             rem.swap(nr);
         }
         // Tile bits in ascending physical order.
@@ -462,7 +588,10 @@ std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out) {
             std::vector<char> inT2(n, 0);
             int ts2 = 0;
             std::vector<int> order;
-            greedy_pass(plan.pgates, rem, n, mg, inT2, ts2, &order, scan_limit, opt.c64);
+            if (blocks)
+                c64_pass(plan.pgates, rem, n, mg, KATE_C64_MAX_BLOCKS, inT2, ts2, &order, c64_scan_limit);
+            else
+                greedy_pass(plan.pgates, rem, n, mg, inT2, ts2, &order, scan_limit, opt.c64);
             for (int q : order)
                 if (inT[q] && (int)newlow.size() < c) newlow.push_back(q);
         }

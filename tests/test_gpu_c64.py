@@ -31,13 +31,16 @@ def test_c64_random_circuits(oracle, n):
     assert np.abs(got - ref).max() <= 1e-4
 
 
-def test_c64_brickwork_su4_fused_blocks(oracle):
+@pytest.mark.parametrize("fuse", [False, True])
+def test_c64_brickwork_su4_fused_blocks(oracle, fuse):
     n = 16
     gates = circuits.brickwork_su4(n, 8, seed=3)
     c = K.Circuit(n, gates)
-    c.gateScheduling()
-    c.gateFusion(5, 1e-6)
+    if fuse:
+        c.gateScheduling()
+        c.gateFusion(5, 1e-6)
     sim = K.Simulator(c, 1, K.C64)
+    assert all(k == 3 for k in sim.pass_kernels())  # every pass on the tensor cores
     sim.execute()
     assert infidelity(sim.state(), oracle.simulate(n, gates)) <= 1e-6
 

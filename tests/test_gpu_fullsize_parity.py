@@ -49,12 +49,16 @@ def test_layered_n30_20_layers_matches_kate_gpu_path_amplitudes():
     assert worst <= 1e-12, worst
 
 
-def test_brickwork_n28_complex64_tensor_cores_infidelity():
+@pytest.mark.parametrize("fuse", [False, True])
+def test_brickwork_n28_complex64_tensor_cores_infidelity(fuse):
+    # fuse=False is the precision workload's plan (the planner forms the
+    # 5-qubit blocks); fuse=True first runs the reference's gateFusion(5).
     n, L = 28, 20
     gates = circuits.brickwork_su4(n, L, seed=1234)
     f = K.Circuit(n, gates)
-    f.gateScheduling()
-    f.gateFusion(5, 1e-6)
+    if fuse:
+        f.gateScheduling()
+        f.gateFusion(5, 1e-6)
     a = K.Simulator(f, 1, K.C64, 0)
     assert all(k == 3 for k in a.pass_kernels())  # every pass on the tensor cores
     a.execute()

@@ -152,17 +152,20 @@ def test_multi_qubit_diagonals_become_register_ops(oracle, seed):
     assert np.abs(pv.run_staged(zero_state(n)) - oracle.simulate(n, gates)).max() <= 1e-12
 
 
+@pytest.mark.parametrize("fuse", [True, False])
 @pytest.mark.parametrize("seed", range(3))
-def test_c64_block_programs_match_oracle(oracle, seed):
+def test_c64_block_programs_match_oracle(oracle, seed, fuse):
     """Complex64 plans: each pass's 5-qubit blocks, read back from their BF16
     hi/lo operand images and applied as the tensor-core kernel does, give the
-    oracle's state (the image split keeps about 16 bits per entry)."""
+    oracle's state (the image split keeps about 16 bits per entry); with and
+    without the reference's gateFusion before planning."""
     rng = np.random.default_rng(700 + seed)
     n = 13 + seed
     gates = circuits.brickwork_su4(n, 6, seed=seed) + random_circuit(n, 40, rng, kinds=("h", "cnot", "crk", "d1", "d2"))
     c = K.Circuit(n, gates)
-    c.gateScheduling()
-    c.gateFusion(5, 1e-6)
+    if fuse:
+        c.gateScheduling()
+        c.gateFusion(5, 1e-6)
     pv = PlanView(c, 12, 4, 4)
     assert any(bp is not None for bp in pv.block_programs)
     got = pv.run_blocks(zero_state(n))
@@ -170,6 +173,17 @@ def test_c64_block_programs_match_oracle(oracle, seed):
     a, b = got / np.linalg.norm(got), ref / np.linalg.norm(ref)
     assert 1 - abs(np.vdot(a, b)) ** 2 <= 1e-8
     assert np.abs(got - ref).max() <= 1e-4
+
+
+def test_c64_block_selector_packs_light_cones():
+    # 32-qubit SU(4) brickwork, 20 layers (310 gates): blocks of at most five
+    # qubits, two per pass. Program-order prefixes gave 42 passes of 83
+    # blocks; the light-cone selector 27 passes of 54 blocks.
+    n = 32
+    pv = PlanView(K.Circuit(n, circuits.brickwork_su4(n, 20, seed=1234)), 12, 4, 4)
+    assert all(bp is not None for bp in pv.block_programs)
+    nblocks = sum(int(bp["nblocks"]) for bp in pv.block_programs)
+    assert len(pv.passes) <= 28 and nblocks <= 56, (len(pv.passes), nblocks)
 
 
 def _warp_local_violations(prog):
