@@ -69,6 +69,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "30q layers/s"
+
+
+def metric_name(n):
+    """The headline metric; another qubit count names its own."""
+    return METRIC if n == 30 else f"{n}q layers/s"
 UNIT = "layers/s"
 
 
@@ -358,7 +363,7 @@ def run_reference(args):
               f"reference CPUSimulator (gateScheduling+gateFusion(5)+gateGrouping(12)), gate phase only, "
               f"{cores} threads")
     cfg = dict(workload_config(args), reference_sample=sample)
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+    line = {"metric": metric_name(args.nqubits), "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c128 (f64)", "data": "synthetic",
             "impl": "reference", "config": cfg,
@@ -491,7 +496,7 @@ def main():
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {e}"}
 
     if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        line = {"metric": metric_name(args.nqubits), "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "c128 (f64)", "data": "synthetic (seeded angles)",
                 "config": workload_config(args),
@@ -879,7 +884,8 @@ def run_batch(args):
     b = K.Batch(circs, precision=K.C64, autotune=not args.no_autotune)
     create_s = time.perf_counter() - t0
     tune = {n: {"fusion_k": b.options.tune[n].fusion, "max_gates": b.options.tune[n].max_gates,
-                "group_m": b.options.tune[n].group_qubits, "coalesce_c": b.options.tune[n].coalesce}
+                "group_m": b.options.tune[n].group_qubits, "coalesce_c": b.options.tune[n].coalesce,
+                "tensor_blocks": b.options.tune[n].blocks}
             for n in sorted(set(ns))}
     info = b.info()
     b.time(max(1, args.warmup))

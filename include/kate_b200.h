@@ -154,6 +154,21 @@ KATE_API kate_status kate_circuit_get_permutations(const kate_circuit* c, int* i
  * ints (k <= 10), out_mat 2*4^k doubles. */
 KATE_API kate_status kate_merge_gates(const kate_circuit* c, int begin, int end, int* out_qbits, int* k, double* out_mat);
 
+/* mergeGate(to_merge, stream) on the GPU  HIPcode/GateMerger.hpp:12-109:
+ * the same product as kate_merge_gates, computed on CUDA device `device`
+ * on `stream` (a cudaStream_t; NULL: the default stream), one CTA per basis
+ * column, and bit-identical to kate_merge_gates (every product and sum
+ * rounded on its own, in the host merger's order). Returns after the
+ * result is in out_mat. KATE_EINVAL without such a device: there is no
+ * silent host fallback (kate_merge_gates is the host merger). */
+KATE_API kate_status kate_merge_gates_device(const kate_circuit* c, int begin, int end, int device, void* stream,
+                                             int* out_qbits, int* k, double* out_mat);
+/* gateFusion(qbitsizelimit, merge_time_matters) with its merges on the GPU
+ * (Circuit.hpp:99-175 with the merge of :168 replaced by the device merger,
+ * every merged block of the pass in one launch on `device`): the same
+ * intervals and bit-identical matrices as kate_circuit_fuse. */
+KATE_API kate_status kate_circuit_fuse_device(kate_circuit* c, int qbitsizelimit, double merge_time_matters, int device);
+
 /* exportqcx(filename)  Circuit.hpp:763-774 */
 KATE_API kate_status kate_circuit_export_qcx(const kate_circuit* c, const char* path);
 
@@ -365,6 +380,9 @@ typedef struct {
     int max_gates; /* gates per pass program (0: default) */
     int group_qubits; /* m: qubits one pass's gates may span, 6..12, as gateGrouping(m) (0: 12) */
     int coalesce;  /* c: low physical bits every pass keeps in its tile, 1..6 (0: 4) */
+    int blocks;    /* 1: complex64 circuits whose state is kept in device memory (more than 12 qubits) run
+                      their passes as dense 5-qubit blocks on the tensor cores (the simulator's complex64
+                      form) instead of register-staged programs; 0: register-staged */
 } kate_batch_tuning;
 typedef struct {
     int chunk;                 /* cosets (4096-amplitude tiles) per pass task; 0: default */
@@ -379,8 +397,10 @@ typedef struct {
 /* Defaults (no window, default tuning for every qubit count). */
 KATE_API kate_status kate_batch_options_default(kate_batch_options* opt);
 /* The autotuner: for each qubit count present in `circuits`, times
- * candidate (fusion, max_gates) plans of a sample of those circuits on
- * `device` and writes the fastest into opt->tune. */
+ * candidate plans of a sample of those circuits on `device` (fusion x
+ * max_gates, then group_qubits, then coalesce, then, for complex64 states
+ * kept in device memory, tensor-core blocks) and writes the fastest into
+ * opt->tune. */
 KATE_API kate_status kate_batch_autotune(const kate_circuit* const* circuits, int count, int precision, int device,
                                          kate_batch_options* opt);
 /* opt: nullable (defaults). precision: KATE_C64 or KATE_C128. */
@@ -398,6 +418,9 @@ KATE_API kate_status kate_batch_expect_z(kate_batch* b, double* out);
 KATE_API kate_status kate_batch_num_outputs(const kate_batch* b, long long* out);
 /* info[0] tasks, info[1] pass programs, info[2] arena bytes, info[3] CTAs. */
 KATE_API kate_status kate_batch_info(const kate_batch* b, long long* info);
+/* Pass programs of the batch that run as tensor-core block passes
+ * (kate_batch_tuning.blocks). */
+KATE_API kate_status kate_batch_block_programs(const kate_batch* b, long long* out);
 /* Per circuit i: programs[i] pass programs, resident_qubits[i] qubits of
  * its device state (0 when it runs in shared memory). Arrays of count. */
 KATE_API kate_status kate_batch_circuit_info(const kate_batch* b, int* programs, int* resident_qubits);

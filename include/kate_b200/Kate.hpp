@@ -231,6 +231,11 @@ public:
     void gateFusion(int qbitsizelimit = 5, double merge_time_matters = 0.000001) {
         check(kate_circuit_fuse(h_, qbitsizelimit, merge_time_matters));
     }
+    // gateFusion with every merge of the pass on CUDA device `device` (one
+    // launch; the same gates, bit for bit).
+    void gateFusion(int qbitsizelimit, double merge_time_matters, int device) {
+        check(kate_circuit_fuse_device(h_, qbitsizelimit, merge_time_matters, device));
+    }
     void gateGrouping(int qbitgroupsize = 8) { check(kate_circuit_group(h_, qbitgroupsize)); }
     void allocate(int numberofgpulog2 = 0, int maxlocalqbitnumber = 300) {
         check(kate_circuit_allocate(h_, numberofgpulog2, maxlocalqbitnumber));
@@ -334,8 +339,8 @@ private:
 };
 using QuantumCircuit = Circuit;
 
-// mergeGate / CPUmergeGate (CPUcode/GateMerger.hpp:8-55).
-inline Gate mergeGate(std::vector<Gate> gates) {
+namespace detail {
+inline Gate merge_gates(const std::vector<Gate>& gates, bool on_device, void* stream, int device) {
     int n = 0;
     for (auto& g : gates)
         for (int q : g.qbits) n = q + 1 > n ? q + 1 : n;
@@ -344,11 +349,25 @@ inline Gate mergeGate(std::vector<Gate> gates) {
     std::vector<int> q(64);
     int k = 0;
     std::vector<double> m(2 * 1024 * 1024);
-    check(kate_merge_gates(c.handle(), 0, (int)gates.size(), q.data(), &k, m.data()));
+    if (on_device)
+        check(kate_merge_gates_device(c.handle(), 0, (int)gates.size(), device, stream, q.data(), &k, m.data()));
+    else
+        check(kate_merge_gates(c.handle(), 0, (int)gates.size(), q.data(), &k, m.data()));
     q.resize(k);
     Matrix<Complex> mat(1 << k);
     for (size_t i = 0; i < mat.storage.size(); i++) mat.storage[i] = Complex(m[2 * i], m[2 * i + 1]);
     return Gate(mat, q);
+}
+}  // namespace detail
+
+// mergeGate / CPUmergeGate (CPUcode/GateMerger.hpp:8-55): on the host.
+inline Gate mergeGate(std::vector<Gate> gates) { return detail::merge_gates(gates, false, nullptr, 0); }
+inline Gate CPUmergeGate(std::vector<Gate> gates) { return detail::merge_gates(gates, false, nullptr, 0); }
+// mergeGate(to_merge, stream) of the GPU build (HIPcode/GateMerger.hpp:43-109):
+// on CUDA device `device`, on `stream` (a cudaStream_t), bit-identical to
+// the host merger.
+inline Gate mergeGate(std::vector<Gate> gates, void* stream, int device = 0) {
+    return detail::merge_gates(gates, true, stream, device);
 }
 
 // Simulator (HIPcode/simulator.hpp:220-811) on one B200. number_of_gpu and

@@ -178,8 +178,14 @@ class Circuit:
     def gateScheduling(self):
         _check(self._lib.kate_circuit_schedule(self._h))
 
-    def gateFusion(self, qbitsizelimit: int = 5, merge_time_matters: float = 0.000001):
-        _check(self._lib.kate_circuit_fuse(self._h, int(qbitsizelimit), float(merge_time_matters)))
+    def gateFusion(self, qbitsizelimit: int = 5, merge_time_matters: float = 0.000001, device: Optional[int] = None):
+        """gateFusion; with `device`, every merge of the pass runs on that
+        CUDA device in one launch (same intervals, bit-identical matrices)."""
+        if device is None:
+            _check(self._lib.kate_circuit_fuse(self._h, int(qbitsizelimit), float(merge_time_matters)))
+        else:
+            _check(self._lib.kate_circuit_fuse_device(self._h, int(qbitsizelimit), float(merge_time_matters),
+                                                      int(device)))
 
     def gateGrouping(self, qbitgroupsize: int = 8):
         _check(self._lib.kate_circuit_group(self._h, int(qbitgroupsize)))
@@ -319,13 +325,19 @@ class Circuit:
             out += "\n\n"
         return out + "-----------------------------\n"
 
-    def merge(self, begin: int, end: int) -> Gate:
-        """mergeGate of gates [begin, end) of this circuit."""
+    def merge(self, begin: int, end: int, device: Optional[int] = None, stream: int = 0) -> Gate:
+        """mergeGate of gates [begin, end) of this circuit; on CUDA device
+        `device` (on `stream`, a cudaStream_t value) when given."""
         q = np.zeros(64, dtype=np.int32)
         d = np.zeros(2 * 4 ** 10, dtype=np.float64)
         k = ctypes.c_int()
-        _check(self._lib.kate_merge_gates(self._h, int(begin), int(end), q.ctypes.data_as(_ip), ctypes.byref(k),
-                                          d.ctypes.data_as(_dp)))
+        if device is None:
+            _check(self._lib.kate_merge_gates(self._h, int(begin), int(end), q.ctypes.data_as(_ip), ctypes.byref(k),
+                                              d.ctypes.data_as(_dp)))
+        else:
+            _check(self._lib.kate_merge_gates_device(self._h, int(begin), int(end), int(device),
+                                                     ctypes.c_void_p(int(stream)), q.ctypes.data_as(_ip),
+                                                     ctypes.byref(k), d.ctypes.data_as(_dp)))
         dim = 1 << k.value
         return Gate(d[: 2 * dim * dim].view(np.complex128).reshape(dim, dim).copy(), [int(x) for x in q[: k.value]])
 
@@ -370,13 +382,15 @@ def printGpuInfo():
     print(f"Shared memory per block : {sm}\n")
 
 
-def mergeGate(gates: Sequence[Gate]) -> Gate:
-    """CPUmergeGate / mergeGate (CPUcode/GateMerger.hpp:8-55): FP64 product
-    of the gates on the sorted union of their qubits."""
+def mergeGate(gates: Sequence[Gate], device: Optional[int] = None, stream: int = 0) -> Gate:
+    """CPUmergeGate / mergeGate (CPUcode/GateMerger.hpp:8-55,
+    HIPcode/GateMerger.hpp:43-109): FP64 product of the gates on the sorted
+    union of their qubits; on CUDA device `device` when given (the same
+    matrix, bit for bit)."""
     gs = [g if isinstance(g, Gate) else Gate(g[3] if g[0] == DENSE else g[0], g[1], g[2]) for g in gates]
     n = 1 + max(q for g in gs for q in g.qbits)
     c = Circuit(n, gs)
-    return c.merge(0, len(gs))
+    return c.merge(0, len(gs), device=device, stream=stream)
 
 
 class Simulator:
@@ -588,7 +602,9 @@ class Batch:
     def info(self) -> dict:
         v = (ctypes.c_longlong * 4)()
         _check(self._lib.kate_batch_info(self._h, v))
-        return {"tasks": v[0], "programs": v[1], "arena_bytes": v[2], "ctas": v[3]}
+        nb = ctypes.c_longlong()
+        _check(self._lib.kate_batch_block_programs(self._h, ctypes.byref(nb)))
+        return {"tasks": v[0], "programs": v[1], "arena_bytes": v[2], "ctas": v[3], "block_programs": nb.value}
 
     def create_times(self) -> dict:
         """Host wall time of the batch's creation, in ms, per phase."""

@@ -44,6 +44,8 @@ SIGNATURES = {
     "kate_circuit_get_instruction": [_vp, _i, _ip, _ip, _ip],
     "kate_circuit_get_permutations": [_vp, _ip, _ip, _ip],
     "kate_merge_gates": [_vp, _i, _i, _ip, _ip, _dp],
+    "kate_merge_gates_device": [_vp, _i, _i, _i, _vp, _ip, _ip, _dp],
+    "kate_circuit_fuse_device": [_vp, _i, _d, _i],
     "kate_circuit_export_qcx": [_vp, _c.c_char_p],
     "kate_sim_create": [_vp, _i, _i, _vpp],
     "kate_sim_destroy": [_vp],
@@ -91,6 +93,7 @@ SIGNATURES = {
     "kate_batch_expect_z": [_vp, _dp],
     "kate_batch_num_outputs": [_vp, _c.POINTER(_c.c_longlong)],
     "kate_batch_info": [_vp, _c.POINTER(_c.c_longlong)],
+    "kate_batch_block_programs": [_vp, _c.POINTER(_c.c_longlong)],
     "kate_batch_time": [_vp, _i, _c.POINTER(_c.c_float)],
     "kate_batch_circuit_info": [_vp, _ip, _ip],
     "kate_batch_create_times": [_vp, _dp],
@@ -109,7 +112,8 @@ KATE_BATCH_MAX_QUBITS = 28
 
 
 class BatchTuning(_c.Structure):
-    _fields_ = [("fusion", _c.c_int), ("max_gates", _c.c_int), ("group_qubits", _c.c_int), ("coalesce", _c.c_int)]
+    _fields_ = [("fusion", _c.c_int), ("max_gates", _c.c_int), ("group_qubits", _c.c_int), ("coalesce", _c.c_int),
+                ("blocks", _c.c_int)]
 
 
 class BatchOptions(_c.Structure):

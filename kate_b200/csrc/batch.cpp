@@ -39,7 +39,7 @@ uint64_t put_bytes(std::vector<uint8_t>& blob, const void* p, size_t bytes) {
 
 }  // namespace
 
-std::string pack_circuit(const Program& in, const BatchTune& tune, bool resident, CircPack& out) {
+std::string pack_circuit(const Program& in, const BatchTune& tune, bool resident, CircPack& out, bool c64) {
     Program p = in;
     const int n = p.nqbits;
     if (n < 1 || n > KATE_BATCH_MAX_QUBITS) return "batch circuits have 1 to 28 qubits";
@@ -75,9 +75,24 @@ std::string pack_circuit(const Program& in, const BatchTune& tune, bool resident
     o.staged = true;
     o.c64 = false;
     o.max_gates_per_pass = std::max(1, tune.max_gates);
+    // Tensor-core block passes for a complex64 state kept in HBM; a plan
+    // with any pass the blocks cannot take keeps register-staged programs.
     Plan plan;
-    e = build_plan(p, o, &plan);
-    if (!e.empty()) return e;
+    out.blocks = false;
+    if (c64 && tune.blocks && !out.small && out.n_sim >= KATE_TILE_BITS) {
+        PlanOptions ob = o;
+        ob.c64 = true;
+        ob.staged = false;
+        e = build_plan(p, ob, &plan);
+        bool all = e.empty() && !plan.passes.empty();
+        for (const PlannedPass& pp : plan.passes) all = all && pp.bprog != nullptr;
+        out.blocks = all;
+    }
+    if (!out.blocks) {
+        plan = Plan();
+        e = build_plan(p, o, &plan);
+        if (!e.empty()) return e;
+    }
     for (int x = 0; x < n; x++) out.zbit.push_back((uint8_t)plan.final_phys[plan.label_to_logical[x]]);
     out.pool = plan.pool;
     out.sops = plan.smem_ops;
@@ -101,7 +116,18 @@ std::string pack_circuit(const Program& in, const BatchTune& tune, bool resident
         header(&pp, bp);
         if (bp.m != KATE_TILE_BITS) return "internal: batch pass tile is not 12 qubits";
         if (!out.small && bp.tphys[0] != 0) return "internal: batch pass tile does not hold physical bit 0";
-        if (pp.prog) {
+        if (out.blocks) {
+            BlockProg b = *pp.bprog;
+            const uint64_t at = put_bytes(out.blob, &b, sizeof(BlockProg));
+            for (int k = 0; k < b.nblocks; k++) {
+                const uint64_t img = put_bytes(out.blob, plan.bimg.data() + pp.bprog->bimg[k], KATE_BLOCK_IMG_BYTES);
+                b.bimg[k] = img - at;
+            }
+            std::memcpy(out.blob.data() + at, &b, sizeof(BlockProg));
+            bp.flags = BPROG_BLOCK;
+            bp.nstages = 0;
+            bp.ops_off = at;
+        } else if (pp.prog) {
             const PassProg& P = *pp.prog;
             bp.nops = P.nops;
             bp.nmats = P.nmats;
@@ -150,12 +176,12 @@ void for_each_item(size_t count, F f) {
 }
 
 // Plans every circuit on host threads.
-std::vector<CircPack> pack_all(const std::vector<const Program*>& circuits, const BatchOptions& opt) {
+std::vector<CircPack> pack_all(const std::vector<const Program*>& circuits, const BatchOptions& opt, bool c64) {
     std::vector<CircPack> packs(circuits.size());
     for_each_item(circuits.size(), [&](size_t i) {
         const BatchTune& tu = opt.for_n(circuits[i]->nqbits);
         try {
-            packs[i].err = pack_circuit(*circuits[i], tu, false, packs[i]);
+            packs[i].err = pack_circuit(*circuits[i], tu, false, packs[i], c64);
         } catch (const std::exception& ex) {
             packs[i].err = ex.what();
         }
@@ -219,6 +245,8 @@ struct BatchImpl {
     double create_ms[4] = {0, 0, 0, 0};  // planning, assembly, device buffers + uploads, graph
     uint64_t upload_bytes = 0;           // host-to-device bytes copied by create()
     uint64_t wait_ns = 5000000000ull;    // a dependency wait in the kernel gives up after this long
+    bool tensor_blocks = false;          // some circuit runs tensor-core block passes
+    int64_t block_programs = 0;          // pass programs run as tensor-core block passes
 
     size_t amp_bytes() const { return precision == 0 ? 16 : 8; }
 
@@ -267,7 +295,7 @@ std::string Batch::create(const std::vector<const Program*>& circuits, int preci
     using clk = std::chrono::steady_clock;
     auto ms_since = [](clk::time_point t) { return std::chrono::duration<double, std::milli>(clk::now() - t).count(); };
     clk::time_point t0 = clk::now();
-    std::vector<CircPack> packs = pack_all(circuits, opt);
+    std::vector<CircPack> packs = pack_all(circuits, opt, precision == 1);
     const double plan_ms = ms_since(t0);
     t0 = clk::now();
     for (size_t i = 0; i < packs.size(); i++)
@@ -318,6 +346,8 @@ std::string Batch::create(const std::vector<const Program*>& circuits, int preci
                 S->arena_amps += 1ull << P.n_sim;
             }
             S->circs[i] = bc;
+            S->tensor_blocks = S->tensor_blocks || P.blocks;
+            if (P.blocks) S->block_programs += (int64_t)P.progs.size();
             S->cprogs[i] = (int)P.progs.size();
             S->cres[i] = P.small ? 0 : P.n_sim;
         }
@@ -503,7 +533,7 @@ std::string Batch::create(const std::vector<const Program*>& circuits, int preci
     cudaMemsetAsync(S->d_zout, 0, sizeof(double) * std::max<int64_t>(1, S->nout), S->stream);
     cudaError_t le = launch_batch(S->d_arena, precision, S->d_tasks, (int)S->tasks.size(), S->d_circs, S->d_progs,
                                   S->d_blob, S->d_sops, S->d_pool, S->d_head, S->d_done, S->d_zout, S->d_err, grid,
-                                  S->stream, nullptr, nullptr, nullptr, S->wait_ns);
+                                  S->stream, nullptr, nullptr, nullptr, S->wait_ns, S->tensor_blocks ? 1 : 0);
     ce = cudaStreamEndCapture(S->stream, &S->graph);
     if (le != cudaSuccess) return fail(cuda_err("launch_batch", le));
     if (ce != cudaSuccess) return fail(cuda_err("cudaStreamEndCapture", ce));
@@ -586,6 +616,7 @@ void Batch::create_times(double* ms4) const {
 }
 uint64_t Batch::upload_bytes() const { return d_->upload_bytes; }
 int64_t Batch::num_programs() const { return (int64_t)d_->progs.size(); }
+int64_t Batch::num_block_programs() const { return d_->block_programs; }
 void Batch::circuit_info(int i, int* programs, int* resident_qubits) const {
     *programs = d_->cprogs[i];
     *resident_qubits = d_->cres[i];
@@ -626,7 +657,7 @@ std::string Batch::get_state(int i, double* out) {
 
 std::string batch_autotune(const std::vector<const Program*>& circuits, int precision, int device,
                            BatchOptions* opt) {
-    if (opt->tune.size() < KATE_BATCH_MAX_QUBITS + 1) opt->tune.resize(KATE_BATCH_MAX_QUBITS + 1, BatchTune{0, 0, 0, 0});
+    if (opt->tune.size() < KATE_BATCH_MAX_QUBITS + 1) opt->tune.resize(KATE_BATCH_MAX_QUBITS + 1, BatchTune{0, 0, 0, 0, 0});
     std::map<int, std::vector<const Program*>> byn;
     for (const Program* p : circuits)
         if (p) byn[p->nqbits].push_back(p);
@@ -677,6 +708,17 @@ std::string batch_autotune(const std::vector<const Program*>& circuits, int prec
                 std::string e = consider(t);
                 if (!e.empty()) return e;
             }
+        // Complex64 states kept in HBM: tensor-core blocks (the planner
+        // forms them, so no prior gateFusion) with the chosen grouping and
+        // coalescing, and with the defaults.
+        if (precision == 1 && n > KATE_BATCH_SMALL_MAX) {
+            const BatchTune cand[2] = {BatchTune{1, bt.max_gates, bt.group, bt.coalesce, 1},
+                                       BatchTune{1, kDefaultTune.max_gates, KATE_TILE_BITS, 4, 1}};
+            for (const BatchTune& t : cand) {
+                std::string e = consider(t);
+                if (!e.empty()) return e;
+            }
+        }
         opt->tune[n] = bt;
     }
     return "";

@@ -25,6 +25,7 @@ struct BatchTune {
     int max_gates = 96;  // gates per pass program
     int group = 12;      // m: qubits one pass's gates may span (gateGrouping(m)); the 12-qubit tile is filled up
     int coalesce = 4;    // c: low physical bits every pass keeps in its tile (runs of 2^c amplitudes per access)
+    int blocks = 0;      // 1: complex64 states kept in HBM run their passes as 5-qubit tensor-core blocks
 };
 
 struct BatchOptions {
@@ -50,11 +51,14 @@ struct CircPack {
     std::vector<DevOp> sops;
     std::vector<Cx> pool;
     std::vector<std::pair<uint64_t, int>> generic;  // (blob offset, count) of DevOp arrays
+    bool blocks = false;  // its passes are tensor-core block passes (BPROG_BLOCK)
 };
 
 // Plans one circuit. resident: keep the state in device memory even when it
 // would fit a tile (at least 12 qubits), so it can be sampled afterwards.
-std::string pack_circuit(const Program& in, const BatchTune& tune, bool resident, CircPack& out);
+// c64: the state is complex64, so tune.blocks may turn its passes into
+// tensor-core block passes (a state kept in HBM, at least 12 qubits).
+std::string pack_circuit(const Program& in, const BatchTune& tune, bool resident, CircPack& out, bool c64 = false);
 
 struct BatchImpl;
 
@@ -74,6 +78,7 @@ public:
     uint64_t arena_bytes() const;
     int grid() const;
     int64_t num_programs() const;
+    int64_t num_block_programs() const;  // pass programs run as tensor-core block passes
     // Host wall time of create() in ms: planning, assembly of the task queue,
     // device buffers and uploads, graph capture and instantiation.
     void create_times(double* ms4) const;

@@ -13,6 +13,7 @@
 #include "plan.hpp"
 #include "serve.hpp"
 #include "jit.hpp"
+#include "launch.hpp"
 #include "sim.hpp"
 
 struct kate_circuit {
@@ -372,6 +373,62 @@ kate_status kate_merge_gates(const kate_circuit* c, int begin, int end, int* out
     });
 }
 
+namespace {
+// The device merger as pass_fuse's block merger; ctx points at the device
+// ordinal. Merges run on the device's default stream.
+struct DeviceMergeCtx {
+    int device;
+};
+std::string device_block_merger(const std::vector<std::vector<kate::Gate>>& blocks, void* ctx,
+                                std::vector<kate::Gate>* out) {
+    return kate::merge_gates_device(blocks, static_cast<DeviceMergeCtx*>(ctx)->device, nullptr, out);
+}
+int device_count() {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+}  // namespace
+
+kate_status kate_merge_gates_device(const kate_circuit* c, int begin, int end, int device, void* stream,
+                                    int* out_qbits, int* k, double* out_mat) {
+    return guarded([&] {
+        REQUIRE(c && out_qbits && k && out_mat, "null pointer");
+        REQUIRE(begin >= 0 && end <= (int)c->prog.gates.size() && begin < end, "bad gate range");
+        REQUIRE(device >= 0 && device < device_count(), "no such CUDA device");
+        std::vector<std::vector<kate::Gate>> blocks(1);
+        blocks[0].assign(c->prog.gates.begin() + begin, c->prog.gates.begin() + end);
+        std::vector<kate::Gate> merged;
+        std::string e = kate::merge_gates_device(blocks, device, static_cast<cudaStream_t>(stream), &merged);
+        if (!e.empty()) return fail(e.rfind("cuda", 0) == 0 ? KATE_ECUDA : KATE_EINVAL, e);
+        const kate::Gate& g = merged[0];
+        *k = (int)g.qbits.size();
+        for (int i = 0; i < *k; i++) out_qbits[i] = g.qbits[i];
+        for (size_t i = 0; i < g.dense.size(); i++) {
+            out_mat[2 * i] = g.dense[i].re;
+            out_mat[2 * i + 1] = g.dense[i].im;
+        }
+        return KATE_OK;
+    });
+}
+
+kate_status kate_circuit_fuse_device(kate_circuit* c, int k, double mtm, int device) {
+    return guarded([&] {
+        REQUIRE(c, "null circuit");
+        REQUIRE(k >= 1, "qbitsizelimit must be >= 1");
+        REQUIRE(device >= 0 && device < device_count(), "no such CUDA device");
+        kate::Program tmp = c->prog;
+        DeviceMergeCtx ctx{device};
+        std::string e = kate::pass_fuse(tmp, k, mtm, device_block_merger, &ctx);
+        if (!e.empty()) return fail(e.rfind("cuda", 0) == 0 ? KATE_ECUDA : KATE_EINVAL, e);
+        c->prog = std::move(tmp);
+        return KATE_OK;
+    });
+}
+
 kate_status kate_circuit_export_qcx(const kate_circuit* c, const char* path) {
     return guarded([&] {
         REQUIRE(c && path, "null pointer");
@@ -707,10 +764,13 @@ kate::BatchOptions to_options(const kate_batch_options* o) {
     r.fault_task = o->fault_task > 0 ? o->fault_task - 1 : -1;
     r.tune.resize(KATE_BATCH_MAX_QUBITS + 1);
     for (int n = 0; n <= KATE_BATCH_MAX_QUBITS; n++) {
-        r.tune[n].fusion = o->tune[n].fusion;
-        r.tune[n].max_gates = o->tune[n].max_gates;
+        // A field left at 0 takes its default, each on its own (so a caller
+        // can set one choice, e.g. blocks, and leave the rest).
+        r.tune[n].fusion = o->tune[n].fusion > 0 ? o->tune[n].fusion : 1;
+        r.tune[n].max_gates = o->tune[n].max_gates > 0 ? o->tune[n].max_gates : 96;
         r.tune[n].group = o->tune[n].group_qubits > 0 ? o->tune[n].group_qubits : KATE_TILE_BITS;
         r.tune[n].coalesce = o->tune[n].coalesce > 0 ? o->tune[n].coalesce : 4;
+        r.tune[n].blocks = o->tune[n].blocks ? 1 : 0;
     }
     return r;
 }
@@ -753,6 +813,7 @@ kate_status kate_batch_autotune(const kate_circuit* const* circuits, int count, 
             opt->tune[n].max_gates = o.tune[n].max_gates;
             opt->tune[n].group_qubits = o.tune[n].group;
             opt->tune[n].coalesce = o.tune[n].coalesce;
+            opt->tune[n].blocks = o.tune[n].blocks;
         }
         return KATE_OK;
     });
@@ -831,6 +892,12 @@ kate_status kate_batch_info(const kate_batch* b, long long* info) {
     info[1] = (long long)b->b->num_programs();
     info[2] = (long long)b->b->arena_bytes();
     info[3] = (long long)b->b->grid();
+    return KATE_OK;
+}
+
+kate_status kate_batch_block_programs(const kate_batch* b, long long* out) {
+    REQUIRE(b && out, "null pointer");
+    *out = (long long)b->b->num_block_programs();
     return KATE_OK;
 }
 

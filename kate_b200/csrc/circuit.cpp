@@ -273,7 +273,7 @@ std::string pass_schedule(Program& p) {
 // merge intervals [i, j) with at most `limit` distinct qubits; cost 2^|q|
 // per merged block plus merge_time_matters * sum 2^|q_j| * 4^|q| / 2^n, and
 // the per-gate costs H 2, CNOT 0.75, CRk 0.25, TOFFOLI 3/8, dense 2^k.
-std::string pass_fuse(Program& p, int limit, double mtm) {
+std::string pass_fuse(Program& p, int limit, double mtm, BlockMerger merger, void* ctx) {
     const int G = (int)p.gates.size();
     if (G == 0) return "";
     if (limit > 10) return "fusion is limited to 10-qubit blocks";
@@ -303,6 +303,8 @@ std::string pass_fuse(Program& p, int limit, double mtm) {
     if (path.size() == 1 && path[0] == -1)
         return "gateFusion found no merge path (a gate has no cost entry and cannot be merged)";
     std::vector<Gate> out;
+    std::vector<std::vector<Gate>> blocks;  // merged intervals, when a block merger is given
+    std::vector<size_t> slot;               // their positions in `out`
     int f = -1;
     for (int el : path) {
         if (f == -1) {
@@ -313,12 +315,25 @@ std::string pass_fuse(Program& p, int limit, double mtm) {
             out.push_back(p.gates[f]);
         } else {
             std::vector<Gate> block(p.gates.begin() + f, p.gates.begin() + el);
-            Gate m;
-            std::string err = merge_gates(block, &m);
-            if (!err.empty()) return err;
-            out.push_back(std::move(m));
+            if (merger) {
+                slot.push_back(out.size());
+                out.emplace_back();
+                blocks.push_back(std::move(block));
+            } else {
+                Gate m;
+                std::string err = merge_gates(block, &m);
+                if (!err.empty()) return err;
+                out.push_back(std::move(m));
+            }
         }
         f = el;
+    }
+    if (merger && !blocks.empty()) {
+        std::vector<Gate> merged;
+        std::string err = merger(blocks, ctx, &merged);
+        if (!err.empty()) return err;
+        if (merged.size() != blocks.size()) return "internal: block merger returned a wrong count";
+        for (size_t b = 0; b < slot.size(); b++) out[slot[b]] = std::move(merged[b]);
     }
     p.gates = std::move(out);
     return "";

@@ -52,7 +52,12 @@ struct Program {
 // left unchanged).
 std::string validate_gate(const Program& p, const Gate& g);
 std::string pass_schedule(Program& p);
-std::string pass_fuse(Program& p, int qbitsizelimit, double merge_time_matters);
+// Merges every block of gates into one dense gate each (out[b] for
+// blocks[b]); "" on success. pass_fuse takes one to run all of its merges in
+// one call (the device merger); without one it merges on the host.
+using BlockMerger = std::string (*)(const std::vector<std::vector<Gate>>& blocks, void* ctx, std::vector<Gate>* out);
+std::string pass_fuse(Program& p, int qbitsizelimit, double merge_time_matters, BlockMerger merger = nullptr,
+                      void* ctx = nullptr);
 std::string pass_group(Program& p, int qbitgroupsize);
 std::string pass_allocate(Program& p, int numberofgpulog2, int maxlocalqbitnumber);
 std::string pass_compile_default(Program& p, int numberofgpulog2, int maxlocalqbitnumber);

@@ -188,6 +188,10 @@ typedef struct {
 // could be built, a generic one (nstages < 0: DevOp ops run on the shared
 // tile one by one). Offsets are in bytes from the blob's start.
 #define BPROG_SMEM 1  // BatchProg.flags: the staged program has SOP_SMEM ops
+// BatchProg.flags: a complex64 tensor-core block pass. ops_off is the blob
+// offset of its BlockProg, whose bimg[b] are block b's operand images as
+// byte offsets from that BlockProg (so the pair moves as one).
+#define BPROG_BLOCK 2
 
 typedef struct {
     int32_t m, ncb, nops, nmats, nstages, sop0;  // sop0: first shared-memory op in the batch's array

@@ -24,6 +24,7 @@
 // (complex128, FP64 arithmetic). <Z> sums are FP64.
 #include <cuda_runtime.h>
 
+#include "k_block.cuh"
 #include "k_stage.cuh"
 #include "launch.hpp"
 
@@ -84,8 +85,96 @@ __device__ __forceinline__ ProgView view(const BatchProg& P, const unsigned char
     return v;
 }
 
-// Dynamic shared memory of the batch kernel: the tile, then its tables.
+// Dynamic shared memory of the batch kernel: two tiles, then the program
+// tables or, for a tensor-core block task, the block region: the B operand
+// images (1024-byte aligned), the BlockProg, the block tables.
 extern __shared__ __align__(16) unsigned char batch_smem_raw[];
+constexpr uint32_t BLK_IMG = KATE_C64_MAX_BLOCKS * KATE_BLOCK_IMG_BYTES;
+constexpr uint32_t BLK_PROG = (sizeof(BlockProg) + 15) & ~15u;
+constexpr uint32_t BLK_REGION = 1024 + BLK_IMG + BLK_PROG + blk::TAB_BYTES + blk::IO_BYTES;
+static_assert(sizeof(BlockProg) % 8 == 0, "BlockProg is copied as 8-byte words");
+// Per CTA, for the whole launch (complex64 batches with block programs):
+// the products' mbarrier and its phase, the TMEM columns, the wait flag.
+__shared__ uint64_t blk_mbar;
+__shared__ uint32_t blk_tmem, blk_phase;
+__shared__ int blk_abort;
+
+// A complex64 tensor-core block pass over cosets [c0, c1) of one circuit
+// (the BatchProg's BPROG_BLOCK program): the BlockProg and its operand
+// images into shared memory, then per coset the staging tile (loaded, or
+// the tile of |0...0> for a circuit's first pass), the blocks, the
+// write-back. The two batch tile buffers are the double-buffered staging
+// tiles. Loads and stores go through L2 only (other SMs wrote the state
+// earlier in this launch). Returns false when a product wait gave up.
+__device__ __noinline__ bool block_task(float2* st, const BatchProg& BP, const unsigned char* blob, uint32_t c0,
+                                        uint32_t c1, bool first) {
+    const uint32_t t = threadIdx.x;
+    const uint32_t tmem = blk_tmem, mbar = blk::smem_u32(&blk_mbar);
+    int* abort_flag = &blk_abort;
+    uint32_t phase = blk_phase;  // every thread keeps the same copy; thread 0 stores it back
+    unsigned char* raw = batch_smem_raw + 2 * TS * sizeof(float2);
+    const uint32_t rawa = blk::smem_u32(raw);
+    const uint32_t bbase = (rawa + 1023u) & ~1023u;
+    unsigned char* g = raw + (bbase - rawa);
+    BlockProg& P = *reinterpret_cast<BlockProg*>(g + BLK_IMG);
+    uint16_t* tab = reinterpret_cast<uint16_t*>(g + BLK_IMG + BLK_PROG);
+    uint16_t* iot = reinterpret_cast<uint16_t*>(g + BLK_IMG + BLK_PROG + blk::TAB_BYTES);
+    const unsigned char* src = blob + BP.ops_off;
+    for (uint32_t i = t; i < sizeof(BlockProg) / 8; i += NT)
+        reinterpret_cast<uint64_t*>(&P)[i] = __ldcg(reinterpret_cast<const unsigned long long*>(src) + i);
+    __syncthreads();
+    for (int b = 0; b < P.nblocks; b++) {
+        const unsigned char* img = src + P.bimg[b];
+        const uint32_t dst = bbase + (uint32_t)b * KATE_BLOCK_IMG_BYTES;
+        for (uint32_t off = t * 16; off < KATE_BLOCK_IMG_BYTES; off += NT * 16)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst + off), "l"(img + off) : "memory");
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    blk::Pass X;
+    blk::setup(P, tab, iot, X);
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    float2* S0 = reinterpret_cast<float2*>(batch_smem_raw);
+    const uint32_t sb0 = blk::smem_u32(batch_smem_raw);
+    bool ok = true;
+    if (first) {
+        for (uint32_t c = c0; c < c1 && ok; c++) {
+            const uint64_t cb = blk::coset_base(P, c);
+            blk::zero_tile(S0, cb == 0);
+            __syncthreads();
+            ok = blk::apply_blocks(P, X, tab, S0, bbase, tmem, mbar, phase, abort_flag);
+            if (ok) blk::store_tile<true>(P, X, iot, st, cb, S0);
+            __syncthreads();
+        }
+        if (t == 0) blk_phase = phase;
+        return ok;
+    }
+    blk::load_tile<true>(st, blk::coset_base(P, c0), sb0, X, iot);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    uint32_t it = 0;
+    for (uint32_t c = c0; c < c1; c++, it++) {
+        const uint32_t cur = it & 1u;
+        float2* S = S0 + cur * TS;
+        // The other buffer was last read by the previous tile's write-back,
+        // closed by the barrier at the end of that iteration.
+        if (c + 1 < c1) blk::load_tile<true>(st, blk::coset_base(P, c + 1), sb0 + (cur ^ 1u) * blk::S_BYTES, X, iot);
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+        __syncthreads();
+        if (!blk::apply_blocks(P, X, tab, S, bbase, tmem, mbar, phase, abort_flag)) {
+            ok = false;
+            break;
+        }
+        blk::store_tile<true>(P, X, iot, st, blk::coset_base(P, c), S);
+        __syncthreads();
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
+    if (t == 0) blk_phase = phase;
+    return ok;
+}
 
 // The register-staged program as a call of its own, so that its registers
 // are allocated apart from the task loop's. The tile and tables are taken
@@ -314,7 +403,8 @@ __global__ void __launch_bounds__(NT, sizeof(C2) == 8 ? 2 : 1)
             const BatchProg* __restrict__ progs, const unsigned char* __restrict__ blob, const DevOp* __restrict__ sops,
             const double2* __restrict__ pool, int* __restrict__ head, int* __restrict__ done,
             double* __restrict__ zout, int* __restrict__ err, double* __restrict__ psum,
-            const double* __restrict__ unif, uint64_t* __restrict__ sout, unsigned long long wait_ns) {
+            const double* __restrict__ unif, uint64_t* __restrict__ sout, unsigned long long wait_ns,
+            int tensor_blocks) {
     // Two tile buffers (a pass task prefetches its next coset into the
     // other one), then the program tables.
     C2* tile = reinterpret_cast<C2*>(batch_smem_raw);
@@ -326,6 +416,21 @@ __global__ void __launch_bounds__(NT, sizeof(C2) == 8 ? 2 : 1)
     __shared__ double red[KATE_BATCH_MAX_QUBITS * (NT / 32) + KATE_BATCH_MAX_QUBITS];
     const uint32_t t = threadIdx.x;
     const uint32_t tb = (uint32_t)__cvta_generic_to_shared(tile);
+    // Tensor-core block tasks (complex64 only): the CTA's TMEM columns and
+    // the products' mbarrier, for the whole launch.
+    if constexpr (sizeof(C2) == 8) {
+        if (tensor_blocks) {
+            if (t == 0) {
+                asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(blk::smem_u32(&blk_mbar)) : "memory");
+                blk_abort = 0;
+                blk_phase = 0;
+            }
+            blk::tmem_alloc(&blk_tmem);
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncthreads();
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        }
+    }
     for (;;) {
         if (t == 0) {
             // After a failed wait anywhere, every CTA stops at its next task.
@@ -354,7 +459,17 @@ __global__ void __launch_bounds__(NT, sizeof(C2) == 8 ? 2 : 1)
         const int nz = circs[K.circ].n;
         const int64_t zoff = circs[K.circ].zoff;
 
-        if (K.kind == BT_SMALL || K.kind == BT_PASS) {
+        bool block_pass = false;
+        if constexpr (sizeof(C2) == 8) block_pass = K.kind == BT_PASS && (progs[K.prog].flags & BPROG_BLOCK);
+        if (block_pass) {
+            if constexpr (sizeof(C2) == 8) {
+                // tensor_blocks is set whenever the batch has block programs.
+                if (!block_task(arena + circs[K.circ].off, progs[K.prog], blob, K.c0, K.c1, K.first != 0)) {
+                    if (t == 0) atomicExch(err, 1);
+                    break;
+                }
+            }
+        } else if (K.kind == BT_SMALL || K.kind == BT_PASS) {
             // SMALL: step s runs program prog + s on the resident tile.
             // PASS: step s runs program prog on coset c0 + s.
             const bool small = K.kind == BT_SMALL;
@@ -419,11 +534,16 @@ __global__ void __launch_bounds__(NT, sizeof(C2) == 8 ? 2 : 1)
             atomicAdd(done + K.circ, 1);
         }
     }
+    if constexpr (sizeof(C2) == 8) {
+        if (tensor_blocks) blk::tmem_free(blk_tmem);
+    }
 }
 
 template <typename C2>
 constexpr size_t batch_smem() {
-    return (size_t)2 * TS * sizeof(C2) + sizeof(TileTables<C2>);
+    // complex64: the tables or the tensor-core block region, whichever is larger.
+    return (size_t)2 * TS * sizeof(C2) +
+           (sizeof(C2) == 8 && BLK_REGION > sizeof(TileTables<C2>) ? BLK_REGION : sizeof(TileTables<C2>));
 }
 
 }  // namespace
@@ -452,15 +572,16 @@ int batch_grid(int device, int prec) {
 cudaError_t launch_batch(void* arena, int prec, const BatchTask* tasks, int ntasks, const BatchCirc* circs,
                          const BatchProg* progs, const void* blob, const DevOp* sops, const void* pool, int* head,
                          int* done, double* zout, int* err, int grid, cudaStream_t s, double* psum,
-                         const double* unif, uint64_t* sout, unsigned long long wait_ns) {
+                         const double* unif, uint64_t* sout, unsigned long long wait_ns, int tensor_blocks) {
     const unsigned char* b = (const unsigned char*)blob;
     const double2* pl = (const double2*)pool;
     if (prec == 1)
         k_batch<float2><<<grid, NT, batch_smem<float2>(), s>>>((float2*)arena, tasks, ntasks, circs, progs, b, sops, pl,
-                                                               head, done, zout, err, psum, unif, sout, wait_ns);
+                                                               head, done, zout, err, psum, unif, sout, wait_ns,
+                                                               tensor_blocks);
     else
         k_batch<double2><<<grid, NT, batch_smem<double2>(), s>>>((double2*)arena, tasks, ntasks, circs, progs, b, sops,
-                                                                 pl, head, done, zout, err, psum, unif, sout, wait_ns);
+                                                                 pl, head, done, zout, err, psum, unif, sout, wait_ns, 0);
     return cudaGetLastError();
 }
 

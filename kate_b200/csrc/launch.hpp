@@ -3,6 +3,8 @@
 
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <string>
+#include <vector>
 
 #include "device_types.h"
 
@@ -35,6 +37,13 @@ size_t renorm_scratch_bytes();
 size_t sample_scratch_doubles(int n);
 cudaError_t launch_sample(const void* st, int prec, int n, const double* unif, int shots, double* scratch,
                           uint64_t* out, cudaStream_t s);
+// Device gate merger (k_merge.cu): out[b] is the product of blocks[b] as one
+// dense gate on the sorted union of its qubits (at most 10), bit-identical
+// to merge_gates (circuit.hpp); all blocks in one launch on `device`, then
+// a synchronise of `stream`. Returns "" or an error message.
+struct Gate;
+std::string merge_gates_device(const std::vector<std::vector<Gate>>& blocks, int device, cudaStream_t stream,
+                               std::vector<Gate>* out);
 constexpr size_t renorm_result_offset() { return 148 * 4 * sizeof(double); }
 cudaError_t launch_renorm_c64(void* st, int n, void* scratch, cudaStream_t s);
 
@@ -74,7 +83,7 @@ cudaError_t launch_batch(void* arena, int prec, const BatchTask* tasks, int ntas
                          const BatchProg* progs, const void* blob, const DevOp* sops, const void* pool, int* head,
                          int* done, double* zout, int* err, int grid, cudaStream_t s, double* psum = nullptr,
                          const double* unif = nullptr, uint64_t* sout = nullptr,
-                         unsigned long long wait_ns = 5000000000ull);
+                         unsigned long long wait_ns = 5000000000ull, int tensor_blocks = 0);
 int batch_grid(int device, int prec);
 
 // Bit sums: per CTA, for every local bit, the sum over amplitudes with the

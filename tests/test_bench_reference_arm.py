@@ -22,7 +22,7 @@ def _run(*args):
 
 
 @pytest.mark.skipif(not os.path.exists(REF_SO), reason="oracle/_ref/libkate_ref.so not built")
-@pytest.mark.parametrize("workload,metric,higher", [("layers", "30q layers/s", True),
+@pytest.mark.parametrize("workload,metric,higher", [("layers", "16q layers/s", True),
                                                      ("qulacs", "QulacsBench 16q wall time", False)])
 def test_reference_arm_prints_the_contract_line(workload, metric, higher):
     d = _run("--workload", workload)

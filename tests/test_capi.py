@@ -144,3 +144,18 @@ def test_device_queries_without_a_gpu_report_zero_devices():
     L = _lib.lib()
     with pytest.raises(K.KateError, match="no such CUDA device"):
         K._check(L.kate_device_properties(0, None, 0, None, None, None))
+
+
+def test_device_merger_without_a_gpu_fails_loudly():
+    # The device merger has no silent host fallback (the host merger is a
+    # separate entry point).
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("GPU present")
+    gates = [(2, [0], 0, None), (3, [1, 0], 0, None)]
+    with pytest.raises(K.KateError, match="no such CUDA device"):
+        K.mergeGate(gates, device=0)
+    c = K.Circuit(2, gates)
+    with pytest.raises(K.KateError, match="no such CUDA device"):
+        c.gateFusion(2, 1e-6, device=0)
+    assert c.num_gates() == 2

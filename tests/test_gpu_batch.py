@@ -176,3 +176,55 @@ def test_batch_state_readback_matches_complex128():
         s.close()
         assert 1.0 - abs(np.vdot(psi128, psi64)) ** 2 <= 1e-6
     b.close()
+
+
+def _block_options(nmin=13, blocks=1):
+    o = _lib.BatchOptions()
+    K._lib.lib().kate_batch_options_default(ctypes_ref(o))
+    for n in range(nmin, K._lib.KATE_BATCH_MAX_QUBITS + 1):
+        o.tune[n].blocks = blocks
+    return o
+
+
+def test_tensor_core_block_passes_match_oracle(oracle):
+    """Complex64 circuits kept in device memory with tensor-core block
+    passes (the batch kernel's block tasks: split-BF16 products, FP32
+    accumulation), mixed in one launch with register-staged and
+    shared-memory circuits: <Z> of every circuit against the oracle
+    (2e-5), and the block passes' states within 1e-6 infidelity of
+    complex128."""
+    specs = mixed(5) + [(15, circuits.brickwork_su4(15, 6, seed=9)), (13, [])]
+    circs = [K.Circuit(n, g) for n, g in specs]
+    b = K.Batch(circs, precision=K.C64, options=_block_options())
+    nres = sum(1 for n, g in specs if n >= 13 and len(g) > 0)
+    assert b.info()["block_programs"] >= nres  # every resident circuit with gates plans to block passes
+    b.run()
+    got = b.expect_z()
+    for (n, g), z in zip(specs, got):
+        assert np.abs(z - zexp(n, oracle.simulate(n, g))).max() <= 2e-5, (n, len(g))
+    b.run()  # a second run of the same graph gives the same outputs
+    for z1, z2 in zip(got, b.expect_z()):
+        assert np.abs(z1 - z2).max() <= 1e-12
+    _, res = b.circuit_info()
+    for i, (n, g) in enumerate(specs):
+        if res[i] >= 13 and len(g) > 0:
+            psi = b.state(i)
+            ref = oracle.simulate(n, g)
+            assert 1.0 - abs(np.vdot(ref, psi)) ** 2 / np.vdot(psi, psi).real <= 1e-6, n
+    b.close()
+
+
+def test_block_and_register_batches_agree():
+    """The same HEA circuits with and without tensor-core block passes: the
+    two complex64 forms agree on <Z> to 2e-5."""
+    rng = np.random.default_rng(11)
+    ns = [int(x) for x in rng.integers(13, 19, 24)]
+    circs = [K.Circuit(n, circuits.hea(n, 2 * n, seed=50 + i)) for i, n in enumerate(ns)]
+    a = K.Batch(circs, precision=K.C64, options=_block_options(blocks=0))
+    a.run()
+    b = K.Batch(circs, precision=K.C64, options=_block_options(blocks=1))
+    assert a.info()["block_programs"] == 0 and b.info()["block_programs"] == b.info()["programs"]
+    b.run()
+    assert np.abs(a.expect_z_flat() - b.expect_z_flat()).max() <= 2e-5
+    a.close()
+    b.close()
