@@ -90,6 +90,8 @@ def parse():
     ap.add_argument("--requests", type=int, default=1000, help="serve: requests per rate")
     ap.add_argument("--rates", default="1000,4000,16000", help="serve: arrival rates (requests/s)")
     ap.add_argument("--step-us", type=int, default=0, help="serve: step latency target in us (0: default)")
+    ap.add_argument("--tensor-blocks", type=int, default=0, choices=[0, 1],
+                    help="serve: 1 runs complex64 requests' passes as tensor-core blocks")
     ap.add_argument("--seed", type=int, default=1234)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true", help="layers: skip the reference's own GPU path")
@@ -1020,7 +1022,8 @@ def run_serve(args):
     cfg = {"workload": f"Poisson stream of {R} requests per rate, n truncated geometric (p=0.3) on 12..28, "
                        f"layered RX/RZ/CNOT-ladder circuit of depth n, complex64, 1024 samples + <Z_q> each, "
                        f"150 GB admission budget", "requests": R, "rates": rates, "seed": args.seed,
-           "mean_n": float(np.mean(ns)), "max_n": int(max(ns)), "parallelism": "replicas"}
+           "mean_n": float(np.mean(ns)), "max_n": int(max(ns)), "parallelism": "replicas",
+           "tensor_blocks": args.tensor_blocks}
     if args.impl == "reference":
         if _reference_unavailable():
             print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built"}))
@@ -1047,7 +1050,7 @@ def run_serve(args):
     torch.cuda.set_device(0)
     circs = [K.Circuit(n, C.layered(n, n, seed=i)) for i, n in enumerate(ns)]
     kw = {"step_latency_us": args.step_us} if args.step_us else {}
-    srv = K.Server(K.C64, 0, budget_bytes=150 * 10 ** 9, **kw)
+    srv = K.Server(K.C64, 0, budget_bytes=150 * 10 ** 9, tensor_blocks=args.tensor_blocks, **kw)
     # Warm-up: a few requests of every size class present.
     for n in sorted(set(ns))[:6]:
         srv.wait(srv.submit(K.Circuit(n, C.layered(n, n, seed=999)), 1024, 1), timeout=600)

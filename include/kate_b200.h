@@ -463,6 +463,8 @@ typedef struct {
     int fusion;                      /* gateFusion width for unfused circuits (1: none) */
     int max_gates;                   /* gates per pass program */
     int step_latency_us;             /* estimated critical path per step (default 1500; <0: no limit) */
+    int tensor_blocks;               /* 1: complex64 requests run their passes as 5-qubit tensor-core blocks
+                                        (as kate_batch_tuning.blocks; default 0: register-staged programs) */
 } kate_server_options;
 
 KATE_API kate_status kate_server_options_default(kate_server_options* opt);

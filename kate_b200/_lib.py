@@ -146,4 +146,5 @@ class ServerOptions(_c.Structure):
     """kate_server_options (include/kate_b200.h)."""
     _fields_ = [("budget_bytes", _c.c_ulonglong), ("aux_bytes", _c.c_ulonglong), ("step_tiles", _c.c_longlong),
                 ("chunk", _c.c_int), ("zchunks", _c.c_int), ("schunks", _c.c_int), ("planners", _c.c_int),
-                ("fusion", _c.c_int), ("max_gates", _c.c_int), ("step_latency_us", _c.c_int)]
+                ("fusion", _c.c_int), ("max_gates", _c.c_int), ("step_latency_us", _c.c_int),
+                ("tensor_blocks", _c.c_int)]

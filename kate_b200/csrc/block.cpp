@@ -8,6 +8,7 @@
 // padded with identities to exactly five tile bits, then written as the
 // real 64x64 operand in BF16 hi + lo parts (split-BF16 products: the kernel
 // sums A_hi B_hi + A_hi B_lo + A_lo B_hi in FP32).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -153,6 +154,126 @@ void choose_swizzle(const std::vector<std::vector<int>>& sets, uint16_t smask[4]
     }
 }
 
+// The FP64 product of a block's gates (at most five qubits) as a dense
+// gate on the sorted union of their qubits. U starts as the identity and
+// each gate multiplies it from the left, row group by row group, each step
+// vectorised over U's 32 columns (the column-by-column gate merger costs
+// several times more on the long blocks the light-cone selector forms).
+// Not bit-identical to merge_gates (the operation order differs); the
+// blocks are rounded to BF16 operands anyway.
+std::string merge_block(const std::vector<Gate>& gl, Gate* out) {
+    std::vector<int> cov;
+    for (const Gate& g : gl) cov.insert(cov.end(), g.qbits.begin(), g.qbits.end());
+    std::sort(cov.begin(), cov.end());
+    cov.erase(std::unique(cov.begin(), cov.end()), cov.end());
+    const int k = (int)cov.size();
+    if (k > 5) return "internal: block wider than five qubits";
+    const int dim = 1 << k;
+    // U in separate real and imaginary planes (row-major), so the row
+    // updates below vectorise.
+    double ure[32 * 32], uim[32 * 32];
+    for (int i = 0; i < dim * dim; i++) ure[i] = uim[i] = 0.0;
+    for (int r = 0; r < dim; r++) ure[r * dim + r] = 1.0;
+    Cx G[32 * 32];
+    double rre[32][32], rim[32][32];
+    for (const Gate& g : gl) {
+        const int nq = (int)g.qbits.size();
+        const int gd = 1 << nq;
+        int lb[5];
+        for (int i = 0; i < nq; i++) lb[i] = (int)(std::lower_bound(cov.begin(), cov.end(), g.qbits[i]) - cov.begin());
+        // The gate's own matrix, bit i of its index = qbits[i].
+        for (int i = 0; i < gd * gd; i++) G[i] = Cx(0, 0);
+        switch (g.id) {
+        case G_DENSE:
+            for (int i = 0; i < gd * gd; i++) G[i] = g.dense[i];
+            break;
+        case G_H: {
+            const double h = 0.7071067811865475;
+            G[0] = Cx(h, 0);
+            G[1] = Cx(h, 0);
+            G[2] = Cx(h, 0);
+            G[3] = Cx(-h, 0);
+            break;
+        }
+        case G_CNOT:  // qbits[0] flips when qbits[1] is 1
+            G[0 * 4 + 0] = G[1 * 4 + 1] = Cx(1, 0);
+            G[2 * 4 + 3] = G[3 * 4 + 2] = Cx(1, 0);
+            break;
+        case G_TOFFOLI:  // qbits[2] flips when qbits[0] and qbits[1] are 1
+            for (int i = 0; i < 8; i++) G[i * 8 + i] = Cx(1, 0);
+            G[3 * 8 + 3] = G[7 * 8 + 7] = Cx(0, 0);
+            G[3 * 8 + 7] = G[7 * 8 + 3] = Cx(1, 0);
+            break;
+        case G_CRK: {
+            const double t = ((double)2 * 3.1415926535897932384626433) / (double)(1ull << g.optarg);
+            for (int i = 0; i < 3; i++) G[i * 4 + i] = Cx(1, 0);
+            G[15] = Cx(std::cos(t), std::sin(t));
+            break;
+        }
+        default:  // RX / RZ identifiers: no arithmetic, as in the reference
+            for (int i = 0; i < gd; i++) G[i * gd + i] = Cx(1, 0);
+            break;
+        }
+        bool diag = true;
+        for (int r = 0; r < gd && diag; r++)
+            for (int c = 0; c < gd; c++)
+                if (r != c && (G[r * gd + c].re != 0.0 || G[r * gd + c].im != 0.0)) {
+                    diag = false;
+                    break;
+                }
+        uint32_t tm = 0;
+        for (int i = 0; i < nq; i++) tm |= 1u << lb[i];
+        for (int base = 0; base < dim; base++) {
+            if ((uint32_t)base & tm) continue;
+            int idx[32];
+            for (int s2 = 0; s2 < gd; s2++) {
+                int x = base;
+                for (int i = 0; i < nq; i++) x |= ((s2 >> i) & 1) << lb[i];
+                idx[s2] = x;
+            }
+            if (diag) {  // scale each row
+                for (int r = 0; r < gd; r++) {
+                    const double ar = G[r * gd + r].re, ai = G[r * gd + r].im;
+                    double* xr = ure + idx[r] * dim;
+                    double* xi = uim + idx[r] * dim;
+                    for (int c = 0; c < dim; c++) {
+                        const double a = xr[c], b = xi[c];
+                        xr[c] = ar * a - ai * b;
+                        xi[c] = ar * b + ai * a;
+                    }
+                }
+                continue;
+            }
+            for (int s2 = 0; s2 < gd; s2++)
+                for (int c = 0; c < dim; c++) {
+                    rre[s2][c] = ure[idx[s2] * dim + c];
+                    rim[s2][c] = uim[idx[s2] * dim + c];
+                }
+            for (int r = 0; r < gd; r++) {
+                double* xr = ure + idx[r] * dim;
+                double* xi = uim + idx[r] * dim;
+                for (int c = 0; c < dim; c++) xr[c] = xi[c] = 0.0;
+                for (int s2 = 0; s2 < gd; s2++) {
+                    const double ar = G[r * gd + s2].re, ai = G[r * gd + s2].im;
+                    if (ar == 0.0 && ai == 0.0) continue;
+                    const double* yr = rre[s2];
+                    const double* yi = rim[s2];
+                    for (int c = 0; c < dim; c++) {
+                        xr[c] += ar * yr[c] - ai * yi[c];
+                        xi[c] += ar * yi[c] + ai * yr[c];
+                    }
+                }
+            }
+        }
+    }
+    out->id = G_DENSE;
+    out->qbits = cov;
+    out->optarg = 0;
+    out->dense.resize((size_t)dim * dim);
+    for (int i = 0; i < dim * dim; i++) out->dense[i] = Cx(ure[i], uim[i]);
+    return "";
+}
+
 }  // namespace
 
 // Greedy block partition of `gates` (qubit sets): returns, for each gate,
@@ -216,7 +337,7 @@ std::string build_block_program(const Plan& plan, const PlannedPass& pass, int n
                 used |= 1u << t;
             }
         Gate U;
-        std::string e = merge_gates(gl, &U);
+        std::string e = merge_block(gl, &U);
         if (!e.empty()) return e;
         if (U.qbits.size() != 5) return "internal: block is not five qubits";
         for (int i = 0; i < 5; i++) out->btb[b][i] = (uint8_t)U.qbits[i];

@@ -955,6 +955,7 @@ kate_status kate_server_options_default(kate_server_options* opt) {
     opt->fusion = d.tune.fusion;
     opt->max_gates = d.tune.max_gates;
     opt->step_latency_us = d.step_latency_us;
+    opt->tensor_blocks = d.tune.blocks;
     return KATE_OK;
 }
 
@@ -975,6 +976,7 @@ kate_status kate_server_create(int precision, int device, const kate_server_opti
             if (opt->max_gates > 0) o.tune.max_gates = opt->max_gates;
             if (opt->step_latency_us > 0) o.step_latency_us = opt->step_latency_us;
             if (opt->step_latency_us < 0) o.step_latency_us = 0;
+            o.tune.blocks = opt->tensor_blocks ? 1 : 0;
         }
         kate::Server* s = nullptr;
         std::string e = kate::Server::create(precision, device, o, &s);

@@ -107,8 +107,9 @@ std::string validate_gate(const Program& p, const Gate& g) {
 // g.qbits[i].
 void apply_gate_local(const Gate& g, const int* lb, int k, Cx* st) {
     const int nq = (int)g.qbits.size();
-    std::vector<int> sorted(lb, lb + nq);
-    std::sort(sorted.begin(), sorted.end());
+    int sorted[16];
+    std::copy(lb, lb + nq, sorted);
+    std::sort(sorted, sorted + nq);
     auto ins = [&](uint64_t line, int cnt) {
         uint64_t v = line;
         for (int i = 0; i < cnt; i++) {
@@ -153,7 +154,9 @@ void apply_gate_local(const Gate& g, const int* lb, int k, Cx* st) {
         break;
     case G_DENSE: {
         const int dim = 1 << nq;
-        std::vector<Cx> cache(dim);
+        Cx cache_small[32];
+        std::vector<Cx> cache_big(dim > 32 ? dim : 0);
+        Cx* cache = dim > 32 ? cache_big.data() : cache_small;
         for (uint64_t line = 0; line < (1ull << (k - nq)); line++) {
             uint64_t base = ins(line, nq);
             for (int s = 0; s < dim; s++) {
@@ -186,14 +189,16 @@ std::string merge_gates(const std::vector<Gate>& gates, Gate* out) {
     std::vector<Cx> m((size_t)dim * dim);
     for (int r = 0; r < dim; r++)
         for (int c = 0; c < dim; c++) m[(size_t)r * dim + c] = Cx((double)(int)(r == c), 0.0);
-    std::vector<int> lb;
-    for (int col = 0; col < dim; col++) {
-        for (auto& g : gates) {
-            lb.clear();
-            for (int q : g.qbits) lb.push_back((int)(std::lower_bound(cov.begin(), cov.end(), q) - cov.begin()));
-            apply_gate_local(g, lb.data(), k, m.data() + (size_t)col * dim);
-        }
+    // Local bits of every gate, once (the columns are simulated one by one).
+    std::vector<int> lbs;
+    std::vector<size_t> lb0;
+    for (auto& g : gates) {
+        lb0.push_back(lbs.size());
+        for (int q : g.qbits) lbs.push_back((int)(std::lower_bound(cov.begin(), cov.end(), q) - cov.begin()));
     }
+    for (int col = 0; col < dim; col++)
+        for (size_t i = 0; i < gates.size(); i++)
+            apply_gate_local(gates[i], lbs.data() + lb0[i], k, m.data() + (size_t)col * dim);
     for (int r = 0; r < dim; r++)
         for (int c = r + 1; c < dim; c++) std::swap(m[(size_t)r * dim + c], m[(size_t)c * dim + r]);
     out->id = G_DENSE;

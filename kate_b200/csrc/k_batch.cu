@@ -144,7 +144,8 @@ __device__ __noinline__ bool block_task(float2* st, const BatchProg& BP, const u
             const uint64_t cb = blk::coset_base(P, c);
             blk::zero_tile(S0, cb == 0);
             __syncthreads();
-            ok = blk::apply_blocks(P, X, tab, S0, bbase, tmem, mbar, phase, abort_flag);
+            float2* const SS[1] = {S0};
+            ok = blk::apply_blocks<1>(P, X, tab, SS, bbase, tmem, mbar, phase, abort_flag);
             if (ok) blk::store_tile<true>(P, X, iot, st, cb, S0);
             __syncthreads();
         }
@@ -163,7 +164,8 @@ __device__ __noinline__ bool block_task(float2* st, const BatchProg& BP, const u
         asm volatile("cp.async.commit_group;\n" ::: "memory");
         asm volatile("cp.async.wait_group 1;\n" ::: "memory");
         __syncthreads();
-        if (!blk::apply_blocks(P, X, tab, S, bbase, tmem, mbar, phase, abort_flag)) {
+        float2* const SS[1] = {S};
+        if (!blk::apply_blocks<1>(P, X, tab, SS, bbase, tmem, mbar, phase, abort_flag)) {
             ok = false;
             break;
         }
@@ -425,7 +427,7 @@ __global__ void __launch_bounds__(NT, sizeof(C2) == 8 ? 2 : 1)
                 blk_abort = 0;
                 blk_phase = 0;
             }
-            blk::tmem_alloc(&blk_tmem);
+            blk::tmem_alloc(&blk_tmem, blk::TMEM_COLS);
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncthreads();
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -535,7 +537,7 @@ __global__ void __launch_bounds__(NT, sizeof(C2) == 8 ? 2 : 1)
         }
     }
     if constexpr (sizeof(C2) == 8) {
-        if (tensor_blocks) blk::tmem_free(blk_tmem);
+        if (tensor_blocks) blk::tmem_free(blk_tmem, blk::TMEM_COLS);
     }
 }
 
@@ -555,12 +557,29 @@ int batch_grid(int device, int prec) {
     if (!cached[device][pi]) {
         int sms = 148, occ = 1;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        // Two CTAs per SM need most of the SM's shared memory (about 100 KiB
+        // each for complex64): ask for the largest carveout.
         if (pi == 1) {
             cudaFuncSetAttribute(k_batch<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)batch_smem<float2>());
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<float2>, NT, batch_smem<float2>());
+            cudaFuncSetAttribute(k_batch<float2>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared);
+            // The occupancy calculator reports one CTA per SM for this kernel
+            // (it holds tcgen05 code), although two fit and run together
+            // (measured: 570 against 932 ms per launch of the batching
+            // workload with tensor-core block tasks). __launch_bounds__
+            // gives the registers for two; shared memory decides.
+            cudaFuncAttributes fa{};
+            cudaFuncGetAttributes(&fa, k_batch<float2>);
+            int smem_sm = 0, reserved = 0;
+            cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device);
+            cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, device);
+            occ = smem_sm / (int)(batch_smem<float2>() + fa.sharedSizeBytes + reserved);
+            if (occ > 2) occ = 2;
         } else {
             cudaFuncSetAttribute(k_batch<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)batch_smem<double2>());
+            cudaFuncSetAttribute(k_batch<double2>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared);
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<double2>, NT, batch_smem<double2>());
         }
         if (occ < 1) occ = 1;

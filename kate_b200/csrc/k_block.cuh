@@ -34,8 +34,8 @@ constexpr int NT = 256;
 constexpr int TB = KATE_TILE_BITS;  // 12 tile bits
 constexpr int TS = 1 << TB;
 constexpr uint32_t S_BYTES = TS * 8;  // one staging tile (float2)
-// TMEM columns: the FP32 accumulator (N = 64), then the A operand's hi and
-// lo parts (128 lanes x 64 BF16 = 32 columns each).
+// TMEM columns per tile: the FP32 accumulator (N = 64), then the A
+// operand's hi and lo parts (128 lanes x 64 BF16 = 32 columns each).
 constexpr uint32_t TMEM_COLS = 128;
 constexpr uint32_t TM_AHI = 64, TM_ALO = 96;
 constexpr long WAIT_LIMIT = 1L << 24;
@@ -115,24 +115,25 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
     return false;
 }
 
-// TMEM allocation of one CTA (warp 0 allocates; every thread reads the base
-// after the barrier the caller places). `slot` is a shared-memory word.
-__device__ __forceinline__ void tmem_alloc(uint32_t* slot) {
+// TMEM allocation of one CTA, `cols` columns (a power of two, 32..512;
+// warp 0 allocates; every thread reads the base after the barrier the
+// caller places). `slot` is a shared-memory word.
+__device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t cols) {
     if ((threadIdx.x >> 5) == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)),
-                     "r"(TMEM_COLS)
+                     "r"(cols)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
 }
 
 // Frees the CTA's TMEM; every thread calls it (it synchronises the CTA).
-__device__ __forceinline__ void tmem_free(uint32_t tmem) {
+__device__ __forceinline__ void tmem_free(uint32_t tmem, uint32_t cols) {
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if ((threadIdx.x >> 5) == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(cols) : "memory");
     }
 }
 
@@ -261,24 +262,32 @@ __device__ __forceinline__ void zero_tile(float2* S, bool one) {
     if (one && threadIdx.x == 0) S[0] = make_float2(1.f, 0.f);
 }
 
-// Applies the pass's blocks to the staging tile S (its copy complete and
-// visible to every thread). B images at shared address bimg (block b at
-// bimg + b * KATE_BLOCK_IMG_BYTES, 1024-byte aligned). Returns false when a
-// product wait gave up (after every thread has left the block loop).
-__device__ __forceinline__ bool apply_blocks(const BlockProg& P, const Pass& X, const uint16_t* tab, float2* S,
-                                             uint32_t bimg, uint32_t tmem, uint32_t mbar, uint32_t& phase,
-                                             int* abort_flag) {
+// Applies the pass's blocks to NTL staging tiles S[0..NTL) in lock-step
+// (each copy complete and visible to every thread). Tile i uses the 128 TMEM
+// columns from tmem + 128 i (accumulator, then the A parts). Per block: the
+// A operands of every tile, one barrier, one batch of products for all
+// tiles behind one mbarrier, the read-backs, one barrier; two tiles halve the
+// barriers and product round trips per tile. B images at shared address
+// bimg (block b at bimg + b * KATE_BLOCK_IMG_BYTES, 1024-byte aligned).
+// Returns false when a product wait gave up (after every thread has left
+// the block loop).
+template <int NTL>
+__device__ __forceinline__ bool apply_blocks(const BlockProg& P, const Pass& X, const uint16_t* tab,
+                                             float2* const (&S)[NTL], uint32_t bimg, uint32_t tmem, uint32_t mbar,
+                                             uint32_t& phase, int* abort_flag) {
     const uint32_t t = threadIdx.x, warp = t >> 5;
     for (int blk = 0; blk < P.nblocks; blk++) {
         const uint16_t* tb = tab + blk * 32;
         const uint32_t ra_sw = blk == 0 ? X.rsa[0] : X.rsa[KATE_C64_MAX_BLOCKS - 1];
         const uint32_t rr_sw = blk == 0 ? X.rsr[0] : X.rsr[KATE_C64_MAX_BLOCKS - 1];
         const bool wide = P.btb[blk][0] == 0 && X.pairs;  // block index bits 0 = tile bit 0: 16-byte pairs
-        // 1. A operand (hi, lo) from the staging tile into TMEM. Thread t:
+        // 1. A operands (hi, lo) from the staging tiles into TMEM. Thread t:
         //    row r = t & 127 (TMEM lane 32 (warp & 3) + lane), K half
         //    h = t >> 7 (block indices 16h..16h+15: TMEM columns 16h..16h+15
         //    of the A parts, one re/im pair per column).
-        {
+#pragma unroll
+        for (int ti = 0; ti < NTL; ti++) {
+            const float2* St = S[ti];
             const uint32_t h = t >> 7;
             uint32_t hw[16], lw[16];
             auto split = [&](int e, float2 a) {
@@ -290,50 +299,57 @@ __device__ __forceinline__ bool apply_blocks(const BlockProg& P, const Pass& X, 
             if (wide) {
 #pragma unroll
                 for (int e = 0; e < 16; e += 2) {
-                    const float4 v = *reinterpret_cast<const float4*>(&S[ra_sw ^ tb[h * 16u + (uint32_t)e]]);
+                    const float4 v = *reinterpret_cast<const float4*>(&St[ra_sw ^ tb[h * 16u + (uint32_t)e]]);
                     split(e, make_float2(v.x, v.y));
                     split(e + 1, make_float2(v.z, v.w));
                 }
             } else {
 #pragma unroll
-                for (int e = 0; e < 16; e++) split(e, S[ra_sw ^ tb[h * 16u + (uint32_t)e]]);
+                for (int e = 0; e < 16; e++) split(e, St[ra_sw ^ tb[h * 16u + (uint32_t)e]]);
             }
-            const uint32_t lane_base = tmem + (((warp & 3u) * 32u) << 16) + h * 16u;
+            const uint32_t lane_base = tmem + (uint32_t)ti * 128u + (((warp & 3u) * 32u) << 16) + h * 16u;
             tmem_st16(lane_base + TM_AHI, hw);
             tmem_st16(lane_base + TM_ALO, lw);
-            asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
         }
+        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads();
-        // 2. Tensor-core products into TMEM.
+        // 2. Tensor-core products into TMEM, every tile behind one commit.
         if (t == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const uint32_t bb = bimg + (uint32_t)blk * KATE_BLOCK_IMG_BYTES;
+#pragma unroll
+            for (int ti = 0; ti < NTL; ti++) {
+                const uint32_t tm = tmem + (uint32_t)ti * 128u;
 #pragma unroll 1
-            for (int s = 0; s < 4; s++) {
-                const uint32_t k = (uint32_t)s * 32u;  // K = 16 BF16 = 32 bytes per step (B)
-                const uint32_t kc = (uint32_t)s * 8u;  // K = 16 BF16 = 8 TMEM columns per step (A)
-                const uint64_t b_hi = sw128_desc(bb + k), b_lo = sw128_desc(bb + KATE_BLOCK_IMG_BYTES / 2 + k);
-                mma_bf16_ts(tmem, tmem + TM_AHI + kc, b_hi, s > 0 ? 1u : 0u);
-                mma_bf16_ts(tmem, tmem + TM_AHI + kc, b_lo, 1u);
-                mma_bf16_ts(tmem, tmem + TM_ALO + kc, b_hi, 1u);
+                for (int s = 0; s < 4; s++) {
+                    const uint32_t k = (uint32_t)s * 32u;  // K = 16 BF16 = 32 bytes per step (B)
+                    const uint32_t kc = (uint32_t)s * 8u;  // K = 16 BF16 = 8 TMEM columns per step (A)
+                    const uint64_t b_hi = sw128_desc(bb + k), b_lo = sw128_desc(bb + KATE_BLOCK_IMG_BYTES / 2 + k);
+                    mma_bf16_ts(tm, tm + TM_AHI + kc, b_hi, s > 0 ? 1u : 0u);
+                    mma_bf16_ts(tm, tm + TM_AHI + kc, b_lo, 1u);
+                    mma_bf16_ts(tm, tm + TM_ALO + kc, b_hi, 1u);
+                }
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
                          : "memory");
         }
-        // One thread waits for the products (the others would only take
-        // issue slots from the SM's other CTA); the barrier releases them.
-        if (t == 0 && !mbar_wait(mbar, phase)) *abort_flag = 1;
+        // Every thread waits for the products itself (try_wait suspends the
+        // waiting thread), so no CTA barrier sits between the products and
+        // the read-back. A wait that gives up raises the flag; the read-back
+        // still runs (its values are then unused) so that every thread
+        // reaches the barrier below, after which all see the flag.
+        if (!mbar_wait(mbar, phase)) *abort_flag = 1;
         phase ^= 1u;
-        __syncthreads();
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        if (*abort_flag) return false;
         // 3. Results: warp w reads TMEM lanes 32(w&3)..+31 (rows) and columns
-        //    32(w>>2)..+31 (block indices 16(w>>2)..+15).
-        {
+        //    32(w>>2)..+31 (block indices 16(w>>2)..+15) of each tile.
+#pragma unroll
+        for (int ti = 0; ti < NTL; ti++) {
+            float2* St = S[ti];
             const uint32_t sub = warp & 3u, ch = warp >> 2;
             uint32_t d[32];
-            const uint32_t taddr = tmem + ((sub * 32u) << 16) + ch * 32u;
+            const uint32_t taddr = tmem + (uint32_t)ti * 128u + ((sub * 32u) << 16) + ch * 32u;
             asm volatile(
                 "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
                 "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
@@ -348,18 +364,19 @@ __device__ __forceinline__ bool apply_blocks(const BlockProg& P, const Pass& X, 
             if (wide) {
 #pragma unroll
                 for (int e = 0; e < 16; e += 2)
-                    *reinterpret_cast<float4*>(&S[rr_sw ^ tb[ch * 16u + (uint32_t)e]]) =
+                    *reinterpret_cast<float4*>(&St[rr_sw ^ tb[ch * 16u + (uint32_t)e]]) =
                         make_float4(__uint_as_float(d[2 * e]), __uint_as_float(d[2 * e + 1]),
                                     __uint_as_float(d[2 * e + 2]), __uint_as_float(d[2 * e + 3]));
             } else {
 #pragma unroll
                 for (int e = 0; e < 16; e++)
-                    S[rr_sw ^ tb[ch * 16u + (uint32_t)e]] =
+                    St[rr_sw ^ tb[ch * 16u + (uint32_t)e]] =
                         make_float2(__uint_as_float(d[2 * e]), __uint_as_float(d[2 * e + 1]));
             }
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads();
+        if (*abort_flag) return false;
     }
     return true;
 }

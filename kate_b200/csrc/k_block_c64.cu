@@ -47,7 +47,7 @@ __global__ void __launch_bounds__(NT, 2)
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
         *abort_flag = 0;
     }
-    tmem_alloc(tmem_slot);
+    tmem_alloc(tmem_slot, TMEM_COLS);
     // Block matrices: B images into shared memory once.
     for (int b = 0; b < P.nblocks; b++) {
         const uint8_t* src = bimg + P.bimg[b];
@@ -82,13 +82,14 @@ __global__ void __launch_bounds__(NT, 2)
         load(c + gridDim.x, cur ^ 1);
         asm volatile("cp.async.wait_group 1;\n" ::: "memory");
         __syncthreads();
-        if (!apply_blocks(P, X, tab, S, base + OFF_B, tmem, mbar, phase, abort_flag)) break;
+        float2* const SS[1] = {S};
+        if (!apply_blocks<1>(P, X, tab, SS, base + OFF_B, tmem, mbar, phase, abort_flag)) break;
         store_tile<false>(P, X, iot, st, coset_base(P, c), S);
         __syncthreads();
     }
     if (*abort_flag && t == 0) atomicExch(err, 1);
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-    tmem_free(tmem);
+    tmem_free(tmem, TMEM_COLS);
 }
 
 }  // namespace

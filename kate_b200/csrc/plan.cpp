@@ -5,6 +5,7 @@
 #include <cmath>
 #include <numeric>
 #include <set>
+#include <unordered_map>
 
 namespace kate {
 
@@ -284,8 +285,19 @@ std::vector<int> c64_pass(const std::vector<PGate>& pg, const std::vector<int>& 
         if (inT[q]) T |= 1ull << q;
     std::vector<int> live(rem), exec, ready, seeds, tmp;
     std::vector<char> mark(pg.size(), 0);
+    // Absorbed-gate counts by qubit set, for the current `live` (many seeds
+    // and growth steps reach the same sets).
+    std::unordered_map<uint64_t, int> memo;
+    auto count = [&](uint64_t Q) {
+        auto it = memo.find(Q);
+        if (it != memo.end()) return it->second;
+        const int c = absorb_set(gm, live, Q, nullptr, scan_limit);
+        memo.emplace(Q, c);
+        return c;
+    };
     for (int b = 0; b < maxb && !live.empty(); b++) {
         std::fill(mark.begin(), mark.end(), 0);
+        memo.clear();
         ready_gates(gm, live, mark, all, scan_limit, seeds);
         int best_cnt = 0, best_tile = 0;
         uint64_t best_Q = 0;
@@ -304,7 +316,7 @@ std::vector<int> c64_pass(const std::vector<PGate>& pg, const std::vector<int>& 
                     const uint64_t nQ = Q | gm[gi];
                     const int sz = __builtin_popcountll(nQ);
                     if (nQ == Q || sz > 5 || __builtin_popcountll(T | nQ) > m) continue;
-                    const int c2 = absorb_set(gm, live, nQ, nullptr, scan_limit);
+                    const int c2 = count(nQ);
                     if (c2 > gc || (c2 == gc && gQ && sz < gsize)) {
                         gc = c2;
                         gQ = nQ;
@@ -588,10 +600,7 @@ std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out) {
             std::vector<char> inT2(n, 0);
             int ts2 = 0;
             std::vector<int> order;
-            if (blocks)
-                c64_pass(plan.pgates, rem, n, mg, KATE_C64_MAX_BLOCKS, inT2, ts2, &order, c64_scan_limit);
-            else
-                greedy_pass(plan.pgates, rem, n, mg, inT2, ts2, &order, scan_limit, opt.c64);
+            greedy_pass(plan.pgates, rem, n, mg, inT2, ts2, &order, scan_limit, opt.c64);
             for (int q : order)
                 if (inT[q] && (int)newlow.size() < c) newlow.push_back(q);
         }

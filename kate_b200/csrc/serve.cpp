@@ -218,7 +218,7 @@ struct ServerImpl {
             }
             std::string e;
             try {
-                e = pack_circuit(r->prog, opt.tune, true, r->pack);
+                e = pack_circuit(r->prog, opt.tune, true, r->pack, precision == 1);
             } catch (const std::exception& ex) {
                 e = ex.what();
             }
@@ -504,7 +504,8 @@ struct ServerImpl {
                                       reinterpret_cast<const DevOp*>(d_aux), d_aux, S.d_ctr, S.d_ctr + 2,
                                       reinterpret_cast<double*>(d_aux), S.d_ctr + 1, g, stream,
                                       reinterpret_cast<double*>(d_aux), reinterpret_cast<const double*>(d_aux),
-                                      reinterpret_cast<uint64_t*>(d_aux));
+                                      reinterpret_cast<uint64_t*>(d_aux), 5000000000ull,
+                                      precision == 1 && opt.tune.blocks ? 1 : 0);
         if (le != cudaSuccess) return cuda_err("launch_batch", le);
         cudaEventRecord(S.ev, stream);
         S.t_launch = tb;

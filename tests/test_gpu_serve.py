@@ -19,9 +19,10 @@ def layered(n, seed):
     return circuits.layered(n, n, seed=seed)
 
 
-@pytest.mark.parametrize("prec,tol", [(K.C128, 1e-12), (K.C64, 2e-5)])
-def test_requests_match_oracle(oracle, prec, tol):
-    srv = K.Server(prec, budget_bytes=1 << 30, aux_bytes=256 << 20)
+@pytest.mark.parametrize("prec,tol,blocks", [(K.C128, 1e-12, 0), (K.C64, 2e-5, 0), (K.C64, 2e-5, 1)])
+def test_requests_match_oracle(oracle, prec, tol, blocks):
+    # blocks=1: complex64 requests run their passes as tensor-core blocks.
+    srv = K.Server(prec, budget_bytes=1 << 30, aux_bytes=256 << 20, tensor_blocks=blocks)
     specs = [(n, layered(n, 10 + n)) for n in (12, 13, 14, 16, 17)]
     ids = [srv.submit(K.Circuit(n, g), shots=4096, seed=7 + n) for n, g in specs]
     for (n, g), rid in zip(specs, ids):
