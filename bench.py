@@ -91,7 +91,8 @@ def parse():
     ap.add_argument("--rates", default="1000,4000,16000", help="serve: arrival rates (requests/s)")
     ap.add_argument("--step-us", type=int, default=0, help="serve: step latency target in us (0: default)")
     ap.add_argument("--tensor-blocks", type=int, default=0, choices=[0, 1],
-                    help="serve: 1 runs complex64 requests' passes as tensor-core blocks")
+                    help="serve, and batch with --no-autotune: 1 runs complex64 passes of states kept in "
+                         "device memory as tensor-core blocks")
     ap.add_argument("--seed", type=int, default=1234)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true", help="layers: skip the reference's own GPU path")
@@ -883,7 +884,14 @@ def run_batch(args):
     torch.cuda.set_device(0)
     ns, circs = _hea_batch(K, C, N)
     t0 = time.perf_counter()
-    b = K.Batch(circs, precision=K.C64, autotune=not args.no_autotune)
+    opts = None
+    if args.no_autotune and args.tensor_blocks:
+        import ctypes
+        opts = K._lib.BatchOptions()
+        K._lib.lib().kate_batch_options_default(ctypes.byref(opts))
+        for n in range(13, K._lib.KATE_BATCH_MAX_QUBITS + 1):
+            opts.tune[n].blocks = 1
+    b = K.Batch(circs, precision=K.C64, options=opts, autotune=not args.no_autotune)
     create_s = time.perf_counter() - t0
     tune = {n: {"fusion_k": b.options.tune[n].fusion, "max_gates": b.options.tune[n].max_gates,
                 "group_m": b.options.tune[n].group_qubits, "coalesce_c": b.options.tune[n].coalesce,

@@ -624,6 +624,47 @@ std::string jit_compile(int device, const std::vector<std::string>& srcs, std::v
     return "";
 }
 
+std::string jit_pass_key(const PassProg& P, bool from_zero, int occ) {
+    std::string k;
+    auto put = [&](const void* p, size_t n) { k.append(static_cast<const char*>(p), n); };
+    const int32_t head[7] = {P.m, P.ncb, P.nops, P.nmats, P.nstages, from_zero ? 1 : 0, occ};
+    put(head, sizeof head);
+    put(P.tphys, sizeof P.tphys);
+    put(P.outsrc, sizeof P.outsrc);
+    put(P.cphys, sizeof P.cphys);
+    const int nops = std::max(0, std::min((int)P.nops, KATE_MAX_SOPS));
+    const int nst = std::max(0, std::min((int)P.nstages, KATE_MAX_STAGES));
+    put(P.ops, sizeof(SOp) * (size_t)nops);
+    put(P.stab, sizeof(P.stab[0]) * (size_t)nst);
+    put(P.srb, sizeof(P.srb[0]) * (size_t)nst);
+    put(P.stb, sizeof(P.stb[0]) * (size_t)nst);
+    return k;
+}
+
+namespace {
+struct KeyCache {
+    std::mutex mu;
+    std::map<std::pair<int, std::string>, void*> fns;
+};
+KeyCache& key_cache() {
+    static KeyCache c;
+    return c;
+}
+}  // namespace
+
+void* jit_find(int device, const std::string& key) {
+    KeyCache& C = key_cache();
+    std::lock_guard<std::mutex> lk(C.mu);
+    auto it = C.fns.find(std::make_pair(device, key));
+    return it == C.fns.end() ? nullptr : it->second;
+}
+
+void jit_remember(int device, const std::string& key, void* fn) {
+    KeyCache& C = key_cache();
+    std::lock_guard<std::mutex> lk(C.mu);
+    C.fns[std::make_pair(device, key)] = fn;
+}
+
 int jit_local_bytes(void* fn) {
     int v = 0;
     if (!api().drv_ok || api().get_attr(&v, CU_FUNC_ATTRIBUTE_LOCAL_SIZE_BYTES, (CUfunction)fn) != CUDA_SUCCESS) return -1;

@@ -37,6 +37,16 @@ std::string jit_pass_source(const PassProg& prog, std::string* why, bool from_ze
 // a kernel handle per source. Returns "" on success.
 std::string jit_compile(int device, const std::vector<std::string>& srcs, std::vector<void*>* fns);
 
+// The fields of `prog` that its generated source depends on (everything but
+// the matrix values), with from_zero and occ: a key a few KB long, so a
+// simulator whose passes were compiled before finds their kernels without
+// generating their sources (about 0.2 ms per pass).
+std::string jit_pass_key(const PassProg& prog, bool from_zero, int occ);
+// The kernel compiled on `device` for a pass key, or null.
+void* jit_find(int device, const std::string& key);
+// Records the kernel of a pass key (from jit_compile).
+void jit_remember(int device, const std::string& key, void* fn);
+
 // Local memory (register spill) bytes per thread of a compiled kernel; -1
 // when unknown.
 int jit_local_bytes(void* fn);

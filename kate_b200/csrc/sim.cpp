@@ -233,25 +233,65 @@ std::string Simulator::create(const Program& prog_in, int precision, int device,
             std::vector<size_t> idx;
             std::vector<std::string> todo;
             std::vector<char> zero_form;
+            // Kernels compiled before for the same pass shape are found by
+            // key; only the others get their source generated (a pass the
+            // generator does not take is remembered as such, by a null).
+            std::vector<void*> fns;
+            std::vector<std::string> keys;
+            std::vector<size_t> miss;
+            auto want = [&](size_t i, bool zf) {
+                std::string key = jit_pass_key(*impl->plan.passes[i].prog, zf, occ_first);
+                void* f = jit_find(device, key);
+                idx.push_back(i);
+                zero_form.push_back(zf ? 1 : 0);
+                if (!f) {
+                    miss.push_back(fns.size());
+                    todo.push_back(jit_pass_source(*impl->plan.passes[i].prog, nullptr, zf, occ_first));
+                }
+                fns.push_back(f);
+                keys.push_back(std::move(key));
+            };
             for (size_t i = 0; i < impl->plan.passes.size(); i++) {
                 const PlannedPass& p = impl->plan.passes[i];
                 if (!p.prog || p.bprog) continue;
-                std::string src = jit_pass_source(*p.prog, nullptr, false, occ_first);
-                if (src.empty()) continue;
-                idx.push_back(i);
-                todo.push_back(std::move(src));
-                zero_form.push_back(0);
+                want(i, false);
             }
             // Pass 0 also in the form that generates |0...0> itself.
-            const bool zero0 = !idx.empty() && idx[0] == 0;
-            if (zero0) {
-                idx.push_back(0);
-                todo.push_back(jit_pass_source(*impl->plan.passes[0].prog, nullptr, true, occ_first));
-                zero_form.push_back(1);
+            bool zero0 = !idx.empty() && idx[0] == 0;
+            if (zero0) want(0, true);
+            {
+                // Sources the generator declined: those passes keep the interpreter.
+                std::vector<std::string> srcs;
+                std::vector<size_t> at;
+                for (size_t m = 0; m < miss.size(); m++)
+                    if (!todo[m].empty()) {
+                        srcs.push_back(std::move(todo[m]));
+                        at.push_back(miss[m]);
+                    }
+                std::vector<void*> got;
+                std::string je = jit_compile(device, srcs, &got);
+                if (!je.empty()) return fail("pass kernel compilation: " + je);
+                for (size_t m = 0; m < at.size(); m++) {
+                    fns[at[m]] = got[m];
+                    jit_remember(device, keys[at[m]], got[m]);
+                }
             }
-            std::vector<void*> fns;
-            std::string je = jit_compile(device, todo, &fns);
-            if (!je.empty()) return fail("pass kernel compilation: " + je);
+            // Drop the passes without a kernel (the generator declined them).
+            {
+                std::vector<size_t> i2;
+                std::vector<char> z2;
+                std::vector<void*> f2;
+                for (size_t k = 0; k < fns.size(); k++) {
+                    if (!fns[k]) continue;
+                    i2.push_back(idx[k]);
+                    z2.push_back(zero_form[k]);
+                    f2.push_back(fns[k]);
+                }
+                zero0 = zero0 && !z2.empty() && z2.back() == 1;
+                idx.swap(i2);
+                zero_form.swap(z2);
+                fns.swap(f2);
+            }
             if (occ_first == 3) {
                 std::vector<size_t> redo;
                 std::vector<std::string> src2;
@@ -262,7 +302,7 @@ std::string Simulator::create(const Program& prog_in, int precision, int device,
                     }
                 if (!redo.empty()) {
                     std::vector<void*> f2;
-                    je = jit_compile(device, src2, &f2);
+                    const std::string je = jit_compile(device, src2, &f2);
                     if (!je.empty()) return fail("pass kernel compilation: " + je);
                     for (size_t r = 0; r < redo.size(); r++) fns[redo[r]] = f2[r];
                 }
