@@ -974,9 +974,11 @@ def run_batch(args):
         "circuits/s", "circuits/s", value, args, ms, "c64 (f32)", cfg,
         e2e={"value": N / e2e_s, "unit": "circuits/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 8 * len(z),
              "ms_per_step": e2e_s * 1000, "note": "plan + upload + run + <Z> readback per step"},
-        roofline={"bound": "fp32 issue (hbm shown)", "achieved": alg / (ms / 1000) / 1e9, "peak": peak, "unit": "GB/s",
+        roofline={"bound": "hbm (latency-bound task queue: tensor-core block tasks and FP32 register tasks)",
+                  "achieved": alg / (ms / 1000) / 1e9, "peak": peak, "unit": "GB/s",
                   "frac": alg / (ms / 1000) / 1e9 / peak, "traffic": None, "peak_source": peak_kind,
-                  "kernel": "k_batch<float2> (persistent task queue)", "alg_bytes_per_launch": alg,
+                  "kernel": "k_batch<float2> (persistent task queue; tcgen05 block tasks where autotuned)",
+                  "alg_bytes_per_launch": alg,
                   "avg_launch_ms": ms},
         gpu_launches=args.steps, clocks=clk.summary(), cpu_baseline=cpu)))
 

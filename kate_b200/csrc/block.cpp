@@ -169,19 +169,36 @@ std::string merge_block(const std::vector<Gate>& gl, Gate* out) {
     const int k = (int)cov.size();
     if (k > 5) return "internal: block wider than five qubits";
     const int dim = 1 << k;
-    // U in separate real and imaginary planes (row-major), so the row
-    // updates below vectorise.
-    double ure[32 * 32], uim[32 * 32];
-    for (int i = 0; i < dim * dim; i++) ure[i] = uim[i] = 0.0;
-    for (int r = 0; r < dim; r++) ure[r * dim + r] = 1.0;
-    Cx G[32 * 32];
-    double rre[32][32], rim[32][32];
-    for (const Gate& g : gl) {
-        const int nq = (int)g.qbits.size();
-        const int gd = 1 << nq;
+    // Each gate as a local matrix; single-qubit gates are first multiplied
+    // into a pending 2x2 per qubit, which the next wider gate on that qubit
+    // absorbs (G' = G (x) pending, on G's column bit) or which is applied
+    // alone at the end: on the light-cone blocks, which are mostly
+    // rotations, U takes about a third of the row operations.
+    struct LocalGate {
+        int nq;
         int lb[5];
-        for (int i = 0; i < nq; i++) lb[i] = (int)(std::lower_bound(cov.begin(), cov.end(), g.qbits[i]) - cov.begin());
+        size_t off;  // its matrix at mats[off], 2^nq x 2^nq
+    };
+    std::vector<LocalGate> ops;
+    std::vector<Cx> mats;
+    ops.reserve(gl.size());
+    Cx Gbuf[32 * 32];
+    Cx pend[5][4];
+    bool has_pend[5] = {false, false, false, false, false};
+    auto mul2 = [](const Cx* a, const Cx* b, Cx* r) {  // r = a b (2x2)
+        Cx t[4];
+        for (int x = 0; x < 2; x++)
+            for (int y = 0; y < 2; y++) t[2 * x + y] = a[2 * x] * b[y] + a[2 * x + 1] * b[2 + y];
+        for (int x = 0; x < 4; x++) r[x] = t[x];
+    };
+    for (const Gate& g : gl) {
+        LocalGate L;
+        L.nq = (int)g.qbits.size();
+        const int gd = 1 << L.nq;
+        for (int i = 0; i < L.nq; i++)
+            L.lb[i] = (int)(std::lower_bound(cov.begin(), cov.end(), g.qbits[i]) - cov.begin());
         // The gate's own matrix, bit i of its index = qbits[i].
+        Cx* G = Gbuf;
         for (int i = 0; i < gd * gd; i++) G[i] = Cx(0, 0);
         switch (g.id) {
         case G_DENSE:
@@ -214,6 +231,50 @@ std::string merge_block(const std::vector<Gate>& gl, Gate* out) {
             for (int i = 0; i < gd; i++) G[i * gd + i] = Cx(1, 0);
             break;
         }
+        if (L.nq == 1) {
+            const int q = L.lb[0];
+            if (has_pend[q]) mul2(G, pend[q], pend[q]);
+            else for (int x = 0; x < 4; x++) pend[q][x] = G[x];
+            has_pend[q] = true;
+            continue;
+        }
+        // G' = G (I (x) P (x) I) for each pending P on the gate's bit i.
+        for (int i = 0; i < L.nq; i++) {
+            const int q = L.lb[i];
+            if (!has_pend[q]) continue;
+            const Cx* P = pend[q];
+            for (int r = 0; r < gd; r++)
+                for (int c0 = 0; c0 < gd; c0++) {
+                    if ((c0 >> i) & 1) continue;
+                    const int c1 = c0 | (1 << i);
+                    const Cx g0 = G[r * gd + c0], g1 = G[r * gd + c1];
+                    G[r * gd + c0] = g0 * P[0] + g1 * P[2];
+                    G[r * gd + c1] = g0 * P[1] + g1 * P[3];
+                }
+            has_pend[q] = false;
+        }
+        L.off = mats.size();
+        mats.insert(mats.end(), G, G + gd * gd);
+        ops.push_back(L);
+    }
+    for (int q = 0; q < k; q++)
+        if (has_pend[q]) {
+            LocalGate L;
+            L.nq = 1;
+            L.lb[0] = q;
+            L.off = mats.size();
+            mats.insert(mats.end(), pend[q], pend[q] + 4);
+            ops.push_back(L);
+        }
+    // U in separate real and imaginary planes (row-major), so the row
+    // updates below vectorise.
+    double ure[32 * 32], uim[32 * 32];
+    for (int i = 0; i < dim * dim; i++) ure[i] = uim[i] = 0.0;
+    for (int r = 0; r < dim; r++) ure[r * dim + r] = 1.0;
+    double rre[32][32], rim[32][32];
+    for (const LocalGate& L : ops) {
+        const int nq = L.nq, gd = 1 << nq;
+        const Cx* G = mats.data() + L.off;
         bool diag = true;
         for (int r = 0; r < gd && diag; r++)
             for (int c = 0; c < gd; c++)
@@ -222,13 +283,13 @@ std::string merge_block(const std::vector<Gate>& gl, Gate* out) {
                     break;
                 }
         uint32_t tm = 0;
-        for (int i = 0; i < nq; i++) tm |= 1u << lb[i];
+        for (int i = 0; i < nq; i++) tm |= 1u << L.lb[i];
         for (int base = 0; base < dim; base++) {
             if ((uint32_t)base & tm) continue;
             int idx[32];
             for (int s2 = 0; s2 < gd; s2++) {
                 int x = base;
-                for (int i = 0; i < nq; i++) x |= ((s2 >> i) & 1) << lb[i];
+                for (int i = 0; i < nq; i++) x |= ((s2 >> i) & 1) << L.lb[i];
                 idx[s2] = x;
             }
             if (diag) {  // scale each row

@@ -95,8 +95,8 @@ constexpr uint32_t BLK_REGION = 1024 + BLK_IMG + BLK_PROG + blk::TAB_BYTES + blk
 static_assert(sizeof(BlockProg) % 8 == 0, "BlockProg is copied as 8-byte words");
 // Per CTA, for the whole launch (complex64 batches with block programs):
 // the products' mbarrier and its phase, the TMEM columns, the wait flag.
-__shared__ uint64_t blk_mbar;
-__shared__ uint32_t blk_tmem, blk_phase;
+__shared__ uint64_t blk_mbar, blk_mbar_img;
+__shared__ uint32_t blk_tmem, blk_phase, blk_phase_img;
 __shared__ int blk_abort;
 
 // A complex64 tensor-core block pass over cosets [c0, c1) of one circuit
@@ -123,16 +123,14 @@ __device__ __noinline__ bool block_task(float2* st, const BatchProg& BP, const u
     for (uint32_t i = t; i < sizeof(BlockProg) / 8; i += NT)
         reinterpret_cast<uint64_t*>(&P)[i] = __ldcg(reinterpret_cast<const unsigned long long*>(src) + i);
     __syncthreads();
-    for (int b = 0; b < P.nblocks; b++) {
-        const unsigned char* img = src + P.bimg[b];
-        const uint32_t dst = bbase + (uint32_t)b * KATE_BLOCK_IMG_BYTES;
-        for (uint32_t off = t * 16; off < KATE_BLOCK_IMG_BYTES; off += NT * 16)
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst + off), "l"(img + off) : "memory");
-    }
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    // The operand images by the bulk-copy engine (the previous task's
+    // products, the last readers of this region, completed before it ended).
+    uint32_t phase_img = blk_phase_img;
+    const bool img_ok = blk::load_images(P.nblocks, [&](int b) { return src + P.bimg[b]; }, bbase,
+                                         blk::smem_u32(&blk_mbar_img), phase_img);
+    if (!img_ok) *abort_flag = 1;
     blk::Pass X;
     blk::setup(P, tab, iot, X);
-    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -149,7 +147,10 @@ __device__ __noinline__ bool block_task(float2* st, const BatchProg& BP, const u
             if (ok) blk::store_tile<true>(P, X, iot, st, cb, S0);
             __syncthreads();
         }
-        if (t == 0) blk_phase = phase;
+        if (t == 0) {
+            blk_phase = phase;
+            blk_phase_img = phase_img;
+        }
         return ok;
     }
     blk::load_tile<true>(st, blk::coset_base(P, c0), sb0, X, iot);
@@ -174,7 +175,10 @@ __device__ __noinline__ bool block_task(float2* st, const BatchProg& BP, const u
     }
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
-    if (t == 0) blk_phase = phase;
+    if (t == 0) {
+        blk_phase = phase;
+        blk_phase_img = phase_img;
+    }
     return ok;
 }
 
@@ -424,8 +428,11 @@ __global__ void __launch_bounds__(NT, sizeof(C2) == 8 ? 2 : 1)
         if (tensor_blocks) {
             if (t == 0) {
                 asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(blk::smem_u32(&blk_mbar)) : "memory");
+                asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(blk::smem_u32(&blk_mbar_img)) : "memory");
+                asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
                 blk_abort = 0;
                 blk_phase = 0;
+                blk_phase_img = 0;
             }
             blk::tmem_alloc(&blk_tmem, blk::TMEM_COLS);
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");

@@ -115,6 +115,31 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
     return false;
 }
 
+// Copies the pass's block operand images (nblocks x KATE_BLOCK_IMG_BYTES,
+// contiguous per block, 16-byte aligned in global memory) into shared memory
+// at `dst` (block b at dst + b * KATE_BLOCK_IMG_BYTES) with the bulk-copy
+// engine: thread 0 announces the bytes on mbarrier `mbar` and issues one
+// cp.async.bulk per image; every thread waits (bounded) for the phase
+// `phase`, which it then flips. src(b) gives block b's global image.
+// Returns false when the wait gave up.
+template <typename Src>
+__device__ __forceinline__ bool load_images(int nblocks, Src src, uint32_t dst, uint32_t mbar, uint32_t& phase) {
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar),
+                     "r"((uint32_t)nblocks * KATE_BLOCK_IMG_BYTES)
+                     : "memory");
+        for (int b = 0; b < nblocks; b++)
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                    dst + (uint32_t)b * KATE_BLOCK_IMG_BYTES),
+                "l"(src(b)), "r"((uint32_t)KATE_BLOCK_IMG_BYTES), "r"(mbar)
+                : "memory");
+    }
+    const bool ok = mbar_wait(mbar, phase);
+    phase ^= 1u;
+    return ok;
+}
+
 // TMEM allocation of one CTA, `cols` columns (a power of two, 32..512;
 // warp 0 allocates; every thread reads the base after the barrier the
 // caller places). `slot` is a shared-memory word.

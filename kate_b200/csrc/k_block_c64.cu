@@ -24,7 +24,7 @@ using namespace blk;
 
 constexpr uint32_t OFF_B = 0;                                                   // blocks' B images
 constexpr uint32_t OFF_S = OFF_B + KATE_C64_MAX_BLOCKS * KATE_BLOCK_IMG_BYTES;  // two staging tiles
-constexpr uint32_t OFF_MISC = OFF_S + 2 * S_BYTES;                              // mbarrier, TMEM slot, abort flag
+constexpr uint32_t OFF_MISC = OFF_S + 2 * S_BYTES;  // products' mbarrier, TMEM slot, abort flag, images' mbarrier
 constexpr uint32_t OFF_TAB = OFF_MISC + 64;
 constexpr uint32_t OFF_IO = OFF_TAB + TAB_BYTES;
 constexpr uint32_t SMEM_BYTES = OFF_IO + IO_BYTES + 1024;  // + alignment slack
@@ -43,20 +43,20 @@ __global__ void __launch_bounds__(NT, 2)
     uint16_t* tab = reinterpret_cast<uint16_t*>(gbase + OFF_TAB);
     uint16_t* iot = reinterpret_cast<uint16_t*>(gbase + OFF_IO);
 
+    const uint32_t mbar_img = base + OFF_MISC + 24;
     if (t == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar_img) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         *abort_flag = 0;
     }
     tmem_alloc(tmem_slot, TMEM_COLS);
-    // Block matrices: B images into shared memory once.
-    for (int b = 0; b < P.nblocks; b++) {
-        const uint8_t* src = bimg + P.bimg[b];
-        const uint32_t dst = base + OFF_B + b * KATE_BLOCK_IMG_BYTES;
-        for (uint32_t off = t * 16; off < KATE_BLOCK_IMG_BYTES; off += NT * 16)
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst + off), "l"(src + off) : "memory");
-    }
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
+    // Block matrices: B images into shared memory once, by the bulk-copy engine.
+    uint32_t phase_img = 0;
+    if (!load_images(P.nblocks, [&](int b) { return bimg + P.bimg[b]; }, base + OFF_B, mbar_img, phase_img) &&
+        t == 0)
+        *abort_flag = 1;
     Pass X;
     setup(P, tab, iot, X);
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
