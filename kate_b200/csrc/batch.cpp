@@ -520,7 +520,7 @@ std::string Batch::create(const std::vector<const Program*>& circuits, int preci
     S->upload_bytes = S->tasks.size() * sizeof(BatchTask) + S->circs.size() * sizeof(BatchCirc) +
                       S->progs.size() * sizeof(BatchProg) + S->sops.size() * sizeof(DevOp) + S->blob_bytes +
                       S->pool.size() * sizeof(Cx);
-    S->grid = batch_grid(device, precision);
+    S->grid = batch_grid(device, precision, S->tensor_blocks);
     const int grid = (int)std::min<size_t>((size_t)S->grid, S->tasks.size());
     S->create_ms[2] = ms_since(t0);
     t0 = clk::now();

@@ -403,14 +403,18 @@ __device__ __forceinline__ void init_basis0(C2* tile, bool one, uint32_t t) {
 }
 
 // complex64: two CTAs per SM (128 registers); complex128 programs need more.
-template <typename C2>
+// TB (complex64 only): the batch has tensor-core block programs; the kernel
+// then holds TMEM and the block region of shared memory. Batches without
+// them use the kernel compiled without that code (less shared memory, more
+// L1, no spills from it in the task loop).
+template <typename C2, bool TB>
 __global__ void __launch_bounds__(NT, sizeof(C2) == 8 ? 2 : 1)
     k_batch(C2* __restrict__ arena, const BatchTask* __restrict__ tasks, int ntasks, const BatchCirc* __restrict__ circs,
             const BatchProg* __restrict__ progs, const unsigned char* __restrict__ blob, const DevOp* __restrict__ sops,
             const double2* __restrict__ pool, int* __restrict__ head, int* __restrict__ done,
             double* __restrict__ zout, int* __restrict__ err, double* __restrict__ psum,
-            const double* __restrict__ unif, uint64_t* __restrict__ sout, unsigned long long wait_ns,
-            int tensor_blocks) {
+            const double* __restrict__ unif, uint64_t* __restrict__ sout, unsigned long long wait_ns) {
+    static_assert(!TB || sizeof(C2) == 8, "tensor-core block tasks are complex64");
     // Two tile buffers (a pass task prefetches its next coset into the
     // other one), then the program tables.
     C2* tile = reinterpret_cast<C2*>(batch_smem_raw);
@@ -424,8 +428,8 @@ __global__ void __launch_bounds__(NT, sizeof(C2) == 8 ? 2 : 1)
     const uint32_t tb = (uint32_t)__cvta_generic_to_shared(tile);
     // Tensor-core block tasks (complex64 only): the CTA's TMEM columns and
     // the products' mbarrier, for the whole launch.
-    if constexpr (sizeof(C2) == 8) {
-        if (tensor_blocks) {
+    if constexpr (TB) {
+        {
             if (t == 0) {
                 asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(blk::smem_u32(&blk_mbar)) : "memory");
                 asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(blk::smem_u32(&blk_mbar_img)) : "memory");
@@ -469,10 +473,9 @@ __global__ void __launch_bounds__(NT, sizeof(C2) == 8 ? 2 : 1)
         const int64_t zoff = circs[K.circ].zoff;
 
         bool block_pass = false;
-        if constexpr (sizeof(C2) == 8) block_pass = K.kind == BT_PASS && (progs[K.prog].flags & BPROG_BLOCK);
+        if constexpr (TB) block_pass = K.kind == BT_PASS && (progs[K.prog].flags & BPROG_BLOCK);
         if (block_pass) {
-            if constexpr (sizeof(C2) == 8) {
-                // tensor_blocks is set whenever the batch has block programs.
+            if constexpr (TB) {
                 if (!block_task(arena + circs[K.circ].off, progs[K.prog], blob, K.c0, K.c1, K.first != 0)) {
                     if (t == 0) atomicExch(err, 1);
                     break;
@@ -543,51 +546,54 @@ __global__ void __launch_bounds__(NT, sizeof(C2) == 8 ? 2 : 1)
             atomicAdd(done + K.circ, 1);
         }
     }
-    if constexpr (sizeof(C2) == 8) {
-        if (tensor_blocks) blk::tmem_free(blk_tmem, blk::TMEM_COLS);
-    }
+    if constexpr (TB) blk::tmem_free(blk_tmem, blk::TMEM_COLS);
 }
 
-template <typename C2>
+template <typename C2, bool TB>
 constexpr size_t batch_smem() {
-    // complex64: the tables or the tensor-core block region, whichever is larger.
+    // Two tiles, then the tables or (TB) the tensor-core block region,
+    // whichever is larger.
     return (size_t)2 * TS * sizeof(C2) +
-           (sizeof(C2) == 8 && BLK_REGION > sizeof(TileTables<C2>) ? BLK_REGION : sizeof(TileTables<C2>));
+           (TB && BLK_REGION > sizeof(TileTables<C2>) ? BLK_REGION : sizeof(TileTables<C2>));
 }
 
 }  // namespace
 
-int batch_grid(int device, int prec) {
-    static int cached[64][2] = {{0}};
+int batch_grid(int device, int prec, bool tensor_blocks) {
+    static int cached[64][3] = {{0}};
     if (device < 0 || device >= 64) device = 0;
-    const int pi = prec == 1 ? 1 : 0;
+    const int pi = prec == 1 ? (tensor_blocks ? 2 : 1) : 0;
     if (!cached[device][pi]) {
         int sms = 148, occ = 1;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-        // Two CTAs per SM need most of the SM's shared memory (about 100 KiB
-        // each for complex64): ask for the largest carveout.
-        if (pi == 1) {
-            cudaFuncSetAttribute(k_batch<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)batch_smem<float2>());
-            cudaFuncSetAttribute(k_batch<float2>, cudaFuncAttributePreferredSharedMemoryCarveout,
+        if (pi == 2) {
+            // About 100 KiB of shared memory per CTA: two CTAs per SM need
+            // the largest carveout. The occupancy calculator reports one CTA
+            // per SM for this kernel (it holds tcgen05 code), although two fit
+            // and run together (measured: 570 against 932 ms per launch of
+            // the batching workload with tensor-core block tasks).
+            // __launch_bounds__ gives the registers for two; shared memory
+            // decides.
+            cudaFuncSetAttribute(k_batch<float2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)batch_smem<float2, true>());
+            cudaFuncSetAttribute(k_batch<float2, true>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                  (int)cudaSharedmemCarveoutMaxShared);
-            // The occupancy calculator reports one CTA per SM for this kernel
-            // (it holds tcgen05 code), although two fit and run together
-            // (measured: 570 against 932 ms per launch of the batching
-            // workload with tensor-core block tasks). __launch_bounds__
-            // gives the registers for two; shared memory decides.
             cudaFuncAttributes fa{};
-            cudaFuncGetAttributes(&fa, k_batch<float2>);
+            cudaFuncGetAttributes(&fa, k_batch<float2, true>);
             int smem_sm = 0, reserved = 0;
             cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device);
             cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, device);
-            occ = smem_sm / (int)(batch_smem<float2>() + fa.sharedSizeBytes + reserved);
+            occ = smem_sm / (int)(batch_smem<float2, true>() + fa.sharedSizeBytes + reserved);
             if (occ > 2) occ = 2;
+        } else if (pi == 1) {
+            cudaFuncSetAttribute(k_batch<float2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)batch_smem<float2, false>());
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<float2, false>, NT, batch_smem<float2, false>());
         } else {
-            cudaFuncSetAttribute(k_batch<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)batch_smem<double2>());
-            cudaFuncSetAttribute(k_batch<double2>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                 (int)cudaSharedmemCarveoutMaxShared);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<double2>, NT, batch_smem<double2>());
+            cudaFuncSetAttribute(k_batch<double2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)batch_smem<double2, false>());
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<double2, false>, NT,
+                                                          batch_smem<double2, false>());
         }
         if (occ < 1) occ = 1;
         cached[device][pi] = sms * occ;
@@ -601,13 +607,15 @@ cudaError_t launch_batch(void* arena, int prec, const BatchTask* tasks, int ntas
                          const double* unif, uint64_t* sout, unsigned long long wait_ns, int tensor_blocks) {
     const unsigned char* b = (const unsigned char*)blob;
     const double2* pl = (const double2*)pool;
-    if (prec == 1)
-        k_batch<float2><<<grid, NT, batch_smem<float2>(), s>>>((float2*)arena, tasks, ntasks, circs, progs, b, sops, pl,
-                                                               head, done, zout, err, psum, unif, sout, wait_ns,
-                                                               tensor_blocks);
+    if (prec == 1 && tensor_blocks)
+        k_batch<float2, true><<<grid, NT, batch_smem<float2, true>(), s>>>(
+            (float2*)arena, tasks, ntasks, circs, progs, b, sops, pl, head, done, zout, err, psum, unif, sout, wait_ns);
+    else if (prec == 1)
+        k_batch<float2, false><<<grid, NT, batch_smem<float2, false>(), s>>>(
+            (float2*)arena, tasks, ntasks, circs, progs, b, sops, pl, head, done, zout, err, psum, unif, sout, wait_ns);
     else
-        k_batch<double2><<<grid, NT, batch_smem<double2>(), s>>>((double2*)arena, tasks, ntasks, circs, progs, b, sops,
-                                                                 pl, head, done, zout, err, psum, unif, sout, wait_ns, 0);
+        k_batch<double2, false><<<grid, NT, batch_smem<double2, false>(), s>>>(
+            (double2*)arena, tasks, ntasks, circs, progs, b, sops, pl, head, done, zout, err, psum, unif, sout, wait_ns);
     return cudaGetLastError();
 }
 

@@ -201,7 +201,6 @@ std::string merge_gates_device(const std::vector<std::vector<Gate>>& blocks, int
     int prev = -1;
     cudaGetDevice(&prev);
     if (cudaSetDevice(device) != cudaSuccess) return "cuda: cannot select the device";
-    std::string err;
     const size_t jb = jobs.size() * sizeof(MJob), gb = gates.size() * sizeof(MGate),
                  pb = pool.size() * sizeof(double2), ob = (size_t)out_elems * sizeof(double2);
     const size_t off_g = (jb + 255) & ~(size_t)255, off_p = (off_g + gb + 255) & ~(size_t)255,
@@ -245,7 +244,7 @@ std::string merge_gates_device(const std::vector<std::vector<Gate>>& blocks, int
         const double2* src = host.data() + jobs[b].out;
         for (size_t i = 0; i < n; i++) g.dense[i] = Cx(src[i].x, src[i].y);
     }
-    return err;
+    return "";
 }
 
 }  // namespace kate

@@ -84,7 +84,7 @@ cudaError_t launch_batch(void* arena, int prec, const BatchTask* tasks, int ntas
                          int* done, double* zout, int* err, int grid, cudaStream_t s, double* psum = nullptr,
                          const double* unif = nullptr, uint64_t* sout = nullptr,
                          unsigned long long wait_ns = 5000000000ull, int tensor_blocks = 0);
-int batch_grid(int device, int prec);
+int batch_grid(int device, int prec, bool tensor_blocks = false);
 
 // Bit sums: per CTA, for every local bit, the sum over amplitudes with the
 // bit 0 and with the bit 1, plus the total. kind 0 sums amplitudes (double2

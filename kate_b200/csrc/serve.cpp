@@ -738,7 +738,7 @@ std::string Server::create(int precision, int device, const ServeOptions& opt, S
     }
     S->states.init(budget, minb, 22);
     S->aux.init(opt.aux_bytes);
-    S->grid = batch_grid(device, precision);
+    S->grid = batch_grid(device, precision, precision == 1 && opt.tune.blocks);
     const int np = opt.planners > 0 ? opt.planners
                                     : (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
     for (int i = 0; i < np; i++) S->planners.emplace_back([S] { S->plan_loop(); });
