@@ -290,8 +290,11 @@ KATE_API kate_status kate_plan_get_program(const kate_plan* p, int i, void* out,
 KATE_API kate_status kate_plan_num_smem_ops(const kate_plan* p, int* out);
 /* CUDA source of the pass-specialised kernel of pass i: its register-staged
  * program as straight-line code, compiled for sm_100a with NVRTC when a
- * complex128 simulator is created. from_zero != 0: the form for the first
- * pass of a run from |0...0>, which generates its input. *size = bytes with
+ * complex128 simulator is created. from_zero 1: the form for the first
+ * pass of a run from |0...0>, which generates its input; 2: the form for
+ * the first pass of a run from a product state (execute(proba_state&)),
+ * which computes its input from per-qubit factors (a second kernel
+ * parameter). *size = bytes with
  * the terminating 0, copied when cap allows; KATE_EINVAL when the pass has
  * no such kernel (the simulator then interprets its program). Replaces the
  * reference's per-group kernel launch (HIPcode/simulator.hpp:143-218). */

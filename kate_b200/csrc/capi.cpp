@@ -706,7 +706,8 @@ kate_status kate_plan_pass_source(const kate_plan* p, int i, int from_zero, char
     const auto& pp = p->plan.passes[i];
     REQUIRE(pp.prog != nullptr, "pass has no register-staged program");
     std::string why;
-    const std::string src = kate::jit_pass_source(*pp.prog, &why, from_zero != 0);
+    REQUIRE(from_zero >= 0 && from_zero <= 2, "from_zero must be 0, 1 or 2");
+    const std::string src = kate::jit_pass_source(*pp.prog, &why, from_zero);
     REQUIRE(!src.empty(), "pass has no specialised kernel: " + why);
     *size = src.size() + 1;
     if (out && cap >= src.size() + 1) std::memcpy(out, src.c_str(), src.size() + 1);

@@ -170,7 +170,8 @@ bool lanes_ok(const PassProg& P, int st, const uint8_t* pos) {
 
 }  // namespace
 
-std::string jit_pass_source(const PassProg& P, std::string* why, bool from_zero, int occ) {
+std::string jit_pass_source(const PassProg& P, std::string* why, int form, int occ) {
+    const bool from_zero = form == 1, from_prod = form == 2;
     auto no = [&](const char* w) {
         if (why) *why = w;
         return std::string();
@@ -202,8 +203,10 @@ std::string jit_pass_source(const PassProg& P, std::string* why, bool from_zero,
     const int nm = std::max(1, (int)P.nmats);
     o << kPreamble;
     o << "struct __align__(16) Mats { double2 m[" << nm << "]; };\n";
+    if (from_prod) o << "struct __align__(16) ProdTab { double2 v[2][" << KATE_MAX_QUBITS << "]; };\n";
     o << "extern \"C\" __global__ void __launch_bounds__(256, " << occ
-      << ") kate_pass(double2* __restrict__ st, const __grid_constant__ Mats M) {\n";
+      << ") kate_pass(double2* __restrict__ st, const __grid_constant__ Mats M"
+      << (from_prod ? ", const __grid_constant__ ProdTab PI" : "") << ") {\n";
     o << "  extern __shared__ __align__(16) unsigned char smem[];\n";
     o << "  const u32 tb = (u32)__cvta_generic_to_shared(smem);\n";
     o << "  const u32 t = threadIdx.x;\n";
@@ -214,6 +217,22 @@ std::string jit_pass_source(const PassProg& P, std::string* why, bool from_zero,
         if (used[s] && s != first) o << "  const u32 s0_" << s << " = " << g.thr_expr("u32", s, false, nullptr) << ";\n";
     o << "  const u32 s0_" << first << " = " << g.thr_expr("u32", first, false, nullptr) << ";\n";
     if (okL) o << "  const u64 pin = " << g.thr_expr("u64", first, true, g.in) << ";\n";
+    // Tile index (bit k = tile bit k, at physical bit tphys[k]) of a
+    // physical offset made of tile bits only.
+    auto tidx = [&](uint64_t x) {
+        uint32_t r = 0;
+        for (int k = 0; k < TB; k++)
+            if ((x >> P.tphys[k]) & 1ull) r |= 1u << k;
+        return r;
+    };
+    if (from_prod && okL) {
+        std::string e = "(u32)0";
+        for (int i = 0; i < 8; i++) {
+            const uint32_t w = tidx(slot_phys(tvec(P, first, i) >> 4, g.in));
+            if (w) e += " ^ ((t & " + hex32(1u << i) + ") ? " + hex32(w) + " : 0u)";
+        }
+        o << "  const u32 tin = " << e << ";\n";
+    }
     if (okS) o << "  const u64 pout = " << g.thr_expr("u64", last, true, g.out) << ";\n";
     if (!okL || !okS) {
         // Copy j of thread t moves tile element t + 256 j: global offset
@@ -262,8 +281,30 @@ std::string jit_pass_source(const PassProg& P, std::string* why, bool from_zero,
         }
         o << "      return;\n    }\n";
     }
+    if (from_prod) {
+        // The input is the product state prod_p v[bit p][p]: its amplitude
+        // is the coset's factor (the coset bits, once per CTA) times the
+        // tile factor, read from two 64-entry tables (tile bits 0..5 and
+        // 6..11) that the CTA builds first.
+        o << "    __shared__ double2 ptl[64], pth[64];\n";
+        o << "    double2 fc = mk(1.0, 0.0);\n";
+        for (int i = 0; i < P.ncb; i++)
+            o << "    fc = cmul(fc, ((cb >> " << (int)P.cphys[i] << ") & 1ull) ? PI.v[1][" << (int)P.cphys[i]
+              << "] : PI.v[0][" << (int)P.cphys[i] << "]);\n";
+        o << "    if (t < 128) {\n      const u32 u = t & 63u;\n      double2 f = mk(1.0, 0.0);\n";
+        o << "      if (t < 64) {\n";
+        for (int k = 0; k < 6; k++)
+            o << "        f = cmul(f, ((u >> " << k << ") & 1u) ? PI.v[1][" << (int)P.tphys[k] << "] : PI.v[0]["
+              << (int)P.tphys[k] << "]);\n";
+        o << "        ptl[u] = f;\n      } else {\n";
+        for (int k = 0; k < 6; k++)
+            o << "        f = cmul(f, ((u >> " << k << ") & 1u) ? PI.v[1][" << (int)P.tphys[6 + k] << "] : PI.v[0]["
+              << (int)P.tphys[6 + k] << "]);\n";
+        o << "        pth[u] = f;\n      }\n    }\n    __syncthreads();\n";
+    }
     o << "    double2 a0, a1, a2, a3, a4, a5, a6, a7, a8, a9, a10, a11, a12, a13, a14, a15;\n";
     o << "    u32 lfl = 0, sfl = 0; u64 lflp = 0, sflp = 0;\n";
+    if (from_prod) o << "    u32 lflt = 0;\n";
     bool open = false, started = false;
     int si = -1;
     for (int k = 0; k < P.nops; k++) {
@@ -275,7 +316,29 @@ std::string jit_pass_source(const PassProg& P, std::string* why, bool from_zero,
                     o << "    sts(tb + ((s0_" << si << " ^ sfl) ^ " << hex32(rvec(P, si, 36, j)) << "), a" << j << ");\n";
             }
             si = op.idx;
-            if (!started && from_zero) {
+            if (!started && from_prod) {
+                if (okL) {
+                    o << "    { const u32 ti = tin ^ lflt;\n";
+                    for (int j = 0; j < 16; j++) {
+                        const uint32_t tc = tidx(slot_phys(rvec(P, si, 32, j) >> 4, g.in));
+                        o << "      { const u32 e = ti ^ " << hex32(tc) << "; a" << j
+                          << " = cmul(fc, cmul(ptl[e & 63u], pth[e >> 6])); }\n";
+                    }
+                    o << "    }\n";
+                } else {
+                    // Element t + 256 j goes where the copy-in would have put it.
+                    for (int j = 0; j < 16; j++)
+                        o << "    { const u32 e = t | " << hex32((uint32_t)j << 8)
+                          << "; sts(tb + (csw ^ " << hex32(swz((uint32_t)j << 8) << 4)
+                          << "), cmul(fc, cmul(ptl[e & 63u], pth[e >> 6]))); }\n";
+                    o << "    __syncthreads();\n";
+                    o << "    { const u32 sl = s0_" << si << " ^ lfl;\n";
+                    for (int j = 0; j < 16; j++)
+                        o << "      a" << j << " = lds(tb + (sl ^ " << hex32(rvec(P, si, 32, j)) << "));\n";
+                    o << "    }\n";
+                }
+                started = true;
+            } else if (!started && from_zero) {
                 // Coset 0 of |0...0>: the amplitude at global index 0 is 1.
                 if (okL) {
                     o << "    { const u64 b = pin ^ lflp;\n";
@@ -329,7 +392,9 @@ std::string jit_pass_source(const PassProg& P, std::string* why, bool from_zero,
             break;
         case SOP_XL:
             o << "    if (" << g.cond(op.cthr, op.ccos) << ") { lfl ^= " << hex32(op.idx)
-              << "; lflp ^= " << hex(slot_phys((uint32_t)op.idx >> 4, g.in)) << "; }\n";
+              << "; lflp ^= " << hex(slot_phys((uint32_t)op.idx >> 4, g.in)) << ";";
+            if (from_prod && !started) o << " lflt ^= " << hex32(tidx(slot_phys((uint32_t)op.idx >> 4, g.in))) << ";";
+            o << " }\n";
             break;
         case SOP_U: {
             const int i = op.idx;
@@ -624,10 +689,10 @@ std::string jit_compile(int device, const std::vector<std::string>& srcs, std::v
     return "";
 }
 
-std::string jit_pass_key(const PassProg& P, bool from_zero, int occ) {
+std::string jit_pass_key(const PassProg& P, int form, int occ) {
     std::string k;
     auto put = [&](const void* p, size_t n) { k.append(static_cast<const char*>(p), n); };
-    const int32_t head[7] = {P.m, P.ncb, P.nops, P.nmats, P.nstages, from_zero ? 1 : 0, occ};
+    const int32_t head[7] = {P.m, P.ncb, P.nops, P.nmats, P.nstages, form, occ};
     put(head, sizeof head);
     put(P.tphys, sizeof P.tphys);
     put(P.outsrc, sizeof P.outsrc);
@@ -674,6 +739,16 @@ int jit_local_bytes(void* fn) {
 int jit_grid(int ncb, int device) {
     (void)device;
     return 1 << ncb;  // one coset per CTA
+}
+
+cudaError_t jit_launch_prod(void* fn, void* st, const PassProg& prog, const ProdTab& pt, int grid, cudaStream_t s) {
+    double2 mats[KATE_MAX_MATS];
+    const int nm = std::max(1, (int)prog.nmats);
+    for (int i = 0; i < nm; i++) mats[i] = make_double2(i < prog.nmats ? prog.mats[i][0] : 0.0, i < prog.nmats ? prog.mats[i][1] : 0.0);
+    ProdTab p = pt;
+    void* args[] = {&st, mats, &p};
+    const CUresult r = api().launch((CUfunction)fn, grid, 1, 1, 256, 1, 1, 65536, (CUstream)s, args, nullptr);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorLaunchFailure;
 }
 
 cudaError_t jit_launch(void* fn, void* st, const PassProg& prog, int grid, cudaStream_t s) {

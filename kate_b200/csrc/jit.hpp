@@ -31,7 +31,12 @@ namespace kate {
 // being read), so the run needs no separate initialisation pass.
 // occ: CTAs per SM the kernel is compiled for (launch bounds; each CTA
 // holds a 64 KiB exchange tile, so at most 3).
-std::string jit_pass_source(const PassProg& prog, std::string* why, bool from_zero = false, int occ = 2);
+// form 2: the first pass of a run from a product state (execute with
+// per-qubit (theta, phi)): its input is computed, as amplitude = prod_p
+// v[bit p][p] (coset factor times two 64-entry tile tables), from a second
+// parameter (ProdTab), so no initialisation pass runs and the state is not
+// read.
+std::string jit_pass_source(const PassProg& prog, std::string* why, int form = 0, int occ = 2);
 
 // Compiles the sources not yet cached on `device` (in parallel) and returns
 // a kernel handle per source. Returns "" on success.
@@ -41,7 +46,7 @@ std::string jit_compile(int device, const std::vector<std::string>& srcs, std::v
 // the matrix values), with from_zero and occ: a key a few KB long, so a
 // simulator whose passes were compiled before finds their kernels without
 // generating their sources (about 0.2 ms per pass).
-std::string jit_pass_key(const PassProg& prog, bool from_zero, int occ);
+std::string jit_pass_key(const PassProg& prog, int form, int occ);
 // The kernel compiled on `device` for a pass key, or null.
 void* jit_find(int device, const std::string& key);
 // Records the kernel of a pass key (from jit_compile).
@@ -57,5 +62,11 @@ int jit_grid(int ncb, int device);
 // Launches kernel fn (from jit_compile) on the complex128 state st with the
 // matrices of prog.
 cudaError_t jit_launch(void* fn, void* st, const PassProg& prog, int grid, cudaStream_t s);
+// The per-qubit factors of a form-2 kernel: v[b][p] multiplies amplitudes
+// whose physical bit p is b.
+struct ProdTab {
+    double2 v[2][KATE_MAX_QUBITS];
+};
+cudaError_t jit_launch_prod(void* fn, void* st, const PassProg& prog, const ProdTab& pt, int grid, cudaStream_t s);
 
 }  // namespace kate

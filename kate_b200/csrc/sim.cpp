@@ -60,6 +60,9 @@ struct SimImpl {
     std::vector<void*> jit_fn;  // pass i runs on its pass-specialised kernel (complex128)
     void* jit_fn0 = nullptr;    // pass 0 generating its input |0...0> (no initialisation pass)
     bool zero_start = false;    // the run being enqueued starts with jit_fn0
+    void* jit_fnP = nullptr;    // pass 0 computing a product-state input (no initialisation pass)
+    bool prod_start = false;    // the run being enqueued starts with jit_fnP and prod_tab
+    ProdTab prod_tab{};
     int jit_grid_n = 0;
 
     // Launches pass i of the plan on stream st.
@@ -67,6 +70,7 @@ struct SimImpl {
         const PlannedPass& p = plan.passes[i];
         if (p.bprog) return launch_block_c64(d_state, *p.bprog, d_bimg, d_err, block_grid, st);
         if (i == 0 && zero_start && jit_fn0) return jit_launch(jit_fn0, d_state, *p.prog, jit_grid_n, st);
+        if (i == 0 && prod_start && jit_fnP) return jit_launch_prod(jit_fnP, d_state, *p.prog, prod_tab, jit_grid_n, st);
         if (p.prog && i < jit_fn.size() && jit_fn[i]) return jit_launch(jit_fn[i], d_state, *p.prog, jit_grid_n, st);
         if (p.prog && i < ws_ok.size() && ws_ok[i]) return launch_tile_ws(d_state, *p.prog, d_err, ws_grid, st);
         if (p.prog) return launch_tile(d_state, precision, *p.prog, d_sops, d_pool, tile_grid, nbuf, st);
@@ -230,23 +234,24 @@ std::string Simulator::create(const Program& prog_in, int precision, int device,
             const char* oe = std::getenv("KATE_JIT_OCC");
             const int occ_force = oe ? std::atoi(oe) : 0;
             const int occ_first = occ_force == 3 ? 3 : 2;
-            std::vector<size_t> idx;
-            std::vector<std::string> todo;
-            std::vector<char> zero_form;
+            // Kernels per (pass, form): form 0 loads its input, form 1 (pass
+            // 0) generates |0...0>, form 2 (pass 0) computes a product state.
             // Kernels compiled before for the same pass shape are found by
-            // key; only the others get their source generated (a pass the
-            // generator does not take is remembered as such, by a null).
+            // key; only the others get their source generated.
+            std::vector<size_t> idx;
+            std::vector<int> forms;
+            std::vector<std::string> todo;
             std::vector<void*> fns;
             std::vector<std::string> keys;
             std::vector<size_t> miss;
-            auto want = [&](size_t i, bool zf) {
-                std::string key = jit_pass_key(*impl->plan.passes[i].prog, zf, occ_first);
+            auto want = [&](size_t i, int form, int occ) {
+                std::string key = jit_pass_key(*impl->plan.passes[i].prog, form, occ);
                 void* f = jit_find(device, key);
                 idx.push_back(i);
-                zero_form.push_back(zf ? 1 : 0);
+                forms.push_back(form);
                 if (!f) {
                     miss.push_back(fns.size());
-                    todo.push_back(jit_pass_source(*impl->plan.passes[i].prog, nullptr, zf, occ_first));
+                    todo.push_back(jit_pass_source(*impl->plan.passes[i].prog, nullptr, form, occ));
                 }
                 fns.push_back(f);
                 keys.push_back(std::move(key));
@@ -254,13 +259,14 @@ std::string Simulator::create(const Program& prog_in, int precision, int device,
             for (size_t i = 0; i < impl->plan.passes.size(); i++) {
                 const PlannedPass& p = impl->plan.passes[i];
                 if (!p.prog || p.bprog) continue;
-                want(i, false);
+                want(i, 0, occ_first);
             }
-            // Pass 0 also in the form that generates |0...0> itself.
-            bool zero0 = !idx.empty() && idx[0] == 0;
-            if (zero0) want(0, true);
-            {
-                // Sources the generator declined: those passes keep the interpreter.
+            if (!idx.empty() && idx[0] == 0) {
+                want(0, 1, occ_first);
+                want(0, 2, occ_first);
+            }
+            auto compile_missing = [&]() -> std::string {
+                // Sources the generator declined stay null: those passes keep the interpreter.
                 std::vector<std::string> srcs;
                 std::vector<size_t> at;
                 for (size_t m = 0; m < miss.size(); m++)
@@ -270,47 +276,42 @@ std::string Simulator::create(const Program& prog_in, int precision, int device,
                     }
                 std::vector<void*> got;
                 std::string je = jit_compile(device, srcs, &got);
-                if (!je.empty()) return fail("pass kernel compilation: " + je);
+                if (!je.empty()) return je;
                 for (size_t m = 0; m < at.size(); m++) {
                     fns[at[m]] = got[m];
                     jit_remember(device, keys[at[m]], got[m]);
                 }
-            }
-            // Drop the passes without a kernel (the generator declined them).
-            {
-                std::vector<size_t> i2;
-                std::vector<char> z2;
-                std::vector<void*> f2;
-                for (size_t k = 0; k < fns.size(); k++) {
-                    if (!fns[k]) continue;
-                    i2.push_back(idx[k]);
-                    z2.push_back(zero_form[k]);
-                    f2.push_back(fns[k]);
-                }
-                zero0 = zero0 && !z2.empty() && z2.back() == 1;
-                idx.swap(i2);
-                zero_form.swap(z2);
-                fns.swap(f2);
-            }
+                miss.clear();
+                todo.clear();
+                return "";
+            };
+            std::string je = compile_missing();
+            if (!je.empty()) return fail("pass kernel compilation: " + je);
             if (occ_first == 3) {
-                std::vector<size_t> redo;
-                std::vector<std::string> src2;
+                // A kernel that spills at three CTAs per SM goes back to two.
                 for (size_t k = 0; k < fns.size(); k++)
-                    if (jit_local_bytes(fns[k]) != 0) {
-                        redo.push_back(k);
-                        src2.push_back(jit_pass_source(*impl->plan.passes[idx[k]].prog, nullptr, zero_form[k] != 0, 2));
+                    if (fns[k] && jit_local_bytes(fns[k]) != 0) {
+                        std::string key = jit_pass_key(*impl->plan.passes[idx[k]].prog, forms[k], 2);
+                        void* f = jit_find(device, key);
+                        if (!f) {
+                            miss.push_back(k);
+                            todo.push_back(jit_pass_source(*impl->plan.passes[idx[k]].prog, nullptr, forms[k], 2));
+                        }
+                        fns[k] = f;
+                        keys[k] = std::move(key);
                     }
-                if (!redo.empty()) {
-                    std::vector<void*> f2;
-                    const std::string je = jit_compile(device, src2, &f2);
-                    if (!je.empty()) return fail("pass kernel compilation: " + je);
-                    for (size_t r = 0; r < redo.size(); r++) fns[redo[r]] = f2[r];
-                }
+                je = compile_missing();
+                if (!je.empty()) return fail("pass kernel compilation: " + je);
             }
-            if (zero0) idx.pop_back();
             impl->jit_fn.assign(impl->plan.passes.size(), nullptr);
-            for (size_t k = 0; k < idx.size(); k++) impl->jit_fn[idx[k]] = fns[k];
-            if (zero0) impl->jit_fn0 = fns.back();
+            for (size_t k = 0; k < idx.size(); k++) {
+                if (!fns[k]) continue;
+                if (forms[k] == 0) impl->jit_fn[idx[k]] = fns[k];
+                else if (forms[k] == 1) impl->jit_fn0 = fns[k];
+                else impl->jit_fnP = fns[k];
+            }
+            // The start forms only serve when pass 0 itself has a kernel.
+            if (impl->jit_fn.empty() || !impl->jit_fn[0]) impl->jit_fn0 = impl->jit_fnP = nullptr;
             impl->jit_grid_n = jit_grid(impl->n - KATE_TILE_BITS, device);
         }
         const char* ws = std::getenv("KATE_TILE_WS");
@@ -388,28 +389,41 @@ std::string Simulator::enqueue_init(void* stream, const double* tp) {
             P.v[1][lab][0] = er * s0;
             P.v[1][lab][1] = ei * s0;
         }
+        S.prod_start = false;
+        if (S.jit_fnP && !S.hpasses.empty()) {
+            // The first pass computes the product state itself (no
+            // initialisation pass, and the state is not read).
+            for (int b = 0; b < 2; b++)
+                for (int p = 0; p < S.n; p++) S.prod_tab.v[b][p] = make_double2(P.v[b][p][0], P.v[b][p][1]);
+            S.prod_start = true;
+            S.zero_start = false;
+            return "";
+        }
         KCHECK(launch_init_product(S.d_state, S.n, P, S.precision, st));
     } else if (S.jit_fn0) {
         // The first pass writes the whole state from |0...0> itself.
         S.zero_start = true;
+        S.prod_start = false;
         return "";
     } else {
         KCHECK(launch_set_basis0(S.d_state, S.dim(), S.precision, st));
     }
     S.zero_start = false;
+    S.prod_start = false;
     return "";
 }
 
 std::string Simulator::enqueue_passes(void* stream) {
     SimImpl& S = *d_;
     cudaStream_t st = (cudaStream_t)stream;
-    const bool zs = S.zero_start;
-    S.zero_start = false;
+    const bool zs = S.zero_start, ps = S.prod_start;
+    S.zero_start = S.prod_start = false;
     if (zs && S.hpasses.empty()) KCHECK(launch_set_basis0(S.d_state, S.dim(), S.precision, st));
     for (size_t i = 0; i < S.hpasses.size(); i++) {
         S.zero_start = zs && i == 0;
+        S.prod_start = ps && i == 0;
         const cudaError_t ce = S.launch_pass(i, st);
-        S.zero_start = false;
+        S.zero_start = S.prod_start = false;
         KCHECK(ce);
     }
     if (S.precision == 1) {

@@ -64,3 +64,24 @@ def test_from_zero_first_pass_equals_product_state_start():
     s.execute(K.proba_state(np.zeros((n, 2))))
     b = s.state()
     assert np.abs(a - b).max() <= TOL
+
+
+@pytest.mark.parametrize("n,kind", [(16, "layered"), (20, "qulacs"), (13, "qft"), (22, "hea")])
+def test_product_state_start_matches_oracle(oracle, n, kind):
+    """execute(proba_state&) on a plan whose first pass has a specialised
+    kernel: that pass computes the product state itself (no initialisation
+    pass); amplitudes against the oracle at 1e-12, proba_state at 1e-9, and a
+    later run from |0...0> on the same simulator is unaffected."""
+    gates = {"layered": lambda: circuits.layered(n, 4, seed=n), "qulacs": lambda: circuits.qulacs_bench(n),
+             "qft": lambda: circuits.qft(n), "hea": lambda: circuits.hea(n, 6, seed=n)}[kind]()
+    rng = np.random.default_rng(50 + n)
+    tp = np.stack([rng.uniform(0, 1, n), rng.uniform(-np.pi, np.pi, n)], axis=1)
+    sim = K.Simulator(K.Circuit(n, gates), 1, K.C128, 0)
+    assert sim.pass_kernels()[0] == 2
+    res = sim.execute(K.proba_state(tp))
+    ref = oracle.simulate(n, gates, proba_in=tp)
+    assert np.abs(sim.state() - ref).max() <= 1e-12
+    assert np.abs(res.as_array() - oracle.measure(n, ref)).max() <= 1e-9
+    sim.execute()
+    assert np.abs(sim.state() - oracle.simulate(n, gates)).max() <= 1e-12
+    sim.close()

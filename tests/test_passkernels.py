@@ -94,10 +94,36 @@ def test_generated_sources_compile_for_sm100a():
     L, h = plan(c)
     try:
         # A two-stage pass with direct HBM I/O, a pass copied in/out through
-        # shared memory, the eight-stage pass, and pass 0 generating |0...0>.
-        for i, fz in ((2, 0), (10, 0), (19, 0), (0, 1)):
+        # shared memory, the eight-stage pass, pass 0 generating |0...0> and
+        # pass 0 computing a product-state input.
+        for i, fz in ((2, 0), (10, 0), (19, 0), (0, 1), (0, 2)):
             r, log, nbytes = nvrtc_compile(lib, source(L, h, i, fz))
             assert r == 0, log
             assert nbytes > 0
     finally:
         L.kate_plan_destroy(h)
+
+
+def test_product_form_of_first_passes_compiles():
+    """The form of pass 0 that computes a product-state input (per-qubit
+    factors as a second parameter): for first passes that load straight from
+    HBM and for ones that copy in through shared memory."""
+    lib = nvrtc()
+    if lib is None:
+        pytest.skip("libnvrtc not available")
+    seen = set()
+    for n, gates in ((30, circuits.layered(30, 20, seed=1234)), (20, circuits.qulacs_bench(20)),
+                     (16, circuits.qft(16)), (22, circuits.hea(22, 4, seed=3))):
+        c = K.Circuit(n, gates)
+        L, h = plan(c)
+        try:
+            src = source(L, h, 0, 2)
+            if src is None:
+                continue
+            assert "ProdTab PI" in src and "ptl[" in src
+            seen.add("cp.async" in source(L, h, 0, 0))
+            r, log, nbytes = nvrtc_compile(lib, src)
+            assert r == 0, log
+        finally:
+            L.kate_plan_destroy(h)
+    assert seen, "no first pass had a product form"
