@@ -271,6 +271,8 @@ KATE_API kate_status kate_sim_norm2_before_renorm(kate_sim* s, double* norm2);
 #define KATE_PLAN_NO_FUSE1Q 2u  /* do not multiply single-qubit chains */
 #define KATE_PLAN_C64 4u        /* complex64 plan: dense 5-qubit tensor-core blocks */
 #define KATE_PLAN_NO_DENSE2 8u  /* dense two-qubit gates as shared-memory ops, not register ops */
+#define KATE_PLAN_REMAP_SEARCH 16u /* choose the qubits moved into the low bits by trying every subset
+                                      of the tile (what complex128 simulators do) */
 KATE_API kate_status kate_plan_create(const kate_circuit* c, int max_tile, int coalesce, unsigned flags,
                                       kate_plan** out);
 KATE_API kate_status kate_plan_destroy(kate_plan* p);

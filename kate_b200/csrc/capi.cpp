@@ -610,6 +610,7 @@ kate_status kate_plan_create(const kate_circuit* c, int max_tile, int coalesce, 
         opt.max_tile = max_tile;
         opt.coalesce = coalesce;
         opt.remap = !(flags & KATE_PLAN_NO_REMAP);
+        opt.remap_search = (flags & KATE_PLAN_REMAP_SEARCH) != 0;
         opt.fuse_1q = !(flags & KATE_PLAN_NO_FUSE1Q);
         opt.c64 = (flags & KATE_PLAN_C64) != 0;
         opt.dense2_reg = !opt.c64 && !(flags & KATE_PLAN_NO_DENSE2);

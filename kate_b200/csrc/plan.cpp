@@ -596,7 +596,36 @@ std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out) {
         std::sort(S.begin(), S.end());
         // Choose the qubits that the next pass wants at the low positions.
         std::vector<int> newlow;
-        if (opt.remap && !rem.empty()) {
+        if (opt.remap && opt.remap_search && !rem.empty() && !blocks && c > 0 && c < m) {
+            // Every c-subset of the tile (ascending logical ids, first best
+            // kept): the one with which the next pass's greedy selection
+            // takes the most gates.
+            std::vector<int> T;
+            for (int q = 0; q < n; q++)
+                if (inT[q]) T.push_back(q);
+            std::vector<int> idx(c);
+            std::iota(idx.begin(), idx.end(), 0);
+            size_t best = 0;
+            std::vector<char> inT2(n, 0);
+            const int nt = (int)T.size();
+            while (true) {
+                std::fill(inT2.begin(), inT2.end(), 0);
+                for (int i : idx) inT2[T[i]] = 1;
+                int ts2 = c;
+                const size_t got =
+                    greedy_pass(plan.pgates, rem, n, mg, inT2, ts2, nullptr, scan_limit, opt.c64).size();
+                if (got > best) {
+                    best = got;
+                    newlow.clear();
+                    for (int i : idx) newlow.push_back(T[i]);
+                }
+                int i = c - 1;
+                while (i >= 0 && idx[i] == nt - c + i) i--;
+                if (i < 0) break;
+                idx[i]++;
+                for (int j = i + 1; j < c; j++) idx[j] = idx[j - 1] + 1;
+            }
+        } else if (opt.remap && !rem.empty()) {
             std::vector<char> inT2(n, 0);
             int ts2 = 0;
             std::vector<int> order;

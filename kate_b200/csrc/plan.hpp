@@ -20,6 +20,11 @@
 // may write its tile back with its tile bits permuted, which moves c qubits
 // that the next pass needs into those low positions at no extra HBM cost.
 // Swap instructions of the compiled program become pure relabelings.
+// Which c tile qubits go low decides what the next pass can take (it holds
+// them and m - c more). With remap_search the planner tries every c-subset
+// of the tile and keeps the one that lets the next pass take the most
+// gates; otherwise it takes the first c tile qubits the next pass's greedy
+// selection reaches.
 #pragma once
 
 #include <cstdint>
@@ -38,6 +43,7 @@ struct PlanOptions {
                            // rest of the tile is filled with other qubits (the reference's gateGrouping(m))
     int coalesce = 4;    // c: low physical bits every tile must contain
     bool remap = true;   // move next-needed qubits into the low bits on write
+    bool remap_search = false;  // choose those qubits by trying every c-subset of the tile
     bool fuse_1q = true; // multiply chains of single-qubit ops on one qubit (FP64, host)
     bool staged = true;  // build register-staged programs for the tile kernel
     bool c64 = false;    // complex64 state: passes become dense 5-qubit tensor-core blocks

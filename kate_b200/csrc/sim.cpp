@@ -161,6 +161,12 @@ std::string Simulator::create(const Program& prog_in, int precision, int device,
         const char* jv = std::getenv("KATE_JIT");
         impl->opt.dense2_reg = precision == 0 && !(jv && std::atoi(jv) == 0);
     }
+    // Complex128 passes choose the qubits they move into the low bits by
+    // trying every subset (a few ms of planning for a 30-qubit circuit).
+    {
+        const char* rs = std::getenv("KATE_REMAP_SEARCH");
+        impl->opt.remap_search = precision == 0 && !(rs && std::atoi(rs) == 0);
+    }
     // Contiguous low physical bits every tile holds (runs of 2^c amplitudes per access).
     if (const char* e = std::getenv("KATE_COALESCE")) {
         const int v = std::atoi(e);
