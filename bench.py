@@ -224,6 +224,40 @@ def pass_roofline(n, npass, launches, ms_per_step, init_ms):
     return step_bytes / npass, step_ms / npass, step_bytes / (step_ms / 1000.0) / 1e9
 
 
+FP64_PER_SM_CLK = 64     # FP64 instructions per SM per clock on B200 (ncu: dfma peak_sustained 64/SM)
+SMEM_BYTES_PER_SM_CLK = 128  # shared-memory bytes per SM per clock (32 banks x 4 B)
+
+
+def pass_bounds(n, work, pass_ms, hbm_gbs, sm_mhz, nsm):
+    """Lower bound of each group pass's time from the three rates it uses:
+    HBM bytes at the measured copy bandwidth, FP64 instructions and
+    shared-memory bytes at B200's per-SM-clock rates times the SM clock
+    sampled during the timed region. A pass is bound by the slowest; the
+    sum over passes against the measured per-pass times says how close
+    the kernels run to that bound."""
+    if not sm_mhz or not work or any(w is None for w in work):
+        return None
+    amps = 2.0 ** n
+    f = sm_mhz * 1e6
+    tot = {"hbm": 0.0, "fp64": 0.0, "smem": 0.0}
+    binding = {"hbm": 0, "fp64": 0, "smem": 0}
+    bound = 0.0
+    for (hb, fp, sb) in work:
+        t = {"hbm": hb * amps / (hbm_gbs * 1e9) * 1e3, "fp64": fp * amps / (FP64_PER_SM_CLK * nsm * f) * 1e3,
+             "smem": sb * amps / (SMEM_BYTES_PER_SM_CLK * nsm * f) * 1e3}
+        for k in tot:
+            tot[k] += t[k]
+        k = max(t, key=t.get)
+        binding[k] += 1
+        bound += t[k]
+    measured = float(sum(pass_ms))
+    return {"unit": "ms per step", "hbm_ms": tot["hbm"], "fp64_ms": tot["fp64"], "smem_ms": tot["smem"],
+            "bound_ms": bound, "measured_ms": measured, "frac": bound / measured if measured > 0 else None,
+            "passes_bound_by": binding, "sm_mhz": sm_mhz,
+            "rates": {"hbm_gbs": hbm_gbs, "fp64_per_sm_clk": FP64_PER_SM_CLK,
+                      "smem_bytes_per_sm_clk": SMEM_BYTES_PER_SM_CLK, "sms": nsm}}
+
+
 def committed_traffic(n):
     """Per-launch DRAM bytes of the group-pass kernel from the committed ncu
     summary (profiles/group_pass_traffic.json), scaled to 2^n amplitudes."""
@@ -451,6 +485,8 @@ def main():
     init_ms, pass_ms = sim.profile_passes()
     alg_bytes, avg_pass_ms, achieved = pass_roofline(n, len(passes), launches, ms_per_step, init_ms)
     peak, peak_kind = measured_hbm_peak()
+    sim_work = sim.pass_work()
+    clk_summary = clk.summary()
 
     # End to end through the C ABI with host buffers.
     e2e_steps = max(1, min(args.steps, 3))
@@ -512,9 +548,11 @@ def main():
                              "profiled_pass_ms": {"min": min(pass_ms), "max": max(pass_ms),
                                                   "mean": sum(pass_ms) / len(pass_ms)},
                              "per_pass_gbs": per_pass_gbs(2.0 * 16.0 * 2 ** n, pass_ms, peak),
-                             "frac_of_nominal": achieved / NOMINAL_HBM_GBS},
+                             "frac_of_nominal": achieved / NOMINAL_HBM_GBS,
+                             "pass_bounds": pass_bounds(n, sim_work, pass_ms, peak, clk_summary.get("sm_mhz"),
+                                                        torch.cuda.get_device_properties(dev).multi_processor_count)},
                 "passes_per_step": len(passes), "passes_per_layer": len(passes) / L,
-                "gpu_launches": launches * args.steps, "clocks": clk.summary(),
+                "gpu_launches": launches * args.steps, "clocks": clk_summary,
                 "cpu_baseline": cpu, "ref_gpu_baseline": ref_gpu}
         print(json.dumps(line))
     if dist:

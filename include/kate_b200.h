@@ -252,6 +252,13 @@ KATE_API kate_status kate_sim_get_pass(kate_sim* s, int i, int* tile_qbits, int*
  * Replaces the choice executeCommand makes per group instruction
  * (HIPcode/simulator.hpp:760-810). */
 KATE_API kate_status kate_sim_pass_kernel(kate_sim* s, int i, int* kind);
+/* Work per amplitude of pass i when its pass-specialised kernel (kind 2)
+ * runs it: out3 = {HBM bytes read and written, FP64 instructions (DFMA,
+ * DMUL, DADD as generated), shared-memory bytes stored and loaded}; with
+ * 2^n amplitudes and the GPU's rates they bound the pass's time.
+ * KATE_EINVAL for passes on other kernels. No counterpart in the
+ * reference. */
+KATE_API kate_status kate_sim_pass_work(kate_sim* s, int i, double* out3);
 /* Complex64 simulators renormalise the state at the end of every run:
  * ||psi||^2 is reduced in FP64 on the device and every amplitude multiplied
  * by 1 / ||psi|| (the tensor-core blocks' split-BF16 products do not keep
@@ -272,7 +279,8 @@ KATE_API kate_status kate_sim_norm2_before_renorm(kate_sim* s, double* norm2);
 #define KATE_PLAN_C64 4u        /* complex64 plan: dense 5-qubit tensor-core blocks */
 #define KATE_PLAN_NO_DENSE2 8u  /* dense two-qubit gates as shared-memory ops, not register ops */
 #define KATE_PLAN_REMAP_SEARCH 16u /* choose the qubits moved into the low bits by trying every subset
-                                      of the tile (what complex128 simulators do) */
+                                      of the tile, and the gate cap per pass among 96..144 (fewest
+                                      passes): what complex128 simulators do */
 KATE_API kate_status kate_plan_create(const kate_circuit* c, int max_tile, int coalesce, unsigned flags,
                                       kate_plan** out);
 KATE_API kate_status kate_plan_destroy(kate_plan* p);

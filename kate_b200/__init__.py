@@ -515,6 +515,18 @@ class Simulator:
             out.append(k.value)
         return out
 
+    def pass_work(self) -> List[Optional[Tuple[float, float, float]]]:
+        """Per pass, when its pass-specialised kernel runs it: (HBM bytes,
+        FP64 instructions, shared-memory bytes) per amplitude; else None."""
+        n = ctypes.c_int()
+        _check(self._lib.kate_sim_num_passes(self._h, ctypes.byref(n)))
+        out = []
+        for i in range(n.value):
+            v = (ctypes.c_double * 3)()
+            st = self._lib.kate_sim_pass_work(self._h, i, v)
+            out.append((v[0], v[1], v[2]) if st == 0 else None)
+        return out
+
     def launches_per_run(self) -> int:
         v = ctypes.c_int()
         _check(self._lib.kate_sim_launches_per_run(self._h, ctypes.byref(v)))

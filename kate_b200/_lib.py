@@ -65,6 +65,7 @@ SIGNATURES = {
     "kate_sim_profile_passes": [_vp, _c.POINTER(_c.c_float), _c.POINTER(_c.c_float)],
     "kate_sim_launches_per_run": [_vp, _ip],
     "kate_sim_pass_kernel": [_vp, _i, _ip],
+    "kate_sim_pass_work": [_vp, _i, _c.POINTER(_c.c_double)],
     "kate_batch_get_state": [_vp, _i, _dp],
     "kate_sim_norm2_before_renorm": [_vp, _dp],
     "kate_sim_num_passes": [_vp, _ip],

@@ -573,6 +573,13 @@ kate_status kate_sim_pass_kernel(kate_sim* s, int i, int* kind) {
     return KATE_OK;
 }
 
+kate_status kate_sim_pass_work(kate_sim* s, int i, double* out3) {
+    REQUIRE(s && out3, "null pointer");
+    REQUIRE(s->sim->pass_kernel(i) >= 0, "pass index out of range");
+    if (!s->sim->pass_work(i, out3)) return fail(KATE_EINVAL, "pass is not run by a pass-specialised kernel");
+    return KATE_OK;
+}
+
 kate_status kate_sim_nqbits(kate_sim* s, int* out) {
     REQUIRE(s && out, "null pointer");
     *out = s->sim->nqbits();
@@ -611,6 +618,7 @@ kate_status kate_plan_create(const kate_circuit* c, int max_tile, int coalesce, 
         opt.coalesce = coalesce;
         opt.remap = !(flags & KATE_PLAN_NO_REMAP);
         opt.remap_search = (flags & KATE_PLAN_REMAP_SEARCH) != 0;
+        opt.cap_search = opt.remap_search;
         opt.fuse_1q = !(flags & KATE_PLAN_NO_FUSE1Q);
         opt.c64 = (flags & KATE_PLAN_C64) != 0;
         opt.dense2_reg = !opt.c64 && !(flags & KATE_PLAN_NO_DENSE2);

@@ -170,6 +170,38 @@ bool lanes_ok(const PassProg& P, int st, const uint8_t* pos) {
 
 }  // namespace
 
+bool jit_pass_work(const PassProg& P, double* fp64, double* smem) {
+    std::string why;
+    if (jit_pass_source(P, &why).empty()) return false;
+    int first = -1, last = -1, exchanges = 0;
+    double f = 0.0;
+    for (int k = 0; k < P.nops; k++) {
+        const SOp& op = P.ops[k];
+        switch (op.kind) {
+        case SOP_STAGE:
+            if (first >= 0) exchanges++;
+            if (first < 0) first = op.idx;
+            last = op.idx;
+            break;
+        case SOP_U: f += 8; break;                          // row2: 2 DMUL + 6 DFMA per amplitude
+        case SOP_UR: case SOP_UX: f += 4; break;            // 2 DMUL + 2 DFMA
+        case SOP_URA: case SOP_URB: case SOP_UXA: case SOP_UXB: f += 2; break;  // 2 DFMA
+        case SOP_H: f += 3; break;                          // 2 DADD + 2 DMUL + 2 DFMA per pair
+        case SOP_U2: f += 16; break;                        // row4: 2 DMUL + 14 DFMA
+        case SOP_D1: case SOP_DR: f += 4; break;            // complex multiply: 2 DMUL + 2 DFMA
+        case SOP_PH: f += 4.0 / (double)(1u << __builtin_popcount(op.creg)); break;
+        default: break;
+        }
+    }
+    Gen g(P);
+    double b = 32.0 * exchanges;
+    if (!lanes_ok(P, first, g.in)) b += 32.0;
+    if (!lanes_ok(P, last, g.out)) b += 32.0;
+    *fp64 = f;
+    *smem = b;
+    return true;
+}
+
 std::string jit_pass_source(const PassProg& P, std::string* why, int form, int occ) {
     const bool from_zero = form == 1, from_prod = form == 2;
     auto no = [&](const char* w) {
@@ -200,6 +232,23 @@ std::string jit_pass_source(const PassProg& P, std::string* why, int form, int o
     const bool okL = lanes_ok(P, first, g.in), okS = lanes_ok(P, last, g.out);
     (void)wide;
     std::ostringstream& o = g.o;
+    int wbo[TB];
+    for (int i = 0; i < TB; i++) wbo[i] = i;
+    {
+        // First three of output tile bits 0..3 whose input bits have
+        // distinct residues mod 3, when there are such.
+        int pick[3] = {-1, -1, -1}, np = 0;
+        for (int a = 0; a < 4 && np < 3; a++)
+            for (int b = a + 1; b < 4 && np < 3; b++)
+                for (int c = b + 1; c < 4 && np < 3; c++) {
+                    const int ra = P.outsrc[a] % 3, rb = P.outsrc[b] % 3, rc = P.outsrc[c] % 3;
+                    if (ra != rb && rb != rc && ra != rc) pick[0] = a, pick[1] = b, pick[2] = c, np = 3;
+                }
+        if (np == 3) {
+            wbo[0] = pick[0], wbo[1] = pick[1], wbo[2] = pick[2];
+            wbo[3] = 6 - pick[0] - pick[1] - pick[2];
+        }
+    }
     const int nm = std::max(1, (int)P.nmats);
     o << kPreamble;
     o << "struct __align__(16) Mats { double2 m[" << nm << "]; };\n";
@@ -238,15 +287,21 @@ std::string jit_pass_source(const PassProg& P, std::string* why, int form, int o
         // Copy j of thread t moves tile element t + 256 j: global offset
         // dT(t) ^ goff(j), shared offset swz(t + 256 j) << 4; on write-back
         // output element t + 256 j reads input slot pT(t) ^ osw(j).
-        std::string dT = "(u64)0", sw = "(u32)0", pT = "(u32)0";
+        // The write-back's thread bits take the output tile bits in the
+        // order wbo: bits 0..3 stay on lanes 0..3 (256-byte runs), with the
+        // first three chosen so that the input slots they read lie in
+        // distinct bank groups (tile bits of distinct residue mod 3 under
+        // the swizzle), which keeps its shared-memory loads conflict-free.
+        std::string dT = "(u64)0", dO = "(u64)0", sw = "(u32)0", pT = "(u32)0";
         for (int i = 0; i < 8; i++) {
             dT += " ^ ((t & " + hex32(1u << i) + ") ? (u64)" + hex(1ull << P.tphys[i]) + " : (u64)0)";
+            dO += " ^ ((t & " + hex32(1u << i) + ") ? (u64)" + hex(1ull << P.tphys[wbo[i]]) + " : (u64)0)";
             sw += " ^ ((t & " + hex32(1u << i) + ") ? (u32)" + hex32(swz(1u << i) << 4) + " : (u32)0)";
-            pT += " ^ ((t & " + hex32(1u << i) + ") ? (u32)" + hex32(swz(1u << P.outsrc[i]) << 4) + " : (u32)0)";
+            pT += " ^ ((t & " + hex32(1u << i) + ") ? (u32)" + hex32(swz(1u << P.outsrc[wbo[i]]) << 4) + " : (u32)0)";
         }
         o << "  const u64 cdT = " << dT << ";\n";
         if (!okL) o << "  const u32 csw = " << sw << ";\n";
-        if (!okS) o << "  const u32 cpT = " << pT << ";\n";
+        if (!okS) o << "  const u64 cdO = " << dO << ";\n  const u32 cpT = " << pT << ";\n";
     }
     // Coset index -> physical offset: runs of consecutive coset bits.
     // One coset per CTA: with no loop there is nothing loop-invariant for
@@ -516,12 +571,12 @@ std::string jit_pass_source(const PassProg& P, std::string* why, int form, int o
     } else {
         for (int j = 0; j < 16; j++)
             o << "    sts(tb + ((s0_" << si << " ^ sfl) ^ " << hex32(rvec(P, si, 36, j)) << "), a" << j << ");\n";
-        o << "    __syncthreads();\n    { const u64 gb = cb ^ cdT;\n";
+        o << "    __syncthreads();\n    { const u64 gb = cb ^ cdO;\n";
         for (int j = 0; j < 16; j++) {
             uint64_t go = 0;
             uint32_t os = 0;
             for (int i = 0; i < 4; i++)
-                if ((j >> i) & 1) go |= 1ull << P.tphys[8 + i], os |= 1u << P.outsrc[8 + i];
+                if ((j >> i) & 1) go |= 1ull << P.tphys[wbo[8 + i]], os |= 1u << P.outsrc[wbo[8 + i]];
             o << "      st[gb ^ " << hex(go) << "] = lds(tb + (cpT ^ " << hex32(swz(os) << 4) << "));\n";
         }
         o << "    }\n";

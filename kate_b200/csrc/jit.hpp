@@ -52,6 +52,14 @@ void* jit_find(int device, const std::string& key);
 // Records the kernel of a pass key (from jit_compile).
 void jit_remember(int device, const std::string& key, void* fn);
 
+// Work per amplitude of the kernel jit_pass_source generates for `prog`
+// (form 0): FP64 instructions (DFMA, DMUL, DADD as emitted; NOTs are
+// register moves or address flips and count nothing) and shared-memory
+// bytes moved (16 B stored and 16 B loaded per amplitude for each stage
+// exchange, for a copy-in through the tile and for a write-back through
+// it). False when the generator does not take the program.
+bool jit_pass_work(const PassProg& prog, double* fp64_per_amp, double* smem_bytes_per_amp);
+
 // Local memory (register spill) bytes per thread of a compiled kernel; -1
 // when unknown.
 int jit_local_bytes(void* fn);

@@ -5,6 +5,7 @@
 #include <cmath>
 #include <numeric>
 #include <set>
+#include <thread>
 #include <unordered_map>
 
 namespace kate {
@@ -489,6 +490,32 @@ std::vector<PlannedPass> plan_relayout(int n, const std::vector<int>& phys0, con
 }
 
 std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out) {
+    if (opt.cap_search && !opt.c64) {
+        // One plan per cap, on its own thread.
+        const int caps[4] = {96, 112, 128, 144};
+        Plan plans[4];
+        std::string errs[4];
+        std::vector<std::thread> th;
+        for (int k = 0; k < 4; k++)
+            th.emplace_back([&, k] {
+                PlanOptions o = opt;
+                o.cap_search = false;
+                o.max_gates_per_pass = caps[k];
+                errs[k] = build_plan(prog, o, &plans[k]);
+            });
+        for (auto& t : th) t.join();
+        long best = -1;
+        int bk = -1;
+        for (int k = 0; k < 4; k++) {
+            if (!errs[k].empty()) continue;
+            long score = 0;
+            for (const auto& pp : plans[k].passes) score += pp.prog ? 1 : 10;
+            if (best < 0 || score < best) best = score, bk = k;
+        }
+        if (bk < 0) return errs[0];
+        *out = std::move(plans[bk]);
+        return "";
+    }
     Plan& plan = *out;
     const int n = prog.nqbits;
     plan = Plan();
@@ -536,6 +563,7 @@ std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out) {
     std::iota(rem.begin(), rem.end(), 0);
     const size_t scan_limit = 1u << 20;
     const size_t c64_scan_limit = 1u << 13;  // the block selector scans this window of the remaining gates
+    std::vector<uint64_t> qmask, tmask;      // per gate: its qubits, its tile qubits (remap search)
     while (!rem.empty()) {
         std::vector<char> inT(n, 0);
         int tsize = 0;
@@ -596,24 +624,55 @@ std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out) {
         std::sort(S.begin(), S.end());
         // Choose the qubits that the next pass wants at the low positions.
         std::vector<int> newlow;
-        if (opt.remap && opt.remap_search && !rem.empty() && !blocks && c > 0 && c < m) {
+        if (opt.remap && opt.remap_search && !rem.empty() && !blocks && c > 0 && c < m && n <= 64) {
             // Every c-subset of the tile (ascending logical ids, first best
             // kept): the one with which the next pass's greedy selection
             // takes the most gates.
+            // The count is greedy_pass's on qubit bitmasks (n <= 64).
             std::vector<int> T;
             for (int q = 0; q < n; q++)
                 if (inT[q]) T.push_back(q);
+            if (qmask.empty()) {
+                qmask.resize(plan.pgates.size());
+                tmask.resize(plan.pgates.size());
+                for (size_t g = 0; g < plan.pgates.size(); g++) {
+                    uint64_t a = 0, t = 0;
+                    for (int q : plan.pgates[g].tq) a |= 1ull << q, t |= 1ull << q;
+                    for (int q : plan.pgates[g].fq) a |= 1ull << q, t |= opt.c64 ? 1ull << q : 0ull;
+                    qmask[g] = a;
+                    tmask[g] = t;
+                }
+            }
+            const uint64_t all = n >= 64 ? ~0ull : (1ull << n) - 1;
+            auto count = [&](uint64_t low) {
+                uint64_t blocked = 0, inT2 = low;
+                int ts2 = __builtin_popcountll(low);
+                size_t got = 0, scanned = 0;
+                for (int gi : rem) {
+                    if (blocked == all || ++scanned > scan_limit) break;
+                    const uint64_t a = qmask[gi];
+                    if (!(a & blocked)) {
+                        const uint64_t need = tmask[gi] & ~inT2;
+                        const int nn = __builtin_popcountll(need);
+                        if (ts2 + nn <= mg) {
+                            inT2 |= need;
+                            ts2 += nn;
+                            got++;
+                            continue;
+                        }
+                    }
+                    blocked |= a;
+                }
+                return got;
+            };
             std::vector<int> idx(c);
             std::iota(idx.begin(), idx.end(), 0);
             size_t best = 0;
-            std::vector<char> inT2(n, 0);
             const int nt = (int)T.size();
             while (true) {
-                std::fill(inT2.begin(), inT2.end(), 0);
-                for (int i : idx) inT2[T[i]] = 1;
-                int ts2 = c;
-                const size_t got =
-                    greedy_pass(plan.pgates, rem, n, mg, inT2, ts2, nullptr, scan_limit, opt.c64).size();
+                uint64_t low = 0;
+                for (int i : idx) low |= 1ull << T[i];
+                const size_t got = count(low);
                 if (got > best) {
                     best = got;
                     newlow.clear();

@@ -24,7 +24,11 @@
 // them and m - c more). With remap_search the planner tries every c-subset
 // of the tile and keeps the one that lets the next pass take the most
 // gates; otherwise it takes the first c tile qubits the next pass's greedy
-// selection reaches.
+// selection reaches. The pass count then depends on the gate cap per pass
+// in no monotone way (a cap cuts a pass's gates to a program-order prefix,
+// which changes what the next pass can reach); with cap_search the planner
+// plans with each of a few caps and keeps the plan with the fewest passes
+// (passes left without a register-staged program count as ten).
 #pragma once
 
 #include <cstdint>
@@ -44,6 +48,7 @@ struct PlanOptions {
     int coalesce = 4;    // c: low physical bits every tile must contain
     bool remap = true;   // move next-needed qubits into the low bits on write
     bool remap_search = false;  // choose those qubits by trying every c-subset of the tile
+    bool cap_search = false;    // plan with several gate caps per pass, keep the plan with the fewest passes
     bool fuse_1q = true; // multiply chains of single-qubit ops on one qubit (FP64, host)
     bool staged = true;  // build register-staged programs for the tile kernel
     bool c64 = false;    // complex64 state: passes become dense 5-qubit tensor-core blocks

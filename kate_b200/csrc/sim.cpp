@@ -162,10 +162,12 @@ std::string Simulator::create(const Program& prog_in, int precision, int device,
         impl->opt.dense2_reg = precision == 0 && !(jv && std::atoi(jv) == 0);
     }
     // Complex128 passes choose the qubits they move into the low bits by
-    // trying every subset (a few ms of planning for a 30-qubit circuit).
+    // trying every subset, and the gate cap per pass among a few (about
+    // 0.1 s of planning for a 30-qubit, 1780-gate circuit).
     {
         const char* rs = std::getenv("KATE_REMAP_SEARCH");
         impl->opt.remap_search = precision == 0 && !(rs && std::atoi(rs) == 0);
+        impl->opt.cap_search = impl->opt.remap_search;
     }
     // Contiguous low physical bits every tile holds (runs of 2^c amplitudes per access).
     if (const char* e = std::getenv("KATE_COALESCE")) {
@@ -175,7 +177,7 @@ std::string Simulator::create(const Program& prog_in, int precision, int device,
     // Gates a pass may take at most (the planner packs greedily up to it).
     if (const char* e = std::getenv("KATE_MAX_GATES")) {
         const int v = std::atoi(e);
-        if (v >= 1 && v <= 96) impl->opt.max_gates_per_pass = v;
+        if (v >= 1 && v <= 160) impl->opt.max_gates_per_pass = v, impl->opt.cap_search = false;
     }
     std::string e = build_plan(impl->prog, impl->opt, &impl->plan);
     if (!e.empty()) return fail(e);
@@ -697,6 +699,12 @@ int Simulator::pass_kernel(int i) const {
     if (p.prog && (size_t)i < S.jit_fn.size() && S.jit_fn[i]) return 2;
     if (p.prog) return 1;
     return 0;
+}
+
+bool Simulator::pass_work(int i, double out[3]) const {
+    if (pass_kernel(i) != 2) return false;
+    out[0] = 2.0 * 16.0;
+    return jit_pass_work(*d_->plan.passes[i].prog, &out[1], &out[2]);
 }
 
 std::string Simulator::state_device(void** dptr, int* phys) {

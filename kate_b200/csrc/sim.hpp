@@ -39,6 +39,10 @@ public:
     // staged interpreter, 2 pass-specialised kernel, 3 complex64 tensor-core
     // blocks; -1 for an index out of range.
     int pass_kernel(int i) const;
+    // Work per amplitude of pass i when a pass-specialised kernel runs it:
+    // out = {HBM bytes, FP64 instructions, shared-memory bytes}; false for
+    // other kernels.
+    bool pass_work(int i, double out[3]) const;
     // Complex64: ||psi||^2 of the last run's state before it was rescaled to
     // norm 1 (FP64 reduction on the device).
     std::string norm2_before_renorm(double* out);

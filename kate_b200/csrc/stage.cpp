@@ -380,51 +380,7 @@ std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n,
                     if (ok) Wb.push_back(t);
                 }
         }
-        // Thread map: lanes first — three low thread bits on tile bits of
-        // distinct residue mod 3 (conflict-free 16-byte accesses under the
-        // XOR swizzle of k_tile.cu), then the other lane bits ascending —
-        // then the warp bits.
-        std::vector<int> lanes, tb;
-        for (int t : nonR)
-            if (std::find(Wb.begin(), Wb.end(), t) == Wb.end()) lanes.push_back(t);
-        bool res_used[3] = {false, false, false};
-        for (int t : lanes)
-            if (tb.size() < 3 && !res_used[t % 3]) {
-                res_used[t % 3] = true;
-                tb.push_back(t);
-            }
-        for (int t : lanes)
-            if (std::find(tb.begin(), tb.end(), t) == tb.end()) tb.push_back(t);
-        for (int t : Wb) tb.push_back(t);
-        prevW = Wb;
-        prev_open = true;
-        auto regpos = [&](int t) { return (int)(std::find(R.begin(), R.end(), t) - R.begin()); };
-        auto thrpos = [&](int t) { return (int)(std::find(tb.begin(), tb.end(), t) - tb.begin()); };
         auto in_R = [&](int t) { return std::find(R.begin(), R.end(), t) != R.end(); };
-        if (out->nstages >= KATE_MAX_STAGES) return "pass program has too many stages";
-        const int si = out->nstages++;
-        for (int i = 0; i < 4; i++) out->srb[si][i] = (uint8_t)R[i];
-        for (int i = 0; i < 8; i++) out->stb[si][i] = (uint8_t)tb[i];
-        uint16_t* stab = out->stab[si];
-        auto swz = [](uint32_t i) { return i ^ (((i >> 3) ^ (i >> 6) ^ (i >> 9)) & 7u); };
-        for (int v = 0; v < 16; v++) {
-            uint32_t lo = 0, hi = 0;
-            for (int i = 0; i < 4; i++) {
-                if ((v >> i) & 1) lo |= 1u << tb[i];
-                if ((v >> i) & 1) hi |= 1u << tb[4 + i];
-            }
-            stab[v] = (uint16_t)(swz(lo) << 4);
-            stab[16 + v] = (uint16_t)(swz(hi) << 4);
-        }
-        uint32_t wnat[4];
-        for (int i = 0; i < 4; i++) wnat[i] = swz(1u << R[i]) << 4;
-        auto W = [&](uint32_t x) {
-            uint32_t r = 0;
-            for (int k = 0; k < 4; k++)
-                if ((x >> k) & 1u) r ^= wnat[k];
-            return r;
-        };
-
         // NOTs/CNOTs folded into addressing. An X is foldable when its
         // controls are either one register bit or only thread/coset bits.
         // It joins the load prefix when it commutes with every op kept in the
@@ -474,6 +430,80 @@ std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n,
         std::vector<int> body;
         for (int i : kept)
             if (std::find(suffix.begin(), suffix.end(), i) == suffix.end()) body.push_back(i);
+        // Thread map: lanes first — three low thread bits (the lanes of one
+        // quarter-warp phase of a 16-byte shared-memory access) on tile bits
+        // of distinct residue mod 3 (distinct bank groups under the XOR
+        // swizzle of the tile), then the other lane bits ascending — then
+        // the warp bits. Among such triples the one with the fewest control
+        // bits of NOTs folded into this stage's loads or stores is taken: a
+        // flip conditioned on a phase lane moves only some of the phase's
+        // addresses and can put two of them in one bank group. The first
+        // and the last stage keep tile bits 0..3 (physical bits 0..3) on
+        // lanes 0..3 for their 256-byte HBM runs.
+        uint32_t flipctl = 0;
+        for (int i : prefix)
+            if (!reg_ctl(L[i])) flipctl |= L[i].tctl;
+        for (int i : suffix)
+            if (!reg_ctl(L[i])) flipctl |= L[i].tctl;
+        std::vector<int> lanes, tb;
+        for (int t : nonR)
+            if (std::find(Wb.begin(), Wb.end(), t) == Wb.end()) lanes.push_back(t);
+        const bool edge = out->nstages == 0 || scheduled + (int)list.size() == N;
+        bool low4 = edge;
+        for (int t = 0; t < 4 && low4; t++)
+            if (std::find(lanes.begin(), lanes.end(), t) == lanes.end()) low4 = false;
+        int best = -1, bt[3] = {-1, -1, -1};
+        const int nl = (int)lanes.size();
+        for (int x = 0; x < nl; x++)
+            for (int y = x + 1; y < nl; y++)
+                for (int z = y + 1; z < nl; z++) {
+                    const int a = lanes[x], b2 = lanes[y], c2 = lanes[z];
+                    if (a % 3 == b2 % 3 || a % 3 == c2 % 3 || b2 % 3 == c2 % 3) continue;
+                    if (low4 && (a > 3 || b2 > 3 || c2 > 3)) continue;
+                    const int cost = (int)((flipctl >> a) & 1u) + (int)((flipctl >> b2) & 1u) + (int)((flipctl >> c2) & 1u);
+                    if (best < 0 || cost < best) best = cost, bt[0] = a, bt[1] = b2, bt[2] = c2;
+                }
+        if (best >= 0) {
+            for (int i = 0; i < 3; i++) tb.push_back(bt[i]);
+        } else {
+            bool res_used[3] = {false, false, false};
+            for (int t : lanes)
+                if (tb.size() < 3 && !res_used[t % 3]) {
+                    res_used[t % 3] = true;
+                    tb.push_back(t);
+                }
+        }
+        for (int t : lanes)
+            if (std::find(tb.begin(), tb.end(), t) == tb.end()) tb.push_back(t);
+        for (int t : Wb) tb.push_back(t);
+        prevW = Wb;
+        prev_open = true;
+        auto regpos = [&](int t) { return (int)(std::find(R.begin(), R.end(), t) - R.begin()); };
+        auto thrpos = [&](int t) { return (int)(std::find(tb.begin(), tb.end(), t) - tb.begin()); };
+        if (out->nstages >= KATE_MAX_STAGES) return "pass program has too many stages";
+        const int si = out->nstages++;
+        for (int i = 0; i < 4; i++) out->srb[si][i] = (uint8_t)R[i];
+        for (int i = 0; i < 8; i++) out->stb[si][i] = (uint8_t)tb[i];
+        uint16_t* stab = out->stab[si];
+        auto swz = [](uint32_t i) { return i ^ (((i >> 3) ^ (i >> 6) ^ (i >> 9)) & 7u); };
+        for (int v = 0; v < 16; v++) {
+            uint32_t lo = 0, hi = 0;
+            for (int i = 0; i < 4; i++) {
+                if ((v >> i) & 1) lo |= 1u << tb[i];
+                if ((v >> i) & 1) hi |= 1u << tb[4 + i];
+            }
+            stab[v] = (uint16_t)(swz(lo) << 4);
+            stab[16 + v] = (uint16_t)(swz(hi) << 4);
+        }
+        uint32_t wnat[4];
+        for (int i = 0; i < 4; i++) wnat[i] = swz(1u << R[i]) << 4;
+        auto W = [&](uint32_t x) {
+            uint32_t r = 0;
+            for (int k = 0; k < 4; k++)
+                if ((x >> k) & 1u) r ^= wnat[k];
+            return r;
+        };
+
 
         // Affine map x -> M x ^ sum_k g_k u_k of a folded X sequence on the
         // 4-bit register index: register CNOTs update M (and the lane vectors
