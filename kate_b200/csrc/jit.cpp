@@ -1,6 +1,7 @@
 // Pass-specialised group-pass kernels: source generation, NVRTC compilation
 // and launch. See jit.hpp.
 #include "jit.hpp"
+#include "plan.hpp"
 
 #include <cuda.h>
 #include <dlfcn.h>
@@ -177,21 +178,12 @@ bool jit_pass_work(const PassProg& P, double* fp64, double* smem) {
     double f = 0.0;
     for (int k = 0; k < P.nops; k++) {
         const SOp& op = P.ops[k];
-        switch (op.kind) {
-        case SOP_STAGE:
+        if (op.kind == SOP_STAGE) {
             if (first >= 0) exchanges++;
             if (first < 0) first = op.idx;
             last = op.idx;
-            break;
-        case SOP_U: f += 8; break;                          // row2: 2 DMUL + 6 DFMA per amplitude
-        case SOP_UR: case SOP_UX: f += 4; break;            // 2 DMUL + 2 DFMA
-        case SOP_URA: case SOP_URB: case SOP_UXA: case SOP_UXB: f += 2; break;  // 2 DFMA
-        case SOP_H: f += 3; break;                          // 2 DADD + 2 DMUL + 2 DFMA per pair
-        case SOP_U2: f += 16; break;                        // row4: 2 DMUL + 14 DFMA
-        case SOP_D1: case SOP_DR: f += 4; break;            // complex multiply: 2 DMUL + 2 DFMA
-        case SOP_PH: f += 4.0 / (double)(1u << __builtin_popcount(op.creg)); break;
-        default: break;
         }
+        f += sop_fp64_per_amp(op);
     }
     Gen g(P);
     double b = 32.0 * exchanges;

@@ -504,12 +504,32 @@ std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out) {
                 errs[k] = build_plan(prog, o, &plans[k]);
             });
         for (auto& t : th) t.join();
-        long best = -1;
+        // Estimated time per amplitude (B200 rates, ps): a pass is bound by
+        // HBM (32 B at 6.5 TB/s), FP64 issue (64 per SM-clock, 148 SMs,
+        // 1.9 GHz) or its shared-memory exchanges (32 B per amplitude each,
+        // 128 B per SM-clock); the on-chip terms carry the 1.5x that the
+        // heavy passes measure against them. Passes with shared-memory ops
+        // (interpreter) or without a register-staged program (generic
+        // kernel) count three and ten HBM passes.
+        auto cost = [](const PlannedPass& pp) {
+            const double hbm = 4.92;
+            if (!pp.prog) return 10 * hbm;
+            double f = 0;
+            int ex = -1;
+            for (int k = 0; k < pp.prog->nops; k++) {
+                const SOp& o = pp.prog->ops[k];
+                if (o.kind == SOP_SMEM) return 3 * hbm;
+                if (o.kind == SOP_STAGE) ex++;
+                f += sop_fp64_per_amp(o);
+            }
+            return std::max(hbm, 1.5 * std::max(0.0556 * f, 0.89 * std::max(ex, 0)));
+        };
+        double best = -1;
         int bk = -1;
         for (int k = 0; k < 4; k++) {
             if (!errs[k].empty()) continue;
-            long score = 0;
-            for (const auto& pp : plans[k].passes) score += pp.prog ? 1 : 10;
+            double score = 0;
+            for (const auto& pp : plans[k].passes) score += cost(pp);
             if (best < 0 || score < best) best = score, bk = k;
         }
         if (bk < 0) return errs[0];
@@ -565,6 +585,13 @@ std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out) {
     const size_t c64_scan_limit = 1u << 13;  // the block selector scans this window of the remaining gates
     std::vector<uint64_t> qmask, tmask;      // per gate: its qubits, its tile qubits (remap search)
     while (!rem.empty()) {
+      // A pass whose register-staged program would not fit (too many
+      // matrices or stages) is planned again with three quarters of its
+      // gates rather than left to the slower shared-memory ops.
+      const std::vector<int> rem0 = rem;
+      const size_t pool0 = plan.pool.size(), smem0 = plan.smem_ops.size();
+      size_t cap = (size_t)opt.max_gates_per_pass;
+      for (;;) {
         std::vector<char> inT(n, 0);
         int tsize = 0;
         for (int p = 0; p < c; p++) {
@@ -576,7 +603,7 @@ std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out) {
                                                   c64_scan_limit)
                                        : greedy_pass(plan.pgates, rem, n, mg, inT, tsize, nullptr, scan_limit, opt.c64);
         size_t keep = exec.size();
-        if (!blocks && (int)keep > opt.max_gates_per_pass) keep = opt.max_gates_per_pass;
+        if (!blocks && keep > cap) keep = cap;
         if (keep < exec.size()) {
             // Keep a prefix of the executable gates (a prefix of a
             // dependency-closed set in program order is dependency-closed).
@@ -742,6 +769,15 @@ std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out) {
             const size_t so = plan.smem_ops.size(), po = plan.pool.size();
             pp.prog_note = opt.dense2_reg ? build_pass_program(plan, pp, n, plan.smem_ops, plan.pool, prog.get(), true)
                                           : std::string("off");
+            if (!pp.prog_note.empty() && opt.dense2_reg && exec.size() > 8 &&
+                (pp.prog_note.find("too large") != std::string::npos ||
+                 pp.prog_note.find("too many") != std::string::npos)) {
+                rem = rem0;
+                plan.pool.resize(pool0);
+                plan.smem_ops.resize(smem0);
+                cap = exec.size() * 3 / 4;
+                continue;
+            }
             if (!pp.prog_note.empty()) {
                 plan.smem_ops.resize(so);
                 plan.pool.resize(po);
@@ -752,6 +788,8 @@ std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out) {
         plan.passes.push_back(std::move(pp));
         L.phys = nphys;
         for (int q = 0; q < n; q++) L.inv[L.phys[q]] = q;
+        break;
+      }
     }
     plan.final_phys = L.phys;
     return "";

@@ -68,6 +68,22 @@ struct PlannedPass {
     std::string prog_note;           // why the generic kernel runs this pass, if it does
 };
 
+// FP64 instructions per amplitude that the pass-specialised kernel spends
+// on register-staged op `o` (DFMA, DMUL, DADD as generated; NOTs are
+// register moves or address flips).
+inline double sop_fp64_per_amp(const SOp& o) {
+    switch (o.kind) {
+    case SOP_U: return 8;                                       // 2 DMUL + 6 DFMA
+    case SOP_UR: case SOP_UX: return 4;                         // 2 DMUL + 2 DFMA
+    case SOP_URA: case SOP_URB: case SOP_UXA: case SOP_UXB: return 2;  // 2 DFMA
+    case SOP_H: return 3;                                       // 2 DADD + 2 DMUL + 2 DFMA per pair
+    case SOP_U2: return 16;                                     // 2 DMUL + 14 DFMA
+    case SOP_D1: case SOP_DR: return 4;                         // complex multiply
+    case SOP_PH: return 4.0 / (double)(1u << __builtin_popcount(o.creg));
+    default: return 0;
+    }
+}
+
 // A gate as the planner sees it (logical qubits).
 struct PGate {
     int kind = 0;             // OPK_* from device_types.h

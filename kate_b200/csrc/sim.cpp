@@ -161,12 +161,16 @@ std::string Simulator::create(const Program& prog_in, int precision, int device,
         const char* jv = std::getenv("KATE_JIT");
         impl->opt.dense2_reg = precision == 0 && !(jv && std::atoi(jv) == 0);
     }
-    // Complex128 passes choose the qubits they move into the low bits by
-    // trying every subset, and the gate cap per pass among a few (about
-    // 0.1 s of planning for a 30-qubit, 1780-gate circuit).
+    // Complex128 passes of 27 qubits and more choose the qubits they move
+    // into the low bits by trying every subset, and the gate cap per pass
+    // among a few (about 15 ms of planning for a 30-qubit, 1780-gate
+    // circuit; below 27 qubits a pass takes under 0.7 ms and the search
+    // would cost more host time than it saves). KATE_REMAP_SEARCH=0 or 1
+    // forces it off or on.
     {
         const char* rs = std::getenv("KATE_REMAP_SEARCH");
-        impl->opt.remap_search = precision == 0 && !(rs && std::atoi(rs) == 0);
+        const bool on = rs ? std::atoi(rs) != 0 : prog_in.nqbits >= 27;
+        impl->opt.remap_search = precision == 0 && on;
         impl->opt.cap_search = impl->opt.remap_search;
     }
     // Contiguous low physical bits every tile holds (runs of 2^c amplitudes per access).

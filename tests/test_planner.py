@@ -86,6 +86,20 @@ def test_remap_search_packs_the_headline_into_fewer_passes():
         assert p["nops"] <= 144
 
 
+def test_remap_search_keeps_dense_two_qubit_gates_in_registers():
+    # A pass that packs more SU(4)s than the register program's matrix pool
+    # holds is planned again with fewer gates instead of falling back to
+    # shared-memory ops (which the pass-specialised kernels do not run).
+    SOP_SMEM = 2
+    pv = PlanView(K.Circuit(32, circuits.brickwork_su4(32, 20)), 12, 4, REMAP_SEARCH)
+    base = PlanView(K.Circuit(32, circuits.brickwork_su4(32, 20)), 12, 4, 0)
+    assert len(pv.passes) < len(base.passes)
+    for prog in pv.programs:
+        assert prog is not None
+        kinds = prog["ops"]["kind"][: int(prog["nops"])]
+        assert not (kinds == SOP_SMEM).any()
+
+
 def test_remap_search_layered_matches_oracle(oracle):
     n = 22
     gates = circuits.layered(n, 8, seed=5)
