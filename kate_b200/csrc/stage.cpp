@@ -359,9 +359,22 @@ std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n,
         // physical bits 0..3 and stay lanes, which keeps the first and last
         // stages' HBM accesses in 256-byte runs (worth more than a warp-local
         // boundary).
+        // The bits that must stay lanes 0..3: the first stage's loads read
+        // HBM in 256-byte runs when tile bits 0..3 (physical bits 0..3) are
+        // its lanes 0..3, and the last stage's stores write them when the
+        // tile bits that the write-back moves to physical bits 0..3
+        // (outsrc[0..3]) are. Other stages keep tile bits 0..3 off the warps.
+        const bool first_stage = out->nstages == 0;
+        const bool last_stage = scheduled + (int)list.size() == N;
+        uint32_t lowset = 0xFu;
+        if (last_stage && !first_stage) {
+            lowset = 0;
+            for (int i = 0; i < 4; i++) lowset |= 1u << out->outsrc[i];
+        }
+        auto is_low = [&](int t) { return ((lowset >> t) & 1u) != 0; };
         bool local_in = prev_open && prevW.size() == 3;
         for (int t : prevW)
-            if (!is_nonR(t) || t < 4) local_in = false;
+            if (!is_nonR(t) || is_low(t)) local_in = false;
         std::vector<int> Wb;
         if (local_in) {
             Wb = prevW;
@@ -376,7 +389,7 @@ std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n,
                 for (int k = (int)nonR.size() - 1; k >= 0 && Wb.size() < 3; k--) {
                     const int t = nonR[k];
                     if (std::find(Wb.begin(), Wb.end(), t) != Wb.end()) continue;
-                    const bool ok = pass2 == 0 ? (t >= 4 && !in_Rn(t)) : pass2 == 1 ? t >= 4 : true;
+                    const bool ok = pass2 == 0 ? (!is_low(t) && !in_Rn(t)) : pass2 == 1 ? !is_low(t) : true;
                     if (ok) Wb.push_back(t);
                 }
         }
@@ -438,8 +451,8 @@ std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n,
         // bits of NOTs folded into this stage's loads or stores is taken: a
         // flip conditioned on a phase lane moves only some of the phase's
         // addresses and can put two of them in one bank group. The first
-        // and the last stage keep tile bits 0..3 (physical bits 0..3) on
-        // lanes 0..3 for their 256-byte HBM runs.
+        // and the last stage keep their low bits (above) on lanes 0..3 for
+        // their 256-byte HBM runs.
         uint32_t flipctl = 0;
         for (int i : prefix)
             if (!reg_ctl(L[i])) flipctl |= L[i].tctl;
@@ -448,10 +461,10 @@ std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n,
         std::vector<int> lanes, tb;
         for (int t : nonR)
             if (std::find(Wb.begin(), Wb.end(), t) == Wb.end()) lanes.push_back(t);
-        const bool edge = out->nstages == 0 || scheduled + (int)list.size() == N;
+        const bool edge = first_stage || last_stage;
         bool low4 = edge;
-        for (int t = 0; t < 4 && low4; t++)
-            if (std::find(lanes.begin(), lanes.end(), t) == lanes.end()) low4 = false;
+        for (int t = 0; t < m && low4; t++)
+            if (is_low(t) && std::find(lanes.begin(), lanes.end(), t) == lanes.end()) low4 = false;
         int best = -1, bt[3] = {-1, -1, -1};
         const int nl = (int)lanes.size();
         for (int x = 0; x < nl; x++)
@@ -459,12 +472,17 @@ std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n,
                 for (int z = y + 1; z < nl; z++) {
                     const int a = lanes[x], b2 = lanes[y], c2 = lanes[z];
                     if (a % 3 == b2 % 3 || a % 3 == c2 % 3 || b2 % 3 == c2 % 3) continue;
-                    if (low4 && (a > 3 || b2 > 3 || c2 > 3)) continue;
+                    if (low4 && !(is_low(a) && is_low(b2) && is_low(c2))) continue;
                     const int cost = (int)((flipctl >> a) & 1u) + (int)((flipctl >> b2) & 1u) + (int)((flipctl >> c2) & 1u);
                     if (best < 0 || cost < best) best = cost, bt[0] = a, bt[1] = b2, bt[2] = c2;
                 }
         if (best >= 0) {
             for (int i = 0; i < 3; i++) tb.push_back(bt[i]);
+        } else if (low4) {
+            // No triple of distinct bank groups among the low bits: the
+            // 256-byte runs come first.
+            for (int t : lanes)
+                if (is_low(t)) tb.push_back(t);
         } else {
             bool res_used[3] = {false, false, false};
             for (int t : lanes)
@@ -473,6 +491,9 @@ std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n,
                     tb.push_back(t);
                 }
         }
+        if (low4)
+            for (int t : lanes)
+                if (is_low(t) && std::find(tb.begin(), tb.end(), t) == tb.end()) tb.push_back(t);
         for (int t : lanes)
             if (std::find(tb.begin(), tb.end(), t) == tb.end()) tb.push_back(t);
         for (int t : Wb) tb.push_back(t);
