@@ -4,6 +4,11 @@
 #include <algorithm>
 #include <cmath>
 #include <numeric>
+#include <atomic>
+#include <condition_variable>
+#include <functional>
+#include <memory>
+#include <mutex>
 #include <set>
 #include <thread>
 #include <unordered_map>
@@ -359,6 +364,84 @@ std::vector<int> c64_pass(const std::vector<PGate>& pg, const std::vector<int>& 
 
 }  // namespace
 
+namespace {
+
+// Evaluates f on every candidate on the calling thread and a few workers
+// (kept for one plan); out[k] = f(cands[k]).
+class CandPool {
+  public:
+    explicit CandPool(int workers) : workers_(workers) {
+        for (int i = 0; i < workers; i++) th_.emplace_back([this] { loop(); });
+    }
+    ~CandPool() {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto& t : th_) t.join();
+    }
+    template <typename F>
+    void run(const std::vector<uint64_t>& cands, F& f, std::vector<size_t>& out) {
+        out.assign(cands.size(), 0);
+        if (workers_ == 0) {
+            for (size_t k = 0; k < cands.size(); k++) out[k] = f(cands[k]);
+            return;
+        }
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            cands_ = &cands;
+            out_ = &out;
+            fn_ = [&f](uint64_t x) { return f(x); };
+            next_ = 0;
+            pending_ = workers_;
+            gen_++;
+        }
+        cv_.notify_all();
+        work();
+        std::unique_lock<std::mutex> lk(mu_);
+        done_.wait(lk, [&] { return pending_ == 0; });
+    }
+
+  private:
+    void work() {
+        for (size_t k; (k = next_.fetch_add(1)) < cands_->size();) (*out_)[k] = fn_((*cands_)[k]);
+    }
+    void loop() {
+        int seen = 0;
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
+                if (stop_) return;
+                seen = gen_;
+            }
+            work();
+            std::lock_guard<std::mutex> lk(mu_);
+            if (--pending_ == 0) done_.notify_one();
+        }
+    }
+    int workers_;
+    std::vector<std::thread> th_;
+    std::mutex mu_;
+    std::condition_variable cv_, done_;
+    const std::vector<uint64_t>* cands_ = nullptr;
+    std::vector<size_t>* out_ = nullptr;
+    std::function<size_t(uint64_t)> fn_;
+    std::atomic<size_t> next_{0};
+    int gen_ = 0, pending_ = 0;
+    bool stop_ = false;
+};
+
+// Workers per plan for the remap search: the four cap plans run at once, so
+// a quarter of the host's threads each, the plan's own thread included.
+int search_workers() {
+    const int hw = (int)std::thread::hardware_concurrency();
+    return std::max(0, std::min(3, hw / 4 - 1));
+}
+
+}  // namespace
+
 DevPass to_devpass(int n, const PlannedPass& p, int op0) {
     DevPass d{};
     int m = (int)p.phys_in.size();
@@ -584,6 +667,7 @@ std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out) {
     const size_t scan_limit = 1u << 20;
     const size_t c64_scan_limit = 1u << 13;  // the block selector scans this window of the remaining gates
     std::vector<uint64_t> qmask, tmask;      // per gate: its qubits, its tile qubits (remap search)
+    std::unique_ptr<CandPool> pool;          // threads that count the remap search's candidates
     while (!rem.empty()) {
       // A pass whose register-staged program would not fit (too many
       // matrices or stages) is planned again with three quarters of its
@@ -692,25 +776,31 @@ std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out) {
                 }
                 return got;
             };
+            std::vector<uint64_t> cands;
             std::vector<int> idx(c);
             std::iota(idx.begin(), idx.end(), 0);
-            size_t best = 0;
             const int nt = (int)T.size();
             while (true) {
                 uint64_t low = 0;
                 for (int i : idx) low |= 1ull << T[i];
-                const size_t got = count(low);
-                if (got > best) {
-                    best = got;
-                    newlow.clear();
-                    for (int i : idx) newlow.push_back(T[i]);
-                }
+                cands.push_back(low);
                 int i = c - 1;
                 while (i >= 0 && idx[i] == nt - c + i) i--;
                 if (i < 0) break;
                 idx[i]++;
                 for (int j = i + 1; j < c; j++) idx[j] = idx[j - 1] + 1;
             }
+            std::vector<size_t> got;
+            if (!pool) pool.reset(new CandPool(search_workers()));
+            pool->run(cands, count, got);
+            size_t best = 0;
+            for (size_t k = 0; k < cands.size(); k++)
+                if (got[k] > best) {
+                    best = got[k];
+                    newlow.clear();
+                    for (int q = 0; q < n; q++)
+                        if ((cands[k] >> q) & 1ull) newlow.push_back(q);
+                }
         } else if (opt.remap && !rem.empty()) {
             std::vector<char> inT2(n, 0);
             int ts2 = 0;
