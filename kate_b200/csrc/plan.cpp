@@ -873,6 +873,29 @@ std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out) {
                 plan.pool.resize(po);
                 pp.prog_note = build_pass_program(plan, pp, n, plan.smem_ops, plan.pool, prog.get(), false);
             }
+            if (pp.prog_note.empty() && opt.dense2_reg && opt.remap_search) {
+                // A first stage that keeps tile bits 0..3 out of its registers
+                // loads straight from HBM; kept when the program then needs
+                // fewer shared-memory round trips.
+                bool low_reg = false;
+                for (int i = 0; i < 4; i++) low_reg |= prog->nstages > 0 && prog->srb[0][i] < 4;
+                if (low_reg) {
+                    const size_t so2 = plan.smem_ops.size(), po2 = plan.pool.size();
+                    std::vector<DevOp> smem_alt(plan.smem_ops.begin(), plan.smem_ops.begin() + (long)so);
+                    std::vector<Cx> pool_alt(plan.pool.begin(), plan.pool.begin() + (long)po);
+                    auto alt = std::make_shared<PassProg>();
+                    const std::string e2 =
+                        build_pass_program(plan, pp, n, smem_alt, pool_alt, alt.get(), true, true);
+                    if (e2.empty() && prog_round_trips(*alt) < prog_round_trips(*prog)) {
+                        plan.smem_ops.swap(smem_alt);
+                        plan.pool.swap(pool_alt);
+                        prog = alt;
+                    } else {
+                        (void)so2;
+                        (void)po2;
+                    }
+                }
+            }
             if (pp.prog_note.empty()) pp.prog = prog;
         }
         plan.passes.push_back(std::move(pp));

@@ -117,8 +117,17 @@ std::vector<PlannedPass> plan_relayout(int n, const std::vector<int>& phys, cons
 
 // Register-staged program of a pass (12-qubit tiles). Non-register ops are
 // appended to smem_ops (their tables to pool). Returns "" on success.
+// low_first: the first stage takes no register among tile bits 0..3 while
+// it has ops without them, so that its lanes 0..3 can read HBM in 256-byte
+// runs (no copy-in through the shared tile).
 std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n, std::vector<DevOp>& smem_ops,
-                               std::vector<Cx>& pool, PassProg* out, bool dense2 = false);
+                               std::vector<Cx>& pool, PassProg* out, bool dense2 = false, bool low_first = false);
+
+// Shared-memory round trips of a register-staged program's tile: one per
+// stage boundary, one for a copy-in when the first stage's registers hold a
+// tile bit among 0..3, one for a write-back when the last stage's lanes 0..3
+// are not the tile bits that go to physical bits 0..3.
+int prog_round_trips(const PassProg& p);
 
 // Complex64 block program of a pass (12-qubit tiles); operand images are
 // appended to `pool`. Returns "" on success.

@@ -126,8 +126,22 @@ int classify_2x2(const Cx* m) {
     return real ? SOP_UR : rx ? SOP_UX : SOP_U;
 }
 
+int prog_round_trips(const PassProg& p) {
+    if (p.nstages <= 0) return 0;
+    int r = p.nstages - 1;
+    for (int i = 0; i < 4; i++)
+        if (p.srb[0][i] < 4) {
+            r++;
+            break;
+        }
+    const int l = p.nstages - 1;
+    uint32_t want = 0, have = 0;
+    for (int i = 0; i < 4; i++) want |= 1u << p.outsrc[i], have |= 1u << p.stb[l][i];
+    return r + (want != have ? 1 : 0);
+}
+
 std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n, std::vector<DevOp>& smem_ops,
-                               std::vector<Cx>& pool, PassProg* out, bool dense2) {
+                               std::vector<Cx>& pool, PassProg* out, bool dense2, bool low_first) {
     const int m = (int)pass.phys_in.size();
     if (m != KATE_TILE_BITS) return "register-staged kernel needs 12-qubit tiles";
     const std::vector<int>& phys = pass.phys_before;
@@ -277,7 +291,7 @@ std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n,
     for (int i = 0; i < N; i++)
         for (int p : preds[i]) succs[p].push_back(i);
     std::vector<int> npend(N);
-    auto select = [&](const std::vector<char>& base, std::vector<int>& R, std::vector<int>& list) {
+    auto select = [&](const std::vector<char>& base, std::vector<int>& R, std::vector<int>& list, uint32_t avoid) {
         std::vector<int> rdy;
         for (int i = 0; i < N; i++) {
             int c = 0;
@@ -302,7 +316,9 @@ std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n,
             if (at == rdy.size() && R.size() < 4)
                 for (size_t k = 0; k < rdy.size() && at == rdy.size(); k++) {
                     const int i = rdy[k];
-                    if (regable(i) && L[i].tgt >= 0 && R.size() + missing(i) <= 4) {
+                    const bool avoided = (L[i].tgt >= 0 && !in_R(L[i].tgt) && ((avoid >> L[i].tgt) & 1u)) ||
+                                         (L[i].tgt2 >= 0 && !in_R(L[i].tgt2) && ((avoid >> L[i].tgt2) & 1u));
+                    if (regable(i) && L[i].tgt >= 0 && R.size() + missing(i) <= 4 && !avoided) {
                         at = k;
                         if (!in_R(L[i].tgt)) R.push_back(L[i].tgt);
                         if (L[i].tgt2 >= 0 && !in_R(L[i].tgt2)) R.push_back(L[i].tgt2);
@@ -316,9 +332,11 @@ std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n,
                 if (--npend[s] == 0 && !base[s]) rdy.insert(std::lower_bound(rdy.begin(), rdy.end(), s), s);
         }
     };
-    auto pad = [&](std::vector<int>& R) {
-        for (int t = 0; t < m && R.size() < 4; t++)
-            if (std::find(R.begin(), R.end(), t) == R.end()) R.push_back(t);
+    auto pad = [&](std::vector<int>& R, uint32_t avoid) {
+        for (int pass2 = 0; pass2 < 2; pass2++)
+            for (int t = 0; t < m && R.size() < 4; t++)
+                if ((pass2 == 1 || !((avoid >> t) & 1u)) && std::find(R.begin(), R.end(), t) == R.end())
+                    R.push_back(t);
     };
     // Warp bits (thread bits 5..7) of the previous stage, when its registers
     // are still open (no shared-memory op since): a stage that keeps them,
@@ -332,7 +350,13 @@ std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n,
     while (scheduled < N) {
         // Tentative register stage.
         std::vector<int> R, list;
-        select(done, R, list);
+        uint32_t avoid = low_first && out->nstages == 0 ? 0xFu : 0u;
+        select(done, R, list, avoid);
+        if (list.empty() && avoid) {
+            avoid = 0;
+            R.clear();
+            select(done, R, list, avoid);
+        }
         if (list.empty()) {
             int first = -1;
             for (int i = 0; i < N && first < 0; i++)
@@ -347,7 +371,7 @@ std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n,
             prev_open = false;
             continue;
         }
-        pad(R);
+        pad(R, avoid);
         std::vector<int> nonR;
         for (int t = 0; t < m; t++)
             if (std::find(R.begin(), R.end(), t) == R.end()) nonR.push_back(t);
@@ -382,8 +406,8 @@ std::string build_pass_program(const Plan& plan, const PlannedPass& pass, int n,
             std::vector<char> dn(done);
             for (int i : list) dn[i] = 1;
             std::vector<int> Rn, ln;
-            select(dn, Rn, ln);
-            if (!ln.empty()) pad(Rn);
+            select(dn, Rn, ln, 0);
+            if (!ln.empty()) pad(Rn, 0);
             auto in_Rn = [&](int t) { return std::find(Rn.begin(), Rn.end(), t) != Rn.end(); };
             for (int pass2 = 0; pass2 < 3 && Wb.size() < 3; pass2++)
                 for (int k = (int)nonR.size() - 1; k >= 0 && Wb.size() < 3; k--) {
