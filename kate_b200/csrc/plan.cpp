@@ -10,6 +10,7 @@
 #include <memory>
 #include <mutex>
 #include <set>
+#include <system_error>
 #include <thread>
 #include <unordered_map>
 
@@ -370,8 +371,15 @@ namespace {
 // (kept for one plan); out[k] = f(cands[k]).
 class CandPool {
   public:
-    explicit CandPool(int workers) : workers_(workers) {
-        for (int i = 0; i < workers; i++) th_.emplace_back([this] { loop(); });
+    explicit CandPool(int workers) : workers_(0) {
+        for (int i = 0; i < workers; i++) {
+            try {
+                th_.emplace_back([this] { loop(); });
+                workers_++;
+            } catch (const std::system_error&) {
+                break;  // fewer workers; the calling thread counts the rest
+            }
+        }
     }
     ~CandPool() {
         {
@@ -578,14 +586,24 @@ std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out) {
         const int caps[4] = {96, 112, 128, 144};
         Plan plans[4];
         std::string errs[4];
-        std::vector<std::thread> th;
-        for (int k = 0; k < 4; k++)
-            th.emplace_back([&, k] {
+        auto one = [&](int k) {
+            try {
                 PlanOptions o = opt;
                 o.cap_search = false;
                 o.max_gates_per_pass = caps[k];
                 errs[k] = build_plan(prog, o, &plans[k]);
-            });
+            } catch (const std::exception& e) {
+                errs[k] = std::string("planner: ") + e.what();
+            }
+        };
+        std::vector<std::thread> th;
+        for (int k = 0; k < 4; k++) {
+            try {
+                th.emplace_back(one, k);
+            } catch (const std::system_error&) {
+                one(k);  // no thread to spare: plan this cap here
+            }
+        }
         for (auto& t : th) t.join();
         // Estimated time per amplitude (B200 rates, ps): a pass is bound by
         // HBM (32 B at 6.5 TB/s), FP64 issue (64 per SM-clock, 148 SMs,
