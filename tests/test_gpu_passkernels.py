@@ -85,3 +85,42 @@ def test_product_state_start_matches_oracle(oracle, n, kind):
     sim.execute()
     assert np.abs(sim.state() - oracle.simulate(n, gates)).max() <= 1e-12
     sim.close()
+
+
+def test_remap_search_plan_runs_specialised_and_matches_oracle(oracle):
+    # The planner's remap and gate-cap search, forced at a size the oracle
+    # checks quickly: fewer passes, every one pass-specialised, same state.
+    n = 20
+    gates = circuits.layered(n, 12, seed=7)
+    old = os.environ.get("KATE_REMAP_SEARCH")
+    try:
+        os.environ["KATE_REMAP_SEARCH"] = "1"
+        a = K.Simulator(K.Circuit(n, gates), 1, K.C128, 0)
+        os.environ["KATE_REMAP_SEARCH"] = "0"
+        b = K.Simulator(K.Circuit(n, gates), 1, K.C128, 0)
+    finally:
+        if old is None:
+            del os.environ["KATE_REMAP_SEARCH"]
+        else:
+            os.environ["KATE_REMAP_SEARCH"] = old
+    assert len(a.pass_kernels()) < len(b.pass_kernels())
+    assert all(k == 2 for k in a.pass_kernels())
+    a.execute()
+    ref = oracle.simulate(n, gates)
+    assert np.abs(a.state() - ref).max() <= TOL
+
+
+def test_pass_work_counts():
+    # HBM bytes, FP64 instructions and shared-memory bytes per amplitude of
+    # each pass-specialised pass: 32 B of HBM; a layered pass applies
+    # rotations (FP64 > 0); shared memory moves 32 B per round trip.
+    n = 22
+    s = K.Simulator(K.Circuit(n, circuits.layered(n, 6, seed=3)), 1, K.C128, 0)
+    work = s.pass_work()
+    assert len(work) == len(s.pass_kernels())
+    for w, k in zip(work, s.pass_kernels()):
+        assert (w is not None) == (k == 2)
+        if w is not None:
+            hbm, fp64, smem = w
+            assert hbm == 32.0 and fp64 >= 0.0 and smem >= 0.0 and smem % 32.0 == 0.0
+    assert any(w[1] > 0 for w in work if w is not None)
