@@ -127,3 +127,40 @@ def test_product_form_of_first_passes_compiles():
         finally:
             L.kate_plan_destroy(h)
     assert seen, "no first pass had a product form"
+
+
+def test_searched_headline_plan_reads_and_writes_hbm_directly():
+    # With the planner's search (what 30-qubit complex128 simulators use),
+    # the first stage of most passes loads straight from HBM and the last
+    # stage stores straight to it (its lanes 0..3 hold the tile bits that
+    # the write-back moves to physical bits 0..3), so those passes skip the
+    # copy-in and write-back through the shared tile.
+    n = 30
+    c = K.Circuit(n, circuits.layered(n, 20, seed=1234))
+    L = _lib.lib()
+    h = ctypes.c_void_p()
+    assert L.kate_plan_create(c.handle, 12, 4, 16, ctypes.byref(h)) == 0
+    npass = ctypes.c_int()
+    L.kate_plan_num_passes(h, ctypes.byref(npass))
+    srcs = [source(L, h, i) for i in range(npass.value)]
+    L.kate_plan_destroy(h)
+    assert all(s for s in srcs)
+    direct_loads = sum("cp.async.cg" not in s for s in srcs)
+    direct_stores = sum("cpT" not in s for s in srcs)
+    assert npass.value <= 21
+    assert direct_loads >= 16 and direct_stores >= 15
+
+
+def test_stage_quarter_warp_lanes_lie_in_distinct_bank_groups():
+    # A 16-byte shared access is served per quarter warp: the three low
+    # lane bits of a stage must sit on tile bits of distinct residue mod 3
+    # (distinct bank groups under the tile's swizzle), or the exchange
+    # loads and stores take extra wavefronts.
+    from plan_emulator import PlanView
+    pv = PlanView(K.Circuit(30, circuits.layered(30, 20, seed=1234)), 12, 4, 16)
+    total = good = 0
+    for prog in pv.programs:
+        for si in range(int(prog["nstages"])):
+            total += 1
+            good += len({int(t) % 3 for t in prog["stb"][si][:3]}) == 3
+    assert total > 100 and good >= 0.95 * total
