@@ -898,7 +898,6 @@ std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out) {
                 bool low_reg = false;
                 for (int i = 0; i < 4; i++) low_reg |= prog->nstages > 0 && prog->srb[0][i] < 4;
                 if (low_reg) {
-                    const size_t so2 = plan.smem_ops.size(), po2 = plan.pool.size();
                     std::vector<DevOp> smem_alt(plan.smem_ops.begin(), plan.smem_ops.begin() + (long)so);
                     std::vector<Cx> pool_alt(plan.pool.begin(), plan.pool.begin() + (long)po);
                     auto alt = std::make_shared<PassProg>();
@@ -908,9 +907,6 @@ std::string build_plan(const Program& prog, const PlanOptions& opt, Plan* out) {
                         plan.smem_ops.swap(smem_alt);
                         plan.pool.swap(pool_alt);
                         prog = alt;
-                    } else {
-                        (void)so2;
-                        (void)po2;
                     }
                 }
             }
